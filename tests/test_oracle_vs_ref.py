@@ -1,0 +1,120 @@
+"""The CPU oracle against the reference compiled from its own sources.
+
+The reference's main() runs unchanged (oracle/ref_hooks.cpp), fed the same
+counter draw stream as the oracle.  Both are built with IEEE double and no
+FMA contraction, so every field must agree bit for bit.  Skipped where the
+reference build (oracle/_ref) is absent.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.skipif(not os.path.exists(O.ref_lib_path("small")),
+                                reason="reference build oracle/_ref/small not present")
+
+
+def _run_ref(stop, seed, want, **kw):
+    R = O.Reference("small")
+    snaps = {}
+
+    def cb(s):
+        if s in want:
+            snaps[s] = R.get_state(s)
+    vf, ef, tf = O.troph_files()
+    assert R.run(vf, ef, tf, 500, stop, seed=seed, on_step=cb, **kw) == 0
+    return R, snaps
+
+
+def _diff(a, b):
+    d = O.compare_states(a, b)
+    return {k: v for k, v in d.items() if v != 0}
+
+
+def test_init_prints_known_answers(capfd):
+    """maincode.cpp:256-257,345-346,366-368,446 printouts (seed-independent)."""
+    R, _ = _run_ref(0, 7, set())
+    out = capfd.readouterr().out
+    for line in ("Mean edge is:\t0.983753", "Standard deviation is:\t0.0948865", "Sarea:\t501.17",
+                 "Volume:\t840.892", "Shear modulus::\t1200", "Young's modulus::\t4711.11",
+                 "Poisson's ratio::\t0.962963", "no of vertices selected:\t500"):
+        assert line in out
+    orc = O.Oracle(R.p, 7)
+    V, E, T = O.load_mesh_files(*O.troph_files())
+    orc.init(V, E, T, 500)
+    rep = orc.report()
+    np.testing.assert_allclose(rep[:8], [0.983753, 0.0948865, 501.17, 840.892, 1200, 4711.11, 0.962963, 500],
+                               rtol=5e-6)
+
+
+def test_oracle_init_and_steps_bit_exact():
+    """Oracle set-up + 119 steps (12 collisions, one llist update at step 82,
+    bonds forming and breaking at raised rates) equal the reference."""
+    want = {0, 9, 10, 40, 81, 82, 83, 119}
+    R, snaps = _run_ref(119, 99, want, onrate=300.0, offrate=50.0)
+    V, E, T = O.load_mesh_files(*O.troph_files())
+    orc = O.Oracle(R.p, 99)
+    orc.init(V, E, T, 500)
+    orc.step_part1()
+    assert _diff(orc.get_state(), snaps[0]) == {}
+    M, M2 = R.get_mesh(), orc.get_mesh()
+    for k in M.a:
+        assert np.array_equal(M.a[k], M2.a[k]), k
+    orc.step_part2()
+    bonds_seen = set()
+    for s in range(1, 120):
+        orc.step_part1()
+        if s in snaps:
+            st = orc.get_state()
+            assert _diff(st, snaps[s]) == {}, s
+            bonds_seen.add(int(st.a["bondi"].sum()))
+            assert st.s["Sarea"] == snaps[s].s["Sarea"] and st.s["Volume"] == snaps[s].s["Volume"]
+            assert np.array_equal(st.s["paraV"], snaps[s].s["paraV"])
+        orc.step_part2()
+    assert max(bonds_seen) > 0
+
+
+def test_phase_functions_bit_exact():
+    """Each reference function called directly on the same state."""
+    R, snaps = _run_ref(30, 5, {19, 30}, onrate=300.0, offrate=50.0)
+    st = snaps[30]
+    M = R.get_mesh()
+    orc = O.Oracle(R.p, 5)
+    orc.set_mesh(M)
+    for name, call_ref, call_orc in (
+            ("collide", lambda: R.call_collide(31), lambda: orc.collide(31)),
+            ("llist", R.call_llist, orc.llist_update),
+            ("totalva", R.call_totalva, orc.total_va),
+            ("pfdt", R.call_pfdt, orc.pfdt),
+            ("forces", R.call_forces, orc.forces)):
+        R.set_state(st)
+        orc.set_state(st)
+        call_ref()
+        call_orc()
+        a, b = R.get_state(30), orc.get_state()
+        assert _diff(a, b) == {}, name
+        assert a.s["Sarea"] == b.s["Sarea"], name
+    # reflectionFed for every particle with a non-empty cell list
+    R.set_state(st)
+    orc.set_state(st)
+    fr = np.array([R.call_reflection(i) for i in range(st.ns)])
+    fo = np.array([orc.reflection(i) for i in range(st.ns)])
+    assert np.array_equal(fr, fo)
+    assert _diff(R.get_state(30), orc.get_state()) == {}
+
+
+def test_cubic_solver_matches_reference():
+    R = O.Reference("small")
+    rng = np.random.default_rng(3)
+    L = O.liboracle()
+    xs_r, xs_o = np.zeros(3), np.zeros(3)
+    for _ in range(2000):
+        a, b, c = rng.normal(size=3) * rng.choice([1e-3, 1, 1e3, 1e6])
+        nr = R.call_solvep3(xs_r.ctypes.data_as(O.D), a, b, c)
+        no = L.orc_solve_p3(xs_o.ctypes.data_as(O.D), a, b, c)
+        assert nr == no
+        assert np.array_equal(xs_r[:nr if nr > 1 else 3], xs_o[:nr if nr > 1 else 3])
+        assert R.call_solve(a, b, c) == L.orc_solve_cubic(a, b, c) or (
+            np.isnan(R.call_solve(a, b, c)) and np.isnan(L.orc_solve_cubic(a, b, c)))
