@@ -1,0 +1,176 @@
+/*
+ * irbc.h -- C ABI of the B200 iRBC timestep library (libirbc.so).
+ *
+ * Drop-in for the step of Dasanna/iRBC-code.  The reference has no library
+ * interface: its step is the loop body of main() (maincode.cpp:461-764)
+ * acting on the globals of define.h:182-429 through the void functions of
+ * Include/solfuncs.h:19-30 and Include/memfuncs.h:49-64.  Each entry point
+ * below names the reference code it replaces.  A handle owns all device
+ * memory of one simulation; one host thread drives a handle at a time;
+ * handles are independent.  Every call returns 0 on success or a negative
+ * status; irbc_last_error() gives the message.  Sizes are plain integers,
+ * arrays are caller-owned host memory, nothing here exposes CUDA or torch
+ * types.
+ */
+#ifndef IRBC_H
+#define IRBC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IRBC_OK 0
+#define IRBC_ERR_ARG -1      /* invalid argument or size                    */
+#define IRBC_ERR_CUDA -2     /* CUDA runtime error (device fault, no device)  */
+#define IRBC_ERR_STATE -3    /* call out of order (no mesh, no solvent)       */
+#define IRBC_ERR_CAPACITY -4 /* a list outgrew its capacity                   */
+#define IRBC_ERR_IO -5       /* file could not be written                     */
+
+#define IRBC_FP64 0          /* all solvent arithmetic in double               */
+#define IRBC_FP32 1          /* solvent state and arithmetic in float          */
+
+/* Runtime form of the compile-time parameters of define.h:35-73, the
+ * constants main() hard-codes (maincode.cpp:347-348, 463-470, 746) and the
+ * argv values (maincode.cpp:73-74).  irbc_params_default() fills the
+ * define.h values. */
+typedef struct irbc_params {
+  double a, Lx, Ly, Lz;          /* define.h:42-45                 */
+  int64_t Ns;                    /* define.h:46                    */
+  double dtcd, navg, Theta, walls, mass, cosalpha, sinalpha; /* define.h:47-54 */
+  int32_t Nt;                    /* define.h:57 (vertex count)     */
+  double kappasa, kappad, kappav, kappab, pmass, dtmd, ks, dthr, FD, Fg, el0; /* :59-69 */
+  double PRmass, paraR;          /* define.h:72-73                 */
+  double Pi;                     /* define.h:35 (3.141592653)      */
+  double elap, shear;            /* maincode.cpp:347-348           */
+  double onrate, offrate;        /* argv[1], argv[2]               */
+  int64_t warm_steps;            /* maincode.cpp:463 (250000)      */
+  double warm_speed;             /* maincode.cpp:465 (0.1)         */
+  int64_t out_every;             /* maincode.cpp:746 (5000)        */
+  int32_t randno;                /* define.h:37 (12345678)         */
+  int32_t pad_;
+  /* not in the reference */
+  uint64_t seed;                 /* key of the Philox draw stream  */
+  int32_t precision;             /* IRBC_FP64 or IRBC_FP32         */
+  int32_t device;                /* CUDA device ordinal            */
+} irbc_params;
+
+/* Static membrane topology (maincode.cpp:227-391): edges, edgest (bending
+ * partners), iedge, triangles with centroids (tricm) and rest areas. */
+typedef struct irbc_mesh {
+  int32_t nv, ne, nt, pad_;
+  int32_t *e1, *e2;
+  double *l0, *kappap;
+  int32_t *es1, *es2, *iedge;
+  int32_t *t1, *t2, *t3;
+  double *cmx, *cmy, *cmz, *tarea;
+  double Sarea0, Volume0, theta0;
+  double center[3];
+} irbc_mesh;
+
+/* Dynamic state in the reference's layout (define.h:82-139 fields as SoA).
+ * Solvent arrays are in the reference's particle order.  The cell ->
+ * triangle lists (Cells[].llist) are llen[ncell] plus their concatenation
+ * lidx[] (capacity lcap).  A NULL array pointer skips that group. */
+typedef struct irbc_view {
+  int64_t ns;
+  double *sx, *sy, *sz, *svx, *svy, *svz;
+  int32_t *spid, *sindio;
+  int32_t nv, pad0_;
+  double *x, *y, *z, *vx, *vy, *vz, *fx, *fy, *fz, *poff, *pon;
+  int32_t *pid, *ix, *iy, *bondi, *bondl, *knob;
+  double para[3], paraV[3], paraft[3], parafdt[3];
+  int32_t paradx, parady, paraid, nlig;
+  int32_t *ligi;
+  int64_t ncell;
+  int32_t *llen;
+  int64_t lcap;
+  int32_t *lidx;
+  double Sarea, Volume, wallspeed;
+  int64_t step;
+  int32_t colsteps, upd, filecc, filec;
+} irbc_view;
+
+typedef struct irbc_handle irbc_handle;
+
+/* ---- lifecycle --------------------------------------------------------- */
+void irbc_params_default(irbc_params* p);              /* define.h:35-73 */
+/* Allocates the simulation on p->device.  Replaces the global definitions of
+ * define.h:182-429 and the grid build of maincode.cpp:112-154. */
+int irbc_create(const irbc_params* p, irbc_handle** out);
+void irbc_destroy(irbc_handle* h);
+const char* irbc_last_error(const irbc_handle* h);
+/* bytes of device memory a simulation with these parameters needs (for
+ * admission by HBM footprint); nv/ne/nt are the mesh sizes */
+int64_t irbc_footprint_bytes(const irbc_params* p, int32_t nv, int32_t ne, int32_t nt);
+
+/* ---- set-up (maincode.cpp:94-446) -----------------------------------------
+ * V: nv*3 raw vertex coordinates as read from the vertex file; E: ne*2 and
+ * T: nt*3 zero-based indices.  Places the cell (maincode.cpp:196-206), builds
+ * edges/edgest/iedge/kappap/tarea (:239-375), draws vertex, parasite and
+ * solvent velocities and positions from the INIT stream, classifies the
+ * solvent inside/outside (Src/solfuncs.cpp:17-94, on the GPU), builds the
+ * cell lists (llistupdate) and places the knobs (:394-433). */
+int irbc_init(irbc_handle* h, const double* V, int32_t nv, const int32_t* E, int32_t ne,
+              const int32_t* T, int32_t nt, int32_t nknobs);
+/* diagnostics main() prints during set-up (maincode.cpp:256-257, 345-346,
+ * 366-368, 446): mean edge, std edge, Sarea0, Volume0, shear, Young,
+ * Poisson, knob count, theta0 */
+int irbc_init_report(const irbc_handle* h, double out[9]);
+
+/* ---- state exchange ---------------------------------------------------- */
+int irbc_set_mesh(irbc_handle* h, const irbc_mesh* m);
+int irbc_get_mesh(irbc_handle* h, irbc_mesh* m);
+int irbc_set_state(irbc_handle* h, const irbc_view* v);
+int irbc_get_state(irbc_handle* h, irbc_view* v);
+int64_t irbc_llist_total(irbc_handle* h);
+int64_t irbc_ncell(const irbc_handle* h);
+int32_t irbc_nlig(const irbc_handle* h);
+
+/* ---- the step ---------------------------------------------------------------
+ * irbc_step runs n reference timesteps (maincode.cpp:461-764).  The split
+ * entry points run the halves either side of the TotalVA call at
+ * maincode.cpp:602 (part 1 = :462-602, part 2 = :603-762). */
+int irbc_step(irbc_handle* h, int64_t n);
+int irbc_step_part1(irbc_handle* h);
+int irbc_step_part2(irbc_handle* h);
+
+/* ---- single phases ------------------------------------------------------------ */
+int irbc_collide(irbc_handle* h, int64_t epoch);   /* CollisionStep, Src/solfuncs.cpp:109-323 */
+int irbc_llist_update(irbc_handle* h);             /* llistupdate, Src/solfuncs.cpp:326-365 */
+int irbc_stream(irbc_handle* h);                   /* maincode.cpp:510-562 + reflectionFed */
+int irbc_total_va(irbc_handle* h);                 /* TotalVA, Src/memfuncs.cpp:161-190 */
+int irbc_pfdt(irbc_handle* h);                     /* pfdt, Src/memfuncs.cpp:443-484 */
+int irbc_forces(irbc_handle* h);                   /* force_calculate_dt, Src/memfuncs.cpp:214-441 */
+int irbc_bond_dynamics(irbc_handle* h, int64_t epoch); /* bond prep + bond_dynamics, maincode.cpp:668-725,16-54 */
+
+/* ---- output (formats of maincode.cpp:749-753 and Src/memfuncs.cpp:590-626) ---- */
+int irbc_write_rbcdata(irbc_handle* h, const char* path, int32_t append);
+int irbc_write_stl(irbc_handle* h, const char* path);
+/* observables not in the reference: out[0..] = mean solvent kT, centre of
+ * mass x,y,z (unwrapped), Sarea, Volume, bond count */
+int irbc_observables(irbc_handle* h, double* out, int32_t nout);
+/* Couette profile: mean vx of the solvent per z-layer of height a, nbins = Lz/a */
+int irbc_velocity_profile(irbc_handle* h, double* out, int32_t nbins);
+
+/* ---- timing and host buffers (not in the reference) ------------------------------ */
+int irbc_sync(irbc_handle* h);
+/* kernel launches issued by this handle since creation */
+int64_t irbc_launch_count(const irbc_handle* h);
+/* CUDA-event timing on the handle's stream between begin and end.
+ * out[0] = ms begin->end, out[1] = ms in the streaming kernel, out[2] = its
+ * launches, out[3] = ms in the collision kernels, out[4] = collisions,
+ * out[5] = ms in the membrane kernels, out[6] = membrane steps, out[7] =
+ * kernel launches in the window */
+int irbc_profile_begin(irbc_handle* h);
+int irbc_profile_end(irbc_handle* h, double* out, int32_t nout);
+/* page-locked host memory for fast state exchange */
+void* irbc_host_alloc(size_t bytes);
+void irbc_host_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

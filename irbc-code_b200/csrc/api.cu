@@ -1,0 +1,1029 @@
+// api.cu -- the C ABI of include/irbc.h: one handle per simulation, the
+// host-side set-up that main() performs before its loop (maincode.cpp:
+// 94-446), state exchange in the reference's layout, the step sequence of
+// the loop body (maincode.cpp:461-764) and the output writers.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "irbc.h"
+#include "sim.h"
+
+using namespace irbc;
+
+namespace irbc {
+std::atomic<int64_t> g_launches{0};
+}
+
+struct irbc_handle {
+  irbc_params P{};
+  DevParams dp{};
+  Solvent s;
+  Cells c;
+  Membrane m;
+  cudaStream_t st = nullptr;
+  std::string err;
+  bool have_mesh = false;
+  int64_t step = 0;
+  int colsteps = -1, upd = 0, filecc = 0, filec = 0, bbi = 0;
+  int csteps = 10, uplist = 83;
+  double report[9] = {0};
+  std::vector<double> xlig, ylig;
+  double* obs = nullptr;  // device scratch for observables
+  int64_t launches0 = 0;
+  // CUDA-event profiling window
+  bool prof = false;
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<std::pair<int, size_t>> ev_marks;  // (category, index of the start event)
+  int64_t prof_launch0 = 0;
+};
+
+namespace {
+
+int fail(irbc_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(h, IRBC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, int64_t n) {
+  *p = nullptr;
+  if (n <= 0) n = 1;
+  return cudaMalloc((void**)p, sizeof(T) * (size_t)n);
+}
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+void fill_devparams(irbc_handle* h) {
+  const irbc_params& P = h->P;
+  DevParams& d = h->dp;
+  d.a = P.a; d.Lx = P.Lx; d.Ly = P.Ly; d.Lz = P.Lz; d.dtcd = P.dtcd; d.navg = P.navg;
+  d.Theta = P.Theta; d.walls = P.walls; d.mass = P.mass; d.cosalpha = P.cosalpha; d.sinalpha = P.sinalpha;
+  d.kappasa = P.kappasa; d.kappad = P.kappad; d.kappav = P.kappav; d.kappab = P.kappab; d.pmass = P.pmass;
+  d.dtmd = P.dtmd; d.ks = P.ks; d.dthr = P.dthr; d.FD = P.FD; d.Fg = P.Fg; d.el0 = P.el0;
+  d.PRmass = P.PRmass; d.paraR = P.paraR; d.Pi = P.Pi; d.elap = P.elap; d.onrate = P.onrate;
+  d.offrate = P.offrate; d.randno = P.randno; d.seed = P.seed;
+  d.nx = (int)(P.Lx / P.a);
+  d.ny = (int)(P.Ly / P.a);
+  d.nz = (int)(P.Lz / P.a) + 1;
+  d.ncell = (int64_t)d.nx * d.ny * d.nz;
+}
+
+// ligand grid (maincode.cpp:77-93)
+void build_ligands(irbc_handle* h) {
+  h->xlig.clear(); h->ylig.clear();
+  double xmin = 0.0, ymin = 0.0;
+  int ny = 0;
+  while (xmin < h->P.Lx) {
+    int k = 0;
+    while (ymin < h->P.Ly) { h->xlig.push_back(xmin); h->ylig.push_back(ymin); ymin += 0.5; ++k; }
+    ny = k;
+    xmin += 0.5; ymin = 0;
+  }
+  h->dp.nligy = ny;
+  h->dp.nlig = (int)h->xlig.size();
+  h->dp.nligx = ny ? h->dp.nlig / ny : 0;
+}
+
+void free_membrane(Membrane& m) {
+  for (double** p : {&m.x, &m.y, &m.z, &m.vx, &m.vy, &m.vz, &m.fx, &m.fy, &m.fz, &m.poff, &m.pon, &m.l0,
+                     &m.kappap, &m.tarea, &m.area, &m.vol, &m.tcx, &m.tcy, &m.tcz, &m.pair_d})
+    dfree(*p);
+  for (int** p : {&m.pid, &m.ix, &m.iy, &m.bondi, &m.bondl, &m.knob, &m.e1, &m.e2, &m.es1, &m.es2, &m.iedge,
+                  &m.t1, &m.t2, &m.t3, &m.inc_start, &m.inc, &m.npair, &m.pair_j})
+    dfree(*p);
+  dfree(m.vkey);
+}
+
+// Host copy of the membrane used during set-up.
+struct HostMesh {
+  int nv = 0, ne = 0, nt = 0;
+  std::vector<double> x, y, z, vx, vy, vz;
+  std::vector<int> ix, iy;
+  std::vector<int> e1, e2, es1, es2, iedge, t1, t2, t3;
+  std::vector<double> l0, kappap, tarea, cmx, cmy, cmz;
+  double Sarea0 = 0, Volume0 = 0, theta0 = 0, center[3] = {0, 0, 0};
+};
+
+inline void hcp(const double A[], const double B[], double C[]) {
+  C[0] = (A[1] * B[2]) - (B[1] * A[2]);
+  C[1] = (A[2] * B[0]) - (B[2] * A[0]);
+  C[2] = (A[0] * B[1]) - (B[0] * A[1]);
+}
+
+double h_areatri(const HostMesh& M, double Lx, double Ly, int p1, int p2, int p3) {
+  auto UX = [&](int v) { return M.x[v] + M.ix[v] * Lx; };
+  auto UY = [&](int v) { return M.y[v] + M.iy[v] * Ly; };
+  double A[3] = {UX(p2) - UX(p1), UY(p2) - UY(p1), M.z[p2] - M.z[p1]};
+  double B[3] = {UX(p3) - UX(p1), UY(p3) - UY(p1), M.z[p3] - M.z[p1]};
+  double eta[3];
+  hcp(A, B, eta);
+  return 0.5 * sqrt(eta[0] * eta[0] + eta[1] * eta[1] + eta[2] * eta[2]);
+}
+
+double h_voltri(const HostMesh& M, double Lx, double Ly, int p1, int p2, int p3) {
+  auto UX = [&](int v) { return M.x[v] + M.ix[v] * Lx; };
+  auto UY = [&](int v) { return M.y[v] + M.iy[v] * Ly; };
+  double A[3] = {UX(p1), UY(p1), M.z[p1]}, B[3] = {UX(p2), UY(p2), M.z[p2]}, C[3] = {UX(p3), UY(p3), M.z[p3]};
+  double Cn[3];
+  for (int k = 0; k < 3; ++k) Cn[k] = (A[k] + B[k] + C[k]) / 3.0;
+  double E1[3] = {UX(p2) - UX(p1), UY(p2) - UY(p1), M.z[p2] - M.z[p1]};
+  double E2[3] = {UX(p3) - UX(p1), UY(p3) - UY(p1), M.z[p3] - M.z[p1]};
+  double D[3];
+  hcp(E1, E2, D);
+  return (1.0 / 6.0) * ((D[0] * Cn[0]) + (D[1] * Cn[1]) + (D[2] * Cn[2]));
+}
+
+// edgest (maincode.cpp:276-342): the third vertex of the first and of the
+// last triangle (in file order) holding both ends of each edge.  A map from
+// the vertex pair to its triangles replaces the E x T scan.
+void build_edgest(HostMesh& M) {
+  M.es1.assign(M.ne, 0); M.es2.assign(M.ne, 0);
+  std::vector<std::vector<int>> vt(M.nv);
+  for (int j = 0; j < M.nt; ++j) { vt[M.t1[j]].push_back(j); vt[M.t2[j]].push_back(j); vt[M.t3[j]].push_back(j); }
+  for (int i = 0; i < M.ne; ++i) {
+    int l1 = M.e1[i], l2 = M.e2[i];
+    std::vector<int> both;
+    for (int j : vt[l1]) {
+      if (M.t1[j] == l2 || M.t2[j] == l2 || M.t3[j] == l2) both.push_back(j);
+    }
+    std::sort(both.begin(), both.end());
+    both.erase(std::unique(both.begin(), both.end()), both.end());
+    auto third = [&](int j, int& out) {
+      if (M.t1[j] != l1 && M.t1[j] != l2) out = M.t1[j];
+      if (M.t2[j] != l1 && M.t2[j] != l2) out = M.t2[j];
+      if (M.t3[j] != l1 && M.t3[j] != l2) out = M.t3[j];
+    };
+    if (!both.empty()) { third(both.front(), M.es1[i]); third(both.back(), M.es2[i]); }
+  }
+}
+
+// makeiedge (Src/memfuncs.cpp:533-588) after centerofmass (:55-74)
+void build_iedge(HostMesh& M, double Lx, double Ly, double Lz) {
+  double rr[3] = {0, 0, 0};
+  for (int i = 0; i < M.nv; ++i) { rr[0] += M.x[i] + M.ix[i] * Lx; rr[1] += M.y[i] + M.iy[i] * Ly; rr[2] += M.z[i]; }
+  M.center[0] = fmod(rr[0] / (double)M.nv, Lx);
+  M.center[1] = fmod(rr[1] / (double)M.nv, Ly);
+  M.center[2] = fmod(rr[2] / (double)M.nv, Lz);
+  M.iedge.assign(M.ne, 1);
+  for (int i = 0; i < M.ne; ++i) {
+    int l2 = M.e1[i], l3 = M.e2[i], l1 = M.es1[i], l4 = M.es2[i];
+    double a21[3] = {M.x[l2] - M.x[l1], M.y[l2] - M.y[l1], M.z[l2] - M.z[l1]};
+    double a31[3] = {M.x[l3] - M.x[l1], M.y[l3] - M.y[l1], M.z[l3] - M.z[l1]};
+    double a24[3] = {M.x[l2] - M.x[l4], M.y[l2] - M.y[l4], M.z[l2] - M.z[l4]};
+    double a34[3] = {M.x[l3] - M.x[l4], M.y[l3] - M.y[l4], M.z[l3] - M.z[l4]};
+    double t1[3], t2[3], eta[3], zeta[3];
+    t1[0] = (M.x[l1] + M.x[l2] + M.x[l3]) / 3.0; t1[1] = (M.y[l1] + M.y[l2] + M.y[l3]) / 3.0;
+    t1[2] = (M.z[l1] + M.z[l2] + M.z[l3]) / 3.0;
+    t2[0] = (M.x[l4] + M.x[l2] + M.x[l3]) / 3.0; t2[1] = (M.y[l4] + M.y[l2] + M.y[l3]) / 3.0;
+    t2[2] = (M.z[l4] + M.z[l2] + M.z[l3]) / 3.0;
+    hcp(a21, a31, eta);
+    hcp(a34, a24, zeta);
+    double che1 = eta[0] * (t1[0] - M.center[0]) + eta[1] * (t1[1] - M.center[1]) + eta[2] * (t1[2] - M.center[2]);
+    double che2 = zeta[0] * (t2[0] - M.center[0]) + zeta[1] * (t2[1] - M.center[1]) + zeta[2] * (t2[2] - M.center[2]);
+    if ((che1 >= 0) && (che2 >= 0)) M.iedge[i] = 1;
+    else if ((che1 < 0) && (che2 < 0)) M.iedge[i] = -1;
+    else M.iedge[i] = 1;
+  }
+}
+
+// per-vertex contribution lists in the order force_calculate_dt adds them
+void build_incidence(const HostMesh& M, std::vector<int>& start, std::vector<int>& inc) {
+  std::vector<std::vector<int>> L(M.nv);
+  auto enc = [](int kind, int role, int item) { return (kind << 30) | (role << 27) | item; };
+  for (int i = 0; i < M.ne; ++i) {
+    L[M.e1[i]].push_back(enc(0, 0, i));
+    L[M.e2[i]].push_back(enc(0, 1, i));
+  }
+  for (int i = 0; i < M.nt; ++i) {
+    L[M.t1[i]].push_back(enc(1, 0, i));
+    L[M.t2[i]].push_back(enc(1, 1, i));
+    L[M.t3[i]].push_back(enc(1, 2, i));
+  }
+  for (int i = 0; i < M.ne; ++i) {
+    int l2, l3;
+    if (M.iedge[i] == -1) { l3 = M.e1[i]; l2 = M.e2[i]; } else { l2 = M.e1[i]; l3 = M.e2[i]; }
+    int l1 = M.es1[i], l4 = M.es2[i];
+    L[l1].push_back(enc(2, 0, i));
+    L[l4].push_back(enc(2, 1, i));
+    L[l2].push_back(enc(2, 2, i));
+    L[l3].push_back(enc(2, 3, i));
+  }
+  start.assign(M.nv + 1, 0);
+  inc.clear();
+  for (int v = 0; v < M.nv; ++v) {
+    start[v] = (int)inc.size();
+    inc.insert(inc.end(), L[v].begin(), L[v].end());
+  }
+  start[M.nv] = (int)inc.size();
+}
+
+template <typename T>
+int up(irbc_handle* h, T* d, const std::vector<T>& v) {
+  if (v.empty()) return 0;
+  CK(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, h->st));
+  return 0;
+}
+template <typename T>
+int up(irbc_handle* h, T* d, const T* v, int64_t n) {
+  if (n <= 0) return 0;
+  CK(cudaMemcpyAsync(d, v, sizeof(T) * (size_t)n, cudaMemcpyHostToDevice, h->st));
+  return 0;
+}
+template <typename T>
+int down(irbc_handle* h, T* v, const T* d, int64_t n) {
+  if (n <= 0 || !v) return 0;
+  CK(cudaMemcpyAsync(v, d, sizeof(T) * (size_t)n, cudaMemcpyDeviceToHost, h->st));
+  return 0;
+}
+
+// allocates the membrane and uploads the topology
+int upload_mesh(irbc_handle* h, const HostMesh& M) {
+  Membrane& m = h->m;
+  if (M.nv > 8192) return fail(h, IRBC_ERR_ARG, "at most 8192 membrane vertices");
+  free_membrane(m);
+  m.nv = M.nv; m.ne = M.ne; m.nt = M.nt;
+  for (double** p : {&m.x, &m.y, &m.z, &m.vx, &m.vy, &m.vz, &m.fx, &m.fy, &m.fz, &m.poff, &m.pon})
+    CK(dalloc(p, M.nv));
+  for (int** p : {&m.pid, &m.ix, &m.iy, &m.bondi, &m.bondl, &m.knob, &m.npair}) CK(dalloc(p, M.nv));
+  CK(dalloc(&m.vkey, M.nv));
+  CK(dalloc(&m.pair_d, (int64_t)M.nv * kMaxPairs));
+  CK(dalloc(&m.pair_j, (int64_t)M.nv * kMaxPairs));
+  for (int** p : {&m.e1, &m.e2, &m.es1, &m.es2, &m.iedge}) CK(dalloc(p, M.ne));
+  for (double** p : {&m.l0, &m.kappap}) CK(dalloc(p, M.ne));
+  for (int** p : {&m.t1, &m.t2, &m.t3}) CK(dalloc(p, M.nt));
+  for (double** p : {&m.tarea, &m.area, &m.vol, &m.tcx, &m.tcy, &m.tcz}) CK(dalloc(p, M.nt));
+  std::vector<int> start, inc;
+  build_incidence(M, start, inc);
+  CK(dalloc(&m.inc_start, M.nv + 1));
+  CK(dalloc(&m.inc, (int64_t)inc.size()));
+  if (up(h, m.inc_start, start) || up(h, m.inc, inc)) return IRBC_ERR_CUDA;
+  if (up(h, m.e1, M.e1) || up(h, m.e2, M.e2) || up(h, m.es1, M.es1) || up(h, m.es2, M.es2) ||
+      up(h, m.iedge, M.iedge) || up(h, m.l0, M.l0) || up(h, m.kappap, M.kappap) || up(h, m.t1, M.t1) ||
+      up(h, m.t2, M.t2) || up(h, m.t3, M.t3) || up(h, m.tarea, M.tarea))
+    return IRBC_ERR_CUDA;
+  CK(cudaMemsetAsync(m.npair, 0, sizeof(int) * M.nv, h->st));
+  h->dp.nv = M.nv; h->dp.ne = M.ne; h->dp.nt = M.nt;
+  h->dp.Sarea0 = M.Sarea0; h->dp.Volume0 = M.Volume0; h->dp.theta0 = M.theta0;
+  // cos/sin(theta0*Pi/180) evaluated on the host exactly as the reference
+  // does inside its bending loop (Src/memfuncs.cpp:401)
+  h->dp.cth0 = cos(M.theta0 * h->P.Pi / 180.0);
+  h->dp.sth0 = sin(M.theta0 * h->P.Pi / 180.0);
+  h->have_mesh = true;
+  return 0;
+}
+
+int64_t launches_in(const irbc_handle* h) { return g_launches.load() - h->launches0; }
+
+// profiling: a pair of events around a launch group of a category
+enum { PROF_STREAM = 0, PROF_COLLIDE = 1, PROF_MEMBRANE = 2 };
+cudaEvent_t next_event(irbc_handle* h) {
+  if (h->ev_used == h->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    h->ev_pool.push_back(e);
+  }
+  return h->ev_pool[h->ev_used++];
+}
+struct ProfScope {
+  irbc_handle* h;
+  size_t idx;
+  ProfScope(irbc_handle* hh, int cat) : h(hh), idx(0) {
+    if (!h->prof) return;
+    idx = h->ev_used;
+    cudaEventRecord(next_event(h), h->st);
+    h->ev_marks.push_back({cat, idx});
+  }
+  ~ProfScope() {
+    if (h->prof) cudaEventRecord(next_event(h), h->st);
+  }
+};
+
+}  // namespace
+
+// ============================================================== C ABI ======
+extern "C" void irbc_params_default(irbc_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->a = 1.0; p->Lx = 60.0; p->Ly = 40.0; p->Lz = 40.0; p->Ns = 960000;
+  p->dtcd = 0.02; p->navg = 10.0; p->Theta = 1.0; p->walls = 3.0; p->mass = 1.0;
+  p->cosalpha = -0.70710678118; p->sinalpha = 0.70710678118;
+  p->Nt = 600; p->kappasa = 60000.0; p->kappad = 1200.0; p->kappav = 6000.0; p->kappab = 100.0;
+  p->pmass = 10.0 * 1.0; p->dtmd = 0.002; p->ks = 6000.0; p->dthr = 0.50; p->FD = 1200.0;
+  p->Fg = 40.0; p->el0 = 0.1; p->PRmass = 10.0; p->paraR = 1.7; p->Pi = 3.141592653;
+  p->elap = 0.0005; p->shear = 1200.0; p->onrate = 0.005; p->offrate = 0.015;
+  p->warm_steps = 250000; p->warm_speed = 0.1; p->out_every = 5000; p->randno = 12345678;
+  p->seed = 12345; p->precision = IRBC_FP64; p->device = 0;
+}
+
+extern "C" int64_t irbc_footprint_bytes(const irbc_params* p, int32_t nv, int32_t ne, int32_t nt) {
+  int64_t nx = (int64_t)(p->Lx / p->a), ny = (int64_t)(p->Ly / p->a), nz = (int64_t)(p->Lz / p->a) + 1;
+  int64_t C = nx * ny * nz;
+  int64_t ns = p->Ns;
+  int64_t b = ns * (2 * (6 * 8 + 3 * 4) + 2 * 4);    // two buffer sets + key/slot
+  b += C * (6 * 4 + 7 * 8) + (C + 1) * 4 * 2;        // cells + llist starts
+  b += (int64_t)nv * (12 * 8 + 8 * 4 + kMaxPairs * 12) + (int64_t)ne * 40 + (int64_t)nt * 80;
+  b += 2 * (int64_t)(4 * p->Lx * 4 * p->Ly) * 16;    // ligands
+  b += 2 * C * 4 * 8;                                 // llist entries (typical)
+  return b;
+}
+
+extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
+  irbc_handle* h = nullptr;
+  if (!p || !out) return IRBC_ERR_ARG;
+  *out = nullptr;
+  if (p->Lx <= 0 || p->Ly <= 0 || p->Lz <= 0 || p->a != 1.0 || p->Ns < 0 || p->dtmd <= 0)
+    return IRBC_ERR_ARG;
+  if (p->precision != IRBC_FP64 && p->precision != IRBC_FP32) return IRBC_ERR_ARG;
+  int64_t nx = (int64_t)(p->Lx / p->a), ny = (int64_t)(p->Ly / p->a), nz = (int64_t)(p->Lz / p->a) + 1;
+  if (nx * ny * nz >= (1LL << 31) || p->Ns >= (1LL << 31)) return IRBC_ERR_ARG;
+  h = new irbc_handle();
+  h->P = *p;
+  cudaError_t e = cudaSetDevice(p->device);
+  if (e != cudaSuccess) { delete h; return IRBC_ERR_CUDA; }
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) { delete h; return IRBC_ERR_CUDA; }
+  fill_devparams(h);
+  build_ligands(h);
+  h->csteps = (int)(p->dtcd / p->dtmd);
+  h->uplist = (int)(0.5 / (p->walls * p->dtmd));
+  Solvent& s = h->s;
+  Cells& c = h->c;
+  s.n = p->Ns;
+  c.n = h->dp.ncell;
+  int rc = 0;
+  auto A = [&](cudaError_t err) { if (err != cudaSuccess && rc == 0) rc = IRBC_ERR_CUDA; };
+  for (double** q : {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.x2, &s.y2, &s.z2, &s.vx2, &s.vy2, &s.vz2})
+    A(dalloc(q, s.n));
+  for (int** q : {&s.id, &s.indio, &s.pid, &s.id2, &s.indio2, &s.pid2, &s.key, &s.slot}) A(dalloc(q, s.n));
+  for (int** q : {&c.cnt, &c.ncm, &c.wrank, &c.mrank, &c.lcnt}) A(dalloc(q, c.n));
+  A(dalloc(&c.start, c.n + 1));
+  A(dalloc(&c.lstart, c.n + 1));
+  A(dalloc(&c.lstart2, c.n + 1));
+  A(dalloc(&c.totals, 8));
+  A(dalloc(&c.par, c.n * 7));
+  c.scan_blocks = scan_part_blocks(c.n + 1);
+  A(dalloc(&c.scan_part, c.scan_blocks * 3 + 3));
+  c.lcap = c.lcap2 = std::max<int64_t>(1024, c.n / 16);
+  A(dalloc(&c.lidx, c.lcap));
+  A(dalloc(&c.lidx2, c.lcap2));
+  A(dalloc(&h->m.ligi, h->dp.nlig));
+  A(dalloc(&h->m.xlig, h->dp.nlig));
+  A(dalloc(&h->m.ylig, h->dp.nlig));
+  A(dalloc(&h->m.sc, 1));
+  A(dalloc(&h->obs, 64 + 4096));
+  if (rc) { irbc_destroy(h); return rc; }
+  cudaMemsetAsync(c.lstart, 0, sizeof(int) * (c.n + 1), h->st);
+  cudaMemsetAsync(h->m.ligi, 0, sizeof(int) * h->dp.nlig, h->st);
+  cudaMemsetAsync(h->m.sc, 0, sizeof(MemScalars), h->st);
+  cudaMemsetAsync(s.pid, 0, sizeof(int) * std::max<int64_t>(1, s.n), h->st);
+  cudaMemcpyAsync(h->m.xlig, h->xlig.data(), sizeof(double) * h->dp.nlig, cudaMemcpyHostToDevice, h->st);
+  cudaMemcpyAsync(h->m.ylig, h->ylig.data(), sizeof(double) * h->dp.nlig, cudaMemcpyHostToDevice, h->st);
+  if (cudaStreamSynchronize(h->st) != cudaSuccess) { irbc_destroy(h); return IRBC_ERR_CUDA; }
+  // the vertex bitonic sort stages up to 8192 keys in dynamic shared memory
+  h->launches0 = g_launches.load();
+  *out = h;
+  return 0;
+}
+
+extern "C" void irbc_destroy(irbc_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->P.device);
+  if (h->st) cudaStreamSynchronize(h->st);
+  Solvent& s = h->s;
+  Cells& c = h->c;
+  for (double** q : {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.x2, &s.y2, &s.z2, &s.vx2, &s.vy2, &s.vz2})
+    dfree(*q);
+  for (int** q : {&s.id, &s.indio, &s.pid, &s.id2, &s.indio2, &s.pid2, &s.key, &s.slot}) dfree(*q);
+  for (int** q : {&c.cnt, &c.ncm, &c.wrank, &c.mrank, &c.lcnt, &c.start, &c.lstart, &c.lstart2, &c.totals,
+                  &c.scan_part, &c.lidx, &c.lidx2})
+    dfree(*q);
+  dfree(c.par);
+  free_membrane(h->m);
+  dfree(h->m.ligi); dfree(h->m.xlig); dfree(h->m.ylig); dfree(h->m.sc); dfree(h->obs);
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  if (h->ev_begin) cudaEventDestroy(h->ev_begin);
+  if (h->ev_end) cudaEventDestroy(h->ev_end);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+}
+
+extern "C" const char* irbc_last_error(const irbc_handle* h) { return h ? h->err.c_str() : "null handle"; }
+extern "C" int64_t irbc_ncell(const irbc_handle* h) { return h ? h->dp.ncell : -1; }
+extern "C" int32_t irbc_nlig(const irbc_handle* h) { return h ? h->dp.nlig : -1; }
+extern "C" int64_t irbc_launch_count(const irbc_handle* h) { return h ? launches_in(h) : -1; }
+extern "C" int irbc_sync(irbc_handle* h) {
+  if (!h) return IRBC_ERR_ARG;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+// ---- llist -----------------------------------------------------------------
+static int do_llist(irbc_handle* h) {
+  Cells& c = h->c;
+  int64_t need = launch_llist_count(h->dp, c, h->m, h->st);
+  g_launches += 3 + 3;
+  if (need > c.lcap2) {
+    dfree(c.lidx2);
+    c.lcap2 = need + need / 4 + 1024;
+    CK(dalloc(&c.lidx2, c.lcap2));
+  }
+  launch_llist_fill(h->dp, c, h->m, h->st);
+  g_launches += 1;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int irbc_llist_update(irbc_handle* h) {
+  if (!h) return IRBC_ERR_ARG;
+  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
+  return do_llist(h);
+}
+
+// ---- set-up ------------------------------------------------------------------
+extern "C" int irbc_init(irbc_handle* h, const double* V, int32_t nv, const int32_t* E, int32_t ne,
+                         const int32_t* T, int32_t nt, int32_t nknobs) {
+  if (!h || !V || !E || !T || nv <= 0 || ne <= 0 || nt <= 0) return IRBC_ERR_ARG;
+  if (nknobs < 0 || nknobs > nv) return fail(h, IRBC_ERR_ARG, "knob count must be in [0, nv]");
+  for (int i = 0; i < 2 * ne; ++i) if (E[i] < 0 || E[i] >= nv) return fail(h, IRBC_ERR_ARG, "edge index out of range");
+  for (int i = 0; i < 3 * nt; ++i) if (T[i] < 0 || T[i] >= nv) return fail(h, IRBC_ERR_ARG, "triangle index out of range");
+  cudaSetDevice(h->P.device);
+  const irbc_params& p = h->P;
+  const uint64_t seed = p.seed;
+  uint64_t k = 6 * (uint64_t)p.Ns;  // INIT draws after the solvent's
+  auto U = [&]() { return draw_uniform(seed, STREAM_INIT, 0, k++); };
+  // solvent (maincode.cpp:96-107) on the device
+  launch_init_solvent(h->dp, h->s, h->st);
+  g_launches += 1;
+  HostMesh M;
+  M.nv = nv; M.ne = ne; M.nt = nt;
+  M.x.resize(nv); M.y.resize(nv); M.z.resize(nv); M.vx.resize(nv); M.vy.resize(nv); M.vz.resize(nv);
+  M.ix.assign(nv, 0); M.iy.assign(nv, 0);
+  // vertices (maincode.cpp:171-206)
+  double vmax = sqrt(3.0 * p.Theta / (p.pmass));
+  std::vector<double> zcrds;
+  for (int i = 0; i < nv; ++i) {
+    zcrds.push_back(V[3 * i + 2]);
+    M.x[i] = V[3 * i]; M.y[i] = V[3 * i + 1]; M.z[i] = V[3 * i + 2];
+    M.vx[i] = -vmax + 2.0 * vmax * U();
+    M.vy[i] = -vmax + 2.0 * vmax * U();
+    M.vz[i] = -vmax + 2.0 * vmax * U();
+  }
+  std::sort(zcrds.begin(), zcrds.end());
+  double Center[3];
+  Center[2] = -zcrds.front() + 0.3;
+  Center[0] = p.Lx / 2.0 + 10.0;
+  Center[1] = p.Ly / 2.0;
+  for (int i = 0; i < nv; ++i) { M.x[i] += Center[0]; M.y[i] += Center[1]; M.z[i] += Center[2]; }
+  double numer = 1.73205080757 * ((double)nv - 2.0) - 5.0 * p.Pi;
+  double denom = 1.73205080757 * ((double)nv - 2.0) - 3.0 * p.Pi;
+  M.theta0 = 180.0 * acos(numer / denom) / p.Pi;
+  // parasite (maincode.cpp:212-225)
+  MemScalars sc{};
+  sc.para[0] = Center[0] - 2.0; sc.para[1] = Center[1]; sc.para[2] = Center[2];
+  vmax = sqrt(3.0 * p.Theta / (p.PRmass));
+  for (int q = 0; q < 3; ++q) sc.paraV[q] = -vmax + 2.0 * vmax * U();
+  // edges (maincode.cpp:239-257)
+  M.e1.resize(ne); M.e2.resize(ne); M.l0.resize(ne); M.kappap.resize(ne);
+  double meanedge = 0, meanedge2 = 0;
+  for (int i = 0; i < ne; ++i) {
+    int a1 = E[2 * i], a2 = E[2 * i + 1];
+    M.e1[i] = a1; M.e2[i] = a2;
+    double distx = (M.x[a1] - M.x[a2]) * (M.x[a1] - M.x[a2]);
+    double disty = (M.y[a1] - M.y[a2]) * (M.y[a1] - M.y[a2]);
+    double distz = (M.z[a1] - M.z[a2]) * (M.z[a1] - M.z[a2]);
+    M.l0[i] = sqrt(distx + disty + distz);
+    meanedge += M.l0[i];
+    meanedge2 += M.l0[i] * M.l0[i];
+  }
+  h->report[0] = meanedge / (double)ne;
+  h->report[1] = sqrt((meanedge2 / (double)ne) - ((meanedge / (double)ne) * (meanedge / (double)ne)));
+  M.t1.resize(nt); M.t2.resize(nt); M.t3.resize(nt);
+  for (int i = 0; i < nt; ++i) { M.t1[i] = T[3 * i]; M.t2[i] = T[3 * i + 1]; M.t3[i] = T[3 * i + 2]; }
+  build_edgest(M);
+  // TotalVA0 (Src/memfuncs.cpp:192-211)
+  {
+    double totA = 0, totV = 0;
+    for (int i = 0; i < nt; ++i) {
+      totA += h_areatri(M, p.Lx, p.Ly, M.t1[i], M.t2[i], M.t3[i]);
+      totV += h_voltri(M, p.Lx, p.Ly, M.t1[i], M.t2[i], M.t3[i]);
+    }
+    M.Sarea0 = totA; M.Volume0 = totV;
+  }
+  // kappap (maincode.cpp:347-361)
+  for (int i = 0; i < ne; ++i) {
+    double ll0 = M.l0[i], lmax = 2.5 * ll0, x0 = ll0 / lmax, onemx0 = 1.0 - x0;
+    double shear1 = 1.0 / (4.0 * onemx0 * onemx0);
+    double shear2 = x0 / (2.0 * onemx0 * onemx0 * onemx0);
+    double shear4 = (1.732 / (4.0 * p.elap * lmax * x0));
+    double sh = shear4 * shear2 - shear4 * shear1 + shear4 * 0.25;
+    M.kappap[i] = (p.shear - sh) * 4.0 * ll0 * ll0 * ll0 / (3.0 * 1.732);
+  }
+  double areaC = 2.0 * p.shear + p.kappasa + p.kappad;
+  h->report[2] = M.Sarea0; h->report[3] = M.Volume0; h->report[4] = p.shear;
+  h->report[5] = (4.0 * areaC * p.shear) / (areaC + p.shear);
+  h->report[6] = (areaC - p.shear) / (areaC + p.shear);
+  h->report[8] = M.theta0;
+  M.tarea.resize(nt);
+  for (int i = 0; i < nt; ++i) M.tarea[i] = h_areatri(M, p.Lx, p.Ly, M.t1[i], M.t2[i], M.t3[i]);
+  build_iedge(M, p.Lx, p.Ly, p.Lz);
+  int rc = upload_mesh(h, M);
+  if (rc) return rc;
+  Membrane& m = h->m;
+  std::vector<int> zeros(nv, 0), randno(nv, p.randno);
+  std::vector<double> dz(nv, 0.0);
+  if (up(h, m.x, M.x) || up(h, m.y, M.y) || up(h, m.z, M.z) || up(h, m.vx, M.vx) || up(h, m.vy, M.vy) ||
+      up(h, m.vz, M.vz) || up(h, m.ix, zeros) || up(h, m.iy, zeros) || up(h, m.pid, zeros) ||
+      up(h, m.bondi, zeros) || up(h, m.bondl, randno) || up(h, m.knob, zeros) || up(h, m.fx, dz) ||
+      up(h, m.fy, dz) || up(h, m.fz, dz) || up(h, m.poff, dz) || up(h, m.pon, dz))
+    return IRBC_ERR_CUDA;
+  CK(cudaMemcpyAsync(m.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemsetAsync(m.ligi, 0, sizeof(int) * h->dp.nlig, h->st));
+  // TotalVA, pfdt, force_calculate_dt (maincode.cpp:385-387)
+  launch_total_va(h->dp, m, h->st);
+  launch_pfdt_forces(h->dp, m, 1, 1, 0, h->st);
+  g_launches += 4;
+  // inside/outside and the reference's sort permutation (Src/solfuncs.cpp:17-106)
+  launch_classify(h->dp, h->s, m, h->st);
+  g_launches += 2;
+  if (p.Ns > 0) {
+    std::vector<int> indio(p.Ns);
+    if (down(h, indio.data(), h->s.indio, p.Ns)) return IRBC_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->st));
+    struct K { int indio; int idx; bool operator<(const K& r) const { return indio < r.indio; } };
+    std::vector<K> keys(p.Ns);
+    for (int64_t i = 0; i < p.Ns; ++i) keys[i] = {indio[i], (int)i};
+    std::sort(keys.begin(), keys.end());
+    std::vector<int> id(p.Ns);
+    for (int64_t r = 0; r < p.Ns; ++r) id[keys[r].idx] = (int)r;
+    if (up(h, h->s.id, id)) return IRBC_ERR_CUDA;
+  }
+  // llistupdate (maincode.cpp:391) on empty lists
+  CK(cudaMemsetAsync(h->c.lstart, 0, sizeof(int) * (h->c.n + 1), h->st));
+  rc = do_llist(h);
+  if (rc) return rc;
+  // knobs (maincode.cpp:394-433): sequential draws on the host
+  std::vector<int> knob(nv, 0);
+  {
+    std::vector<double> parea;
+    for (int i = 0; i < nt; ++i) parea.push_back(M.tarea[i] / M.Sarea0);
+    int knob_count = 0;
+    while (knob_count < nknobs) {
+      double rad = U();
+      double aaa = 0;
+      for (int j = 0; j < nt; ++j) {
+        aaa += parea[j];
+        if (aaa > rad) {
+          // IRandom(1,3) (Src/mersenne.cpp:115-125)
+          int radi = int((double)(uint32_t)(3 - 1 + 1) * U() + 1);
+          if (radi > 3) radi = 3;
+          if ((radi == 1) && (knob[M.t1[j]] == 0)) { knob[M.t1[j]] = 1; knob_count += 1; break; }
+          else if ((radi == 2) && (knob[M.t2[j]] == 0)) { knob[M.t2[j]] = 1; knob_count += 1; break; }
+          else if ((radi == 3) && (knob[M.t3[j]] == 0)) { knob[M.t3[j]] = 1; knob_count += 1; break; }
+        }
+      }
+    }
+    h->report[7] = knob_count;
+  }
+  if (up(h, m.knob, knob)) return IRBC_ERR_CUDA;
+  h->step = 0; h->colsteps = -1; h->upd = 0; h->filecc = 0; h->filec = 0; h->bbi = 0;
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int irbc_init_report(const irbc_handle* h, double out[9]) {
+  if (!h || !out) return IRBC_ERR_ARG;
+  for (int k = 0; k < 9; ++k) out[k] = h->report[k];
+  return 0;
+}
+
+// ---- mesh / state exchange ---------------------------------------------------
+extern "C" int irbc_set_mesh(irbc_handle* h, const irbc_mesh* mm) {
+  if (!h || !mm || mm->nv <= 0) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
+  HostMesh M;
+  M.nv = mm->nv; M.ne = mm->ne; M.nt = mm->nt;
+  M.e1.assign(mm->e1, mm->e1 + mm->ne); M.e2.assign(mm->e2, mm->e2 + mm->ne);
+  M.es1.assign(mm->es1, mm->es1 + mm->ne); M.es2.assign(mm->es2, mm->es2 + mm->ne);
+  M.iedge.assign(mm->iedge, mm->iedge + mm->ne);
+  M.l0.assign(mm->l0, mm->l0 + mm->ne); M.kappap.assign(mm->kappap, mm->kappap + mm->ne);
+  M.t1.assign(mm->t1, mm->t1 + mm->nt); M.t2.assign(mm->t2, mm->t2 + mm->nt); M.t3.assign(mm->t3, mm->t3 + mm->nt);
+  M.tarea.assign(mm->tarea, mm->tarea + mm->nt);
+  M.Sarea0 = mm->Sarea0; M.Volume0 = mm->Volume0; M.theta0 = mm->theta0;
+  for (int k = 0; k < 3; ++k) M.center[k] = mm->center[k];
+  return upload_mesh(h, M);
+}
+
+extern "C" int irbc_get_mesh(irbc_handle* h, irbc_mesh* mm) {
+  if (!h || !mm) return IRBC_ERR_ARG;
+  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
+  const Membrane& m = h->m;
+  mm->nv = m.nv; mm->ne = m.ne; mm->nt = m.nt;
+  if (mm->e1) {
+    if (down(h, mm->e1, m.e1, m.ne) || down(h, mm->e2, m.e2, m.ne) || down(h, mm->l0, m.l0, m.ne) ||
+        down(h, mm->kappap, m.kappap, m.ne) || down(h, mm->es1, m.es1, m.ne) || down(h, mm->es2, m.es2, m.ne) ||
+        down(h, mm->iedge, m.iedge, m.ne))
+      return IRBC_ERR_CUDA;
+  }
+  if (mm->t1) {
+    if (down(h, mm->t1, m.t1, m.nt) || down(h, mm->t2, m.t2, m.nt) || down(h, mm->t3, m.t3, m.nt) ||
+        down(h, mm->tarea, m.tarea, m.nt))
+      return IRBC_ERR_CUDA;
+  }
+  mm->Sarea0 = h->dp.Sarea0; mm->Volume0 = h->dp.Volume0; mm->theta0 = h->dp.theta0;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+extern "C" int irbc_set_state(irbc_handle* h, const irbc_view* v) {
+  if (!h || !v) return IRBC_ERR_ARG;
+  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "set the mesh first");
+  if (v->ns != h->s.n) return fail(h, IRBC_ERR_ARG, "solvent count differs from Ns");
+  if (v->nv != h->m.nv) return fail(h, IRBC_ERR_ARG, "vertex count differs from the mesh");
+  if (v->ncell != h->dp.ncell || v->nlig != h->dp.nlig) return fail(h, IRBC_ERR_ARG, "grid size differs");
+  cudaSetDevice(h->P.device);
+  Solvent& s = h->s;
+  Membrane& m = h->m;
+  const int64_t n = s.n;
+  if (v->sx) {
+    std::vector<int> id(n);
+    for (int64_t i = 0; i < n; ++i) id[i] = (int)i;
+    if (up(h, s.x, v->sx, n) || up(h, s.y, v->sy, n) || up(h, s.z, v->sz, n) || up(h, s.vx, v->svx, n) ||
+        up(h, s.vy, v->svy, n) || up(h, s.vz, v->svz, n) || up(h, s.pid, v->spid, n) ||
+        up(h, s.indio, v->sindio, n) || up(h, s.id, id))
+      return IRBC_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->st));
+  }
+  const int nv = m.nv;
+  if (v->x) {
+    if (up(h, m.x, v->x, nv) || up(h, m.y, v->y, nv) || up(h, m.z, v->z, nv) || up(h, m.vx, v->vx, nv) ||
+        up(h, m.vy, v->vy, nv) || up(h, m.vz, v->vz, nv) || up(h, m.fx, v->fx, nv) || up(h, m.fy, v->fy, nv) ||
+        up(h, m.fz, v->fz, nv) || up(h, m.poff, v->poff, nv) || up(h, m.pon, v->pon, nv) ||
+        up(h, m.pid, v->pid, nv) || up(h, m.ix, v->ix, nv) || up(h, m.iy, v->iy, nv) ||
+        up(h, m.bondi, v->bondi, nv) || up(h, m.bondl, v->bondl, nv) || up(h, m.knob, v->knob, nv))
+      return IRBC_ERR_CUDA;
+  }
+  MemScalars sc{};
+  for (int k = 0; k < 3; ++k) {
+    sc.para[k] = v->para[k]; sc.paraV[k] = v->paraV[k]; sc.paraft[k] = v->paraft[k]; sc.parafdt[k] = v->parafdt[k];
+  }
+  sc.paradx = v->paradx; sc.parady = v->parady; sc.paraid = v->paraid;
+  sc.Sarea = v->Sarea; sc.Volume = v->Volume;
+  CK(cudaMemcpyAsync(m.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, h->st));
+  if (v->ligi && up(h, m.ligi, v->ligi, h->dp.nlig)) return IRBC_ERR_CUDA;
+  if (v->llen) {
+    Cells& c = h->c;
+    std::vector<int> start(c.n + 1, 0);
+    int64_t tot = 0;
+    for (int64_t i = 0; i < c.n; ++i) { start[i] = (int)tot; tot += v->llen[i]; }
+    start[c.n] = (int)tot;
+    if (tot > c.lcap) {
+      dfree(c.lidx);
+      c.lcap = tot + 1024;
+      CK(dalloc(&c.lidx, c.lcap));
+    }
+    if (up(h, c.lstart, start) || up(h, c.lidx, v->lidx, tot)) return IRBC_ERR_CUDA;
+  }
+  h->dp.wallspeed = v->wallspeed;
+  h->step = v->step; h->colsteps = v->colsteps; h->upd = v->upd; h->filecc = v->filecc; h->filec = v->filec;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+extern "C" int64_t irbc_llist_total(irbc_handle* h) {
+  if (!h) return IRBC_ERR_ARG;
+  int t = 0;
+  if (cudaMemcpy(&t, h->c.lstart + h->c.n, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return IRBC_ERR_CUDA;
+  return t;
+}
+
+extern "C" int irbc_get_state(irbc_handle* h, irbc_view* v) {
+  if (!h || !v) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
+  Solvent& s = h->s;
+  Membrane& m = h->m;
+  v->ns = s.n; v->nv = m.nv; v->ncell = h->dp.ncell; v->nlig = h->dp.nlig;
+  CK(cudaStreamSynchronize(h->st));
+  const int64_t n = s.n;
+  if (v->sx && n) {
+    std::vector<int> id(n);
+    std::vector<double> buf(n);
+    std::vector<int> ibuf(n);
+    if (down(h, id.data(), s.id, n)) return IRBC_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->st));
+    for (int64_t i = 0; i < n; ++i)
+      if (id[i] < 0 || id[i] >= n) return fail(h, IRBC_ERR_STATE, "corrupt particle ids");
+    auto pull = [&](double* dst, const double* src) -> int {
+      if (down(h, buf.data(), src, n)) return IRBC_ERR_CUDA;
+      if (cudaStreamSynchronize(h->st) != cudaSuccess) return IRBC_ERR_CUDA;
+      for (int64_t i = 0; i < n; ++i) dst[id[i]] = buf[i];
+      return 0;
+    };
+    auto pulli = [&](int* dst, const int* src) -> int {
+      if (down(h, ibuf.data(), src, n)) return IRBC_ERR_CUDA;
+      if (cudaStreamSynchronize(h->st) != cudaSuccess) return IRBC_ERR_CUDA;
+      for (int64_t i = 0; i < n; ++i) dst[id[i]] = ibuf[i];
+      return 0;
+    };
+    if (pull(v->sx, s.x) || pull(v->sy, s.y) || pull(v->sz, s.z) || pull(v->svx, s.vx) || pull(v->svy, s.vy) ||
+        pull(v->svz, s.vz) || pulli(v->spid, s.pid) || pulli(v->sindio, s.indio))
+      return IRBC_ERR_CUDA;
+  }
+  const int nv = m.nv;
+  if (v->x && nv) {
+    if (down(h, v->x, m.x, nv) || down(h, v->y, m.y, nv) || down(h, v->z, m.z, nv) || down(h, v->vx, m.vx, nv) ||
+        down(h, v->vy, m.vy, nv) || down(h, v->vz, m.vz, nv) || down(h, v->fx, m.fx, nv) ||
+        down(h, v->fy, m.fy, nv) || down(h, v->fz, m.fz, nv) || down(h, v->poff, m.poff, nv) ||
+        down(h, v->pon, m.pon, nv) || down(h, v->pid, m.pid, nv) || down(h, v->ix, m.ix, nv) ||
+        down(h, v->iy, m.iy, nv) || down(h, v->bondi, m.bondi, nv) || down(h, v->bondl, m.bondl, nv) ||
+        down(h, v->knob, m.knob, nv))
+      return IRBC_ERR_CUDA;
+  }
+  MemScalars sc{};
+  CK(cudaMemcpyAsync(&sc, m.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->st));
+  if (v->ligi && down(h, v->ligi, m.ligi, h->dp.nlig)) return IRBC_ERR_CUDA;
+  CK(cudaStreamSynchronize(h->st));
+  for (int k = 0; k < 3; ++k) {
+    v->para[k] = sc.para[k]; v->paraV[k] = sc.paraV[k]; v->paraft[k] = sc.paraft[k]; v->parafdt[k] = sc.parafdt[k];
+  }
+  v->paradx = sc.paradx; v->parady = sc.parady; v->paraid = sc.paraid;
+  v->Sarea = sc.Sarea; v->Volume = sc.Volume; v->wallspeed = h->dp.wallspeed;
+  if (v->llen) {
+    Cells& c = h->c;
+    std::vector<int> start(c.n + 1);
+    if (down(h, start.data(), c.lstart, c.n + 1)) return IRBC_ERR_CUDA;
+    CK(cudaStreamSynchronize(h->st));
+    for (int64_t i = 0; i < c.n; ++i) v->llen[i] = start[i + 1] - start[i];
+    if (v->lidx) {
+      if (start[c.n] > v->lcap) return fail(h, IRBC_ERR_CAPACITY, "lidx capacity too small");
+      if (down(h, v->lidx, c.lidx, start[c.n])) return IRBC_ERR_CUDA;
+    }
+  }
+  v->step = h->step; v->colsteps = h->colsteps; v->upd = h->upd; v->filecc = h->filecc; v->filec = h->filec;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+// ---- phases --------------------------------------------------------------------
+extern "C" int irbc_collide(irbc_handle* h, int64_t epoch) {
+  if (!h) return IRBC_ERR_ARG;
+  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
+  launch_collide(h->dp, h->s, h->c, h->m, (uint64_t)epoch, h->st);
+  g_launches += 10;
+  CK(cudaGetLastError());
+  return 0;
+}
+extern "C" int irbc_stream(irbc_handle* h) {
+  if (!h) return IRBC_ERR_ARG;
+  launch_stream(h->dp, h->s, h->c, h->m, h->st);
+  g_launches += 1;
+  CK(cudaGetLastError());
+  return 0;
+}
+extern "C" int irbc_total_va(irbc_handle* h) {
+  if (!h || !h->have_mesh) return IRBC_ERR_ARG;
+  launch_total_va(h->dp, h->m, h->st);
+  g_launches += 2;
+  CK(cudaGetLastError());
+  return 0;
+}
+extern "C" int irbc_pfdt(irbc_handle* h) {
+  if (!h || !h->have_mesh) return IRBC_ERR_ARG;
+  launch_pfdt_forces(h->dp, h->m, 1, 0, 0, h->st);
+  g_launches += 2;
+  CK(cudaGetLastError());
+  return 0;
+}
+extern "C" int irbc_forces(irbc_handle* h) {
+  if (!h || !h->have_mesh) return IRBC_ERR_ARG;
+  launch_pfdt_forces(h->dp, h->m, 0, 1, 0, h->st);
+  g_launches += 1;
+  CK(cudaGetLastError());
+  return 0;
+}
+extern "C" int irbc_bond_dynamics(irbc_handle* h, int64_t epoch) {
+  if (!h || !h->have_mesh) return IRBC_ERR_ARG;
+  launch_bonds(h->dp, h->m, (uint64_t)epoch, h->st);
+  g_launches += 2;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// maincode.cpp:462-602
+extern "C" int irbc_step_part1(irbc_handle* h) {
+  if (!h) return IRBC_ERR_ARG;
+  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
+  const irbc_params& p = h->P;
+  const int64_t s = h->step;
+  h->dp.wallspeed = (s < p.warm_steps) ? p.warm_speed : p.walls;
+  h->colsteps += 1; h->bbi += 1; h->upd += 1;
+  if (s > 0) h->filecc += 1;
+  if (h->colsteps == h->csteps) {
+    ProfScope ps(h, PROF_COLLIDE);
+    launch_collide(h->dp, h->s, h->c, h->m, (uint64_t)s, h->st);
+    g_launches += 10;
+    h->colsteps = 0;
+  }
+  {
+    ProfScope ps(h, PROF_MEMBRANE);
+    launch_half_kick(h->dp, h->m, h->st);
+    g_launches += 1;
+  }
+  if (h->upd == h->uplist) {
+    int rc = do_llist(h);
+    if (rc) return rc;
+    h->upd = 0;
+  }
+  {
+    ProfScope ps(h, PROF_STREAM);
+    launch_stream(h->dp, h->s, h->c, h->m, h->st);
+  }
+  {
+    ProfScope ps(h, PROF_MEMBRANE);
+    launch_drift(h->dp, h->m, h->st);
+    launch_total_va(h->dp, h->m, h->st);
+  }
+  g_launches += 4;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// maincode.cpp:603-762
+extern "C" int irbc_step_part2(irbc_handle* h) {
+  if (!h) return IRBC_ERR_ARG;
+  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
+  const int64_t s = h->step;
+  {
+    ProfScope ps(h, PROF_MEMBRANE);
+    launch_pfdt_forces(h->dp, h->m, 1, 1, 1, h->st);
+    launch_bonds(h->dp, h->m, (uint64_t)s, h->st);
+    launch_kick2(h->dp, h->m, h->st);
+  }
+  g_launches += 5;
+  if (h->filecc == h->P.out_every) { h->filec += 1; h->filecc = 0; }
+  h->step = s + 1;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int irbc_step(irbc_handle* h, int64_t n) {
+  if (!h || n < 0) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
+  for (int64_t k = 0; k < n; ++k) {
+    int rc = irbc_step_part1(h);
+    if (rc) return rc;
+    rc = irbc_step_part2(h);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+// ---- output ----------------------------------------------------------------------
+namespace {
+struct VertexCopy {
+  std::vector<double> x, y, z;
+  std::vector<int> ix, iy, bondi;
+};
+int pull_vertices(irbc_handle* h, VertexCopy& V) {
+  const Membrane& m = h->m;
+  V.x.resize(m.nv); V.y.resize(m.nv); V.z.resize(m.nv); V.ix.resize(m.nv); V.iy.resize(m.nv); V.bondi.resize(m.nv);
+  if (down(h, V.x.data(), m.x, m.nv) || down(h, V.y.data(), m.y, m.nv) || down(h, V.z.data(), m.z, m.nv) ||
+      down(h, V.ix.data(), m.ix, m.nv) || down(h, V.iy.data(), m.iy, m.nv) || down(h, V.bondi.data(), m.bondi, m.nv))
+    return IRBC_ERR_CUDA;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+}  // namespace
+
+// RBCdata record (maincode.cpp:749-753)
+extern "C" int irbc_write_rbcdata(irbc_handle* h, const char* path, int32_t append) {
+  if (!h || !path || !h->have_mesh) return IRBC_ERR_ARG;
+  VertexCopy V;
+  int rc = pull_vertices(h, V);
+  if (rc) return rc;
+  FILE* f = fopen(path, append ? "a" : "w");
+  if (!f) return fail(h, IRBC_ERR_IO, std::string("cannot open ") + path);
+  fprintf(f, "#%d\n", h->filec);
+  for (int i = 0; i < h->m.nv; ++i)
+    fprintf(f, "%lf\t%lf\t%lf\t%d\t%d\t%d\n", V.x[i], V.y[i], V.z[i], V.ix[i], V.iy[i], V.bondi[i]);
+  fclose(f);
+  return 0;
+}
+
+// STL surface (filewrite, Src/memfuncs.cpp:590-626): iostream default format
+extern "C" int irbc_write_stl(irbc_handle* h, const char* path) {
+  if (!h || !path || !h->have_mesh) return IRBC_ERR_ARG;
+  VertexCopy V;
+  int rc = pull_vertices(h, V);
+  if (rc) return rc;
+  const Membrane& m = h->m;
+  std::vector<int> t1(m.nt), t2(m.nt), t3(m.nt);
+  if (down(h, t1.data(), m.t1, m.nt) || down(h, t2.data(), m.t2, m.nt) || down(h, t3.data(), m.t3, m.nt))
+    return IRBC_ERR_CUDA;
+  CK(cudaStreamSynchronize(h->st));
+  std::ofstream f(path);
+  if (!f) return fail(h, IRBC_ERR_IO, std::string("cannot open ") + path);
+  const double Lx = h->P.Lx, Ly = h->P.Ly;
+  auto UX = [&](int q) { return V.x[q] + V.ix[q] * Lx; };
+  auto UY = [&](int q) { return V.y[q] + V.iy[q] * Ly; };
+  f << "solid ascii" << std::endl;
+  for (int kk = 0; kk < m.nt; ++kk) {
+    int l1 = t1[kk], l2 = t2[kk], l3 = t3[kk];
+    double A[3] = {UX(l2) - UX(l1), UY(l2) - UY(l1), V.z[l2] - V.z[l1]};
+    double B[3] = {UX(l3) - UX(l1), UY(l3) - UY(l1), V.z[l3] - V.z[l1]};
+    double N[3];
+    hcp(A, B, N);
+    f << "facet normal" << "\t" << N[0] << "\t" << N[1] << "\t" << N[2] << std::endl;
+    f << "outer loop" << std::endl;
+    f << "vertex" << "\t" << UX(l1) << "\t" << UY(l1) << "\t" << V.z[l1] << std::endl;
+    f << "vertex" << "\t" << UX(l2) << "\t" << UY(l2) << "\t" << V.z[l2] << std::endl;
+    f << "vertex" << "\t" << UX(l3) << "\t" << UY(l3) << "\t" << V.z[l3] << std::endl;
+    f << "endloop" << std::endl;
+    f << "endfacet" << std::endl;
+  }
+  f << "endsolid" << std::endl;
+  return 0;
+}
+
+extern "C" int irbc_observables(irbc_handle* h, double* out, int32_t nout) {
+  if (!h || !out || nout <= 0) return IRBC_ERR_ARG;
+  launch_observables(h->dp, h->s, h->m, h->obs, nullptr, 0, h->st);
+  g_launches += 2;
+  double buf[16] = {0};
+  CK(cudaMemcpyAsync(buf, h->obs, sizeof(double) * 16, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  for (int k = 0; k < nout && k < 16; ++k) out[k] = buf[k];
+  return 0;
+}
+
+extern "C" int irbc_velocity_profile(irbc_handle* h, double* out, int32_t nbins) {
+  if (!h || !out || nbins <= 0 || nbins > 2048) return IRBC_ERR_ARG;
+  launch_observables(h->dp, h->s, h->m, h->obs, h->obs + 64, nbins, h->st);
+  g_launches += 3;
+  std::vector<double> buf(2 * nbins);
+  CK(cudaMemcpyAsync(buf.data(), h->obs + 64, sizeof(double) * 2 * nbins, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  for (int k = 0; k < nbins; ++k) out[k] = buf[2 * k + 1] > 0 ? buf[2 * k] / buf[2 * k + 1] : 0.0;
+  return 0;
+}
+
+// ---- profiling window and host buffers ------------------------------------------------
+extern "C" int irbc_profile_begin(irbc_handle* h) {
+  if (!h) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
+  if (!h->ev_begin) { CK(cudaEventCreate(&h->ev_begin)); CK(cudaEventCreate(&h->ev_end)); }
+  h->ev_used = 0;
+  h->ev_marks.clear();
+  h->prof = true;
+  h->prof_launch0 = g_launches.load();
+  CK(cudaEventRecord(h->ev_begin, h->st));
+  return 0;
+}
+
+extern "C" int irbc_profile_end(irbc_handle* h, double* out, int32_t nout) {
+  if (!h || !out) return IRBC_ERR_ARG;
+  if (!h->prof) return fail(h, IRBC_ERR_STATE, "no profiling window open");
+  CK(cudaEventRecord(h->ev_end, h->st));
+  CK(cudaEventSynchronize(h->ev_end));
+  h->prof = false;
+  double r[8] = {0};
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->ev_begin, h->ev_end));
+  r[0] = ms;
+  for (auto& mk : h->ev_marks) {
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, h->ev_pool[mk.second], h->ev_pool[mk.second + 1]));
+    r[1 + 2 * mk.first] += t;
+    r[2 + 2 * mk.first] += 1;
+  }
+  r[7] = (double)(g_launches.load() - h->prof_launch0);
+  for (int k = 0; k < nout && k < 8; ++k) out[k] = r[k];
+  return 0;
+}
+
+extern "C" void* irbc_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+  return p;
+}
+extern "C" void irbc_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}

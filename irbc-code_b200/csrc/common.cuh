@@ -1,0 +1,92 @@
+// common.cuh -- device parameters, the Philox draw stream and the small
+// geometric helpers shared by the solvent and membrane kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace irbc {
+
+// Everything a kernel needs to know about one simulation, passed by value.
+struct DevParams {
+  double a, Lx, Ly, Lz, dtcd, navg, Theta, walls, mass, cosalpha, sinalpha;
+  double kappasa, kappad, kappav, kappab, pmass, dtmd, ks, dthr, FD, Fg, el0, PRmass, paraR;
+  double Pi, elap, onrate, offrate, wallspeed;
+  double Sarea0, Volume0, theta0, cth0, sth0;  // cos/sin(theta0*Pi/180) from the host libm
+  int nx, ny, nz;        // collision grid: Lx/a, Ly/a, Lz/a + 1 (maincode.cpp:113-115)
+  int64_t ncell;
+  int nv, ne, nt;
+  int nligx, nligy, nlig;  // ligand grid 0.5 apart (maincode.cpp:77-93)
+  int randno;
+  uint64_t seed;
+};
+
+// draw streams (counter word 3); the same numbering as the oracle's
+enum : uint32_t { STREAM_INIT = 1, STREAM_COLLIDE_U = 2, STREAM_COLLIDE_N = 3, STREAM_BOND = 4 };
+
+// Philox4x32-10 (Salmon et al., SC'11): 10 rounds of the published
+// multiply/xor round with the Weyl key schedule.
+__host__ __device__ inline void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                              uint32_t k0, uint32_t k1, uint32_t out[4]) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    c1 = (uint32_t)p1;
+    c3 = (uint32_t)p0;
+    c0 = n0;
+    c2 = n2;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+__host__ __device__ inline void draw_block(uint64_t seed, uint32_t stream, uint64_t epoch, uint64_t blk,
+                                           uint32_t out[4]) {
+  philox4x32_10((uint32_t)blk, (uint32_t)(blk >> 32), (uint32_t)epoch,
+                stream | ((uint32_t)(epoch >> 32) << 8), (uint32_t)seed, (uint32_t)(seed >> 32), out);
+}
+
+// k-th uniform of (stream, epoch): 32 random bits times 2^-32, the
+// resolution of the reference's Random() (Src/mersenne.cpp:108-112)
+__host__ __device__ inline double draw_uniform(uint64_t seed, uint32_t stream, uint64_t epoch, uint64_t k) {
+  uint32_t o[4];
+  draw_block(seed, stream, epoch, k >> 2, o);
+  return (double)o[k & 3u] * (1.0 / 4294967296.0);
+}
+
+// k-th standard normal: Box-Muller on block k
+__device__ inline double draw_normal(uint64_t seed, uint32_t stream, uint64_t epoch, uint64_t k) {
+  uint32_t o[4];
+  draw_block(seed, stream, epoch, k, o);
+  double u1 = ((double)o[0] + 1.0) * (1.0 / 4294967296.0);
+  double u2 = (double)o[1] * (1.0 / 4294967296.0);
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+// periodic wrap by repeated subtraction (bbound, Src/solfuncs.cpp:603-622)
+template <typename R>
+__device__ __forceinline__ R bbound(R x, R lx) {
+  if (x > lx) { while (x > lx) x -= lx; }
+  if (x < R(0)) { while (x < R(0)) x += lx; }
+  return x;
+}
+
+// cindex[fx][fy][fz] (maincode.cpp:112-136); entries never assigned are 0
+__device__ __forceinline__ int cell_of(const DevParams& p, int fx, int fy, int fz) {
+  if (fx >= 0 && fx < p.nx && fy >= 0 && fy < p.ny && fz >= 0 && fz < p.nz)
+    return (fx * p.ny + fy) * p.nz + fz;
+  return 0;
+}
+
+// cross product cp (Src/memfuncs.cpp:47-52)
+template <typename R>
+__device__ __forceinline__ void cp(const R A[3], const R B[3], R C[3]) {
+  C[0] = (A[1] * B[2]) - (B[1] * A[2]);
+  C[1] = (A[2] * B[0]) - (B[2] * A[0]);
+  C[2] = (A[0] * B[1]) - (B[0] * A[1]);
+}
+
+}  // namespace irbc

@@ -1,0 +1,89 @@
+// sim.h -- device-resident state of one simulation and the launchers of the
+// kernels that advance it.  Layout in HBM (FP64 build):
+//   solvent    SoA double x,y,z,vx,vy,vz + int id (reference index),
+//              indio, pid; kept physically sorted by collision cell (the
+//              counting sort of each collision writes the second buffer set)
+//   cells      int cnt, start (exclusive scan), ncm (membrane vertices),
+//              ghost ranks; 7 doubles of collision parameters per cell
+//   llist      CSR lstart[C+1], lidx[cap], double-buffered
+//   membrane   SoA vertex arrays, topology, per-vertex incidence lists
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace irbc {
+
+struct Solvent {
+  int64_t n = 0;
+  double *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  int *id = nullptr, *indio = nullptr, *pid = nullptr;
+  double *x2 = nullptr, *y2 = nullptr, *z2 = nullptr, *vx2 = nullptr, *vy2 = nullptr, *vz2 = nullptr;
+  int *id2 = nullptr, *indio2 = nullptr, *pid2 = nullptr;
+  int *key = nullptr, *slot = nullptr;
+};
+
+struct Cells {
+  int64_t n = 0;
+  int *cnt = nullptr, *start = nullptr, *ncm = nullptr, *wrank = nullptr, *mrank = nullptr;
+  int *totals = nullptr;        // [0] particles, [1] wall ghost cells, [2] membrane ghost cells, [3] llist entries
+  double *par = nullptr;        // 7 per cell: vcm[3], unit[3], ThE
+  int *lstart = nullptr, *lidx = nullptr, *lstart2 = nullptr, *lidx2 = nullptr, *lcnt = nullptr;
+  int64_t lcap = 0, lcap2 = 0;
+  int *scan_part = nullptr;     // scan scratch: 3 ints per block
+  int64_t scan_blocks = 0;
+};
+
+// device scalars of the membrane / parasite (one small struct)
+struct MemScalars {
+  double Sarea, Volume;
+  double para[3], paraV[3], paraft[3], parafdt[3];
+  int paradx, parady, paraid, pad;
+};
+
+struct Membrane {
+  int nv = 0, ne = 0, nt = 0;
+  double *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  double *fx = nullptr, *fy = nullptr, *fz = nullptr, *poff = nullptr, *pon = nullptr;
+  int *pid = nullptr, *ix = nullptr, *iy = nullptr, *bondi = nullptr, *bondl = nullptr, *knob = nullptr;
+  int *e1 = nullptr, *e2 = nullptr, *es1 = nullptr, *es2 = nullptr, *iedge = nullptr;
+  int *t1 = nullptr, *t2 = nullptr, *t3 = nullptr;
+  double *l0 = nullptr, *kappap = nullptr, *tarea = nullptr;
+  double *area = nullptr, *vol = nullptr;     // per triangle, TotalVA terms
+  double *tcx = nullptr, *tcy = nullptr, *tcz = nullptr;  // centroids for llistupdate
+  int *inc_start = nullptr, *inc = nullptr;   // per-vertex contributions in reference order
+  uint64_t *vkey = nullptr;                   // (cell << 32 | vertex), sorted each collision
+  int *npair = nullptr;                       // bond candidates per vertex
+  double *pair_d = nullptr;
+  int *pair_j = nullptr;
+  int *ligi = nullptr;
+  double *xlig = nullptr, *ylig = nullptr;   // ligand grid (maincode.cpp:77-93)
+  MemScalars* sc = nullptr;
+};
+
+constexpr int kMaxPairs = 64;        // bond candidates per vertex (<= 25 with dthr = 0.5)
+
+// ---- launchers (kernels.cu) ---------------------------------------------------
+void launch_init_solvent(const DevParams& p, Solvent& s, cudaStream_t st);
+void launch_classify(const DevParams& p, Solvent& s, const Membrane& m, cudaStream_t st);
+void launch_collide(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
+                    cudaStream_t st);
+void launch_stream(const DevParams& p, Solvent& s, const Cells& c, const Membrane& m, cudaStream_t st);
+// returns the total list length the update needs (host sync inside)
+int64_t launch_llist_count(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
+void launch_llist_fill(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
+void launch_half_kick(const DevParams& p, Membrane& m, cudaStream_t st);
+void launch_drift(const DevParams& p, Membrane& m, cudaStream_t st);
+void launch_total_va(const DevParams& p, Membrane& m, cudaStream_t st);
+void launch_pfdt_forces(const DevParams& p, Membrane& m, int do_pfdt, int do_forces, int do_ext,
+                        cudaStream_t st);
+void launch_bonds(const DevParams& p, Membrane& m, uint64_t epoch, cudaStream_t st);
+void launch_kick2(const DevParams& p, Membrane& m, cudaStream_t st);
+void launch_scan3(const int* a, const int* b, const int* c, int* oa, int* ob, int* oc, int* totals,
+                  int64_t n, int* part, cudaStream_t st);
+void launch_observables(const DevParams& p, const Solvent& s, const Membrane& m, double* out,
+                        double* prof, int nbins, cudaStream_t st);
+
+int64_t scan_part_blocks(int64_t n);
+
+}  // namespace irbc

@@ -1,0 +1,326 @@
+"""irbc_b200 -- Python access to libirbc.so (the B200 iRBC timestep).
+
+A thin ctypes layer over the C ABI of include/irbc.h, used by the tests,
+bench.py and the MAIN driver.  All arithmetic runs in the CUDA library; if
+libirbc.so is missing or cannot reach a GPU the calls raise, there is no
+fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libirbc.so")
+HEADER = os.path.join(ROOT, "include", "irbc.h")
+
+FP64, FP32 = 0, 1
+D = C.POINTER(C.c_double)
+I = C.POINTER(C.c_int32)
+
+
+class IrbcError(RuntimeError):
+    pass
+
+
+class Params(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("a", "Lx", "Ly", "Lz")] + [("Ns", C.c_int64)] + \
+        [(n, C.c_double) for n in ("dtcd", "navg", "Theta", "walls", "mass", "cosalpha", "sinalpha")] + \
+        [("Nt", C.c_int32)] + \
+        [(n, C.c_double) for n in ("kappasa", "kappad", "kappav", "kappab", "pmass", "dtmd", "ks",
+                                   "dthr", "FD", "Fg", "el0", "PRmass", "paraR", "Pi", "elap", "shear",
+                                   "onrate", "offrate")] + \
+        [("warm_steps", C.c_int64), ("warm_speed", C.c_double), ("out_every", C.c_int64),
+         ("randno", C.c_int32), ("pad_", C.c_int32), ("seed", C.c_uint64), ("precision", C.c_int32),
+         ("device", C.c_int32)]
+
+
+class Mesh(C.Structure):
+    _fields_ = [("nv", C.c_int32), ("ne", C.c_int32), ("nt", C.c_int32), ("pad_", C.c_int32),
+                ("e1", I), ("e2", I), ("l0", D), ("kappap", D), ("es1", I), ("es2", I), ("iedge", I),
+                ("t1", I), ("t2", I), ("t3", I), ("cmx", D), ("cmy", D), ("cmz", D), ("tarea", D),
+                ("Sarea0", C.c_double), ("Volume0", C.c_double), ("theta0", C.c_double),
+                ("center", C.c_double * 3)]
+
+
+class View(C.Structure):
+    _fields_ = [("ns", C.c_int64)] + [(n, D) for n in ("sx", "sy", "sz", "svx", "svy", "svz")] + \
+        [("spid", I), ("sindio", I), ("nv", C.c_int32), ("pad0_", C.c_int32)] + \
+        [(n, D) for n in ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "poff", "pon")] + \
+        [(n, I) for n in ("pid", "ix", "iy", "bondi", "bondl", "knob")] + \
+        [(n, C.c_double * 3) for n in ("para", "paraV", "paraft", "parafdt")] + \
+        [("paradx", C.c_int32), ("parady", C.c_int32), ("paraid", C.c_int32), ("nlig", C.c_int32),
+         ("ligi", I), ("ncell", C.c_int64), ("llen", I), ("lcap", C.c_int64), ("lidx", I),
+         ("Sarea", C.c_double), ("Volume", C.c_double), ("wallspeed", C.c_double),
+         ("step", C.c_int64), ("colsteps", C.c_int32), ("upd", C.c_int32), ("filecc", C.c_int32),
+         ("filec", C.c_int32)]
+
+
+def exported_names():
+    """Function names declared in include/irbc.h."""
+    import re
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(irbc_[a-z0-9_]+)\s*\(", txt)))
+
+
+_lib = None
+
+
+def lib():
+    """Loads libirbc.so (built by irbc-code_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise IrbcError("libirbc.so not built: run irbc-code_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    H = C.c_void_p
+    L.irbc_params_default.argtypes = [C.POINTER(Params)]
+    L.irbc_create.argtypes = [C.POINTER(Params), C.POINTER(H)]
+    L.irbc_destroy.argtypes = [H]
+    L.irbc_last_error.restype = C.c_char_p
+    L.irbc_last_error.argtypes = [H]
+    L.irbc_footprint_bytes.restype = C.c_int64
+    L.irbc_footprint_bytes.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, C.c_int32]
+    L.irbc_init.argtypes = [H, D, C.c_int32, I, C.c_int32, I, C.c_int32, C.c_int32]
+    L.irbc_init_report.argtypes = [H, D]
+    L.irbc_set_mesh.argtypes = [H, C.POINTER(Mesh)]
+    L.irbc_get_mesh.argtypes = [H, C.POINTER(Mesh)]
+    L.irbc_set_state.argtypes = [H, C.POINTER(View)]
+    L.irbc_get_state.argtypes = [H, C.POINTER(View)]
+    L.irbc_llist_total.restype = C.c_int64
+    L.irbc_llist_total.argtypes = [H]
+    L.irbc_ncell.restype = C.c_int64
+    L.irbc_ncell.argtypes = [H]
+    L.irbc_nlig.argtypes = [H]
+    for f in ("irbc_step", "irbc_collide", "irbc_bond_dynamics"):
+        getattr(L, f).argtypes = [H, C.c_int64]
+    for f in ("irbc_step_part1", "irbc_step_part2", "irbc_llist_update", "irbc_stream", "irbc_total_va",
+              "irbc_pfdt", "irbc_forces", "irbc_sync"):
+        getattr(L, f).argtypes = [H]
+    L.irbc_write_rbcdata.argtypes = [H, C.c_char_p, C.c_int32]
+    L.irbc_write_stl.argtypes = [H, C.c_char_p]
+    L.irbc_observables.argtypes = [H, D, C.c_int32]
+    L.irbc_velocity_profile.argtypes = [H, D, C.c_int32]
+    L.irbc_launch_count.restype = C.c_int64
+    L.irbc_launch_count.argtypes = [H]
+    L.irbc_profile_begin.argtypes = [H]
+    L.irbc_profile_end.argtypes = [H, D, C.c_int32]
+    L.irbc_host_alloc.restype = C.c_void_p
+    L.irbc_host_alloc.argtypes = [C.c_size_t]
+    L.irbc_host_free.argtypes = [C.c_void_p]
+    _lib = L
+    return L
+
+
+def default_params(**over):
+    p = Params()
+    lib().irbc_params_default(C.byref(p))
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+class State:
+    """Host copy of a simulation state in the reference's layout."""
+    SOLVENT_D = ("sx", "sy", "sz", "svx", "svy", "svz")
+    SOLVENT_I = ("spid", "sindio")
+    VERT_D = ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "poff", "pon")
+    VERT_I = ("pid", "ix", "iy", "bondi", "bondl", "knob")
+    PARA_V = ("para", "paraV", "paraft", "parafdt")
+    SCAL = ("paradx", "parady", "paraid", "Sarea", "Volume", "wallspeed", "step", "colsteps", "upd",
+            "filecc", "filec")
+
+    def __init__(self, ns, nv, nlig, ncell, lcap=1, solvent=True, llist=True):
+        self.ns, self.nv, self.nlig, self.ncell = ns, nv, nlig, ncell
+        self.a = {}
+        if solvent:
+            self.a.update({k: np.zeros(ns) for k in self.SOLVENT_D})
+            self.a.update({k: np.zeros(ns, np.int32) for k in self.SOLVENT_I})
+        self.a.update({k: np.zeros(nv) for k in self.VERT_D})
+        self.a.update({k: np.zeros(nv, np.int32) for k in self.VERT_I})
+        self.a["ligi"] = np.zeros(nlig, np.int32)
+        if llist:
+            self.a["llen"] = np.zeros(ncell, np.int32)
+            self.a["lidx"] = np.zeros(max(lcap, 1), np.int32)
+        self.s = {k: np.zeros(3) for k in self.PARA_V}
+        self.s.update({k: 0 for k in self.SCAL})
+
+    def view(self):
+        v = View()
+        v.ns, v.nv, v.nlig, v.ncell = self.ns, self.nv, self.nlig, self.ncell
+        for k, arr in self.a.items():
+            setattr(v, k, _p(arr, D if arr.dtype == np.float64 else I))
+        if "lidx" in self.a:
+            v.lcap = self.a["lidx"].size
+        for k in self.PARA_V:
+            getattr(v, k)[:] = [float(x) for x in self.s[k]]
+        for k in self.SCAL:
+            setattr(v, k, self.s[k])
+        return v
+
+    def absorb(self, v):
+        for k in self.PARA_V:
+            self.s[k] = np.array(getattr(v, k)[:])
+        for k in self.SCAL:
+            self.s[k] = getattr(v, k)
+
+    @classmethod
+    def from_other(cls, other):
+        """Copies any object with .a/.s dicts and ns/nv/nlig/ncell (e.g. an oracle state)."""
+        st = cls.__new__(cls)
+        st.ns, st.nv, st.nlig, st.ncell = other.ns, other.nv, other.nlig, other.ncell
+        st.a = {k: np.ascontiguousarray(v).copy() for k, v in other.a.items()}
+        st.s = {k: (np.array(v).copy() if isinstance(v, np.ndarray) else v) for k, v in other.s.items()}
+        return st
+
+
+class Simulation:
+    """One simulation on one GPU (a handle of libirbc.so)."""
+
+    def __init__(self, params):
+        self.L = lib()
+        self.params = params
+        self.h = C.c_void_p()
+        rc = self.L.irbc_create(C.byref(params), C.byref(self.h))
+        if rc != 0:
+            raise IrbcError("irbc_create failed (%d): no CUDA device or bad parameters" % rc)
+        self.ncell = int(self.L.irbc_ncell(self.h))
+        self.nlig = int(self.L.irbc_nlig(self.h))
+        self.nv = 0
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.L.irbc_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            raise IrbcError("%s failed (%d): %s" % (what, rc, self.L.irbc_last_error(self.h).decode()))
+
+    def init(self, V, E, T, nknobs):
+        V = np.ascontiguousarray(V, np.float64)
+        E = np.ascontiguousarray(E, np.int32)
+        T = np.ascontiguousarray(T, np.int32)
+        self._ck(self.L.irbc_init(self.h, _p(V, D), len(V), _p(E, I), len(E), _p(T, I), len(T), nknobs),
+                 "irbc_init")
+        self.nv = len(V)
+
+    def report(self):
+        out = np.zeros(9)
+        self._ck(self.L.irbc_init_report(self.h, _p(out, D)), "irbc_init_report")
+        return out
+
+    def set_mesh(self, M):
+        """M: object with .a dict (e1,e2,l0,kappap,es1,es2,iedge,t1,t2,t3,tarea,...) and .s scalars."""
+        m = Mesh()
+        m.nv, m.ne, m.nt = M.nv, M.ne, M.nt
+        keep = {}
+        for k in ("e1", "e2", "es1", "es2", "iedge", "t1", "t2", "t3"):
+            keep[k] = np.ascontiguousarray(M.a[k], np.int32)
+            setattr(m, k, _p(keep[k], I))
+        for k in ("l0", "kappap", "tarea", "cmx", "cmy", "cmz"):
+            keep[k] = np.ascontiguousarray(M.a[k], np.float64)
+            setattr(m, k, _p(keep[k], D))
+        m.Sarea0, m.Volume0, m.theta0 = M.s["Sarea0"], M.s["Volume0"], M.s["theta0"]
+        m.center[:] = [float(x) for x in M.s["center"]]
+        self._ck(self.L.irbc_set_mesh(self.h, C.byref(m)), "irbc_set_mesh")
+        self.nv = M.nv
+
+    def get_mesh_arrays(self):
+        m0 = Mesh()
+        self._ck(self.L.irbc_get_mesh(self.h, C.byref(m0)), "irbc_get_mesh")
+        a = {k: np.zeros(m0.ne, np.int32) for k in ("e1", "e2", "es1", "es2", "iedge")}
+        a.update({k: np.zeros(m0.ne) for k in ("l0", "kappap")})
+        a.update({k: np.zeros(m0.nt, np.int32) for k in ("t1", "t2", "t3")})
+        a.update({k: np.zeros(m0.nt) for k in ("cmx", "cmy", "cmz", "tarea")})
+        m = Mesh()
+        m.nv, m.ne, m.nt = m0.nv, m0.ne, m0.nt
+        for k, arr in a.items():
+            setattr(m, k, _p(arr, I if arr.dtype == np.int32 else D))
+        self._ck(self.L.irbc_get_mesh(self.h, C.byref(m)), "irbc_get_mesh")
+        return a, {"Sarea0": m.Sarea0, "Volume0": m.Volume0, "theta0": m.theta0}
+
+    def set_state(self, st):
+        v = st.view()
+        self._ck(self.L.irbc_set_state(self.h, C.byref(v)), "irbc_set_state")
+
+    def get_state(self, solvent=True, llist=True):
+        lcap = int(self.L.irbc_llist_total(self.h)) if llist else 1
+        st = State(self.params.Ns, self.nv, self.nlig, self.ncell, lcap, solvent=solvent, llist=llist)
+        v = st.view()
+        self._ck(self.L.irbc_get_state(self.h, C.byref(v)), "irbc_get_state")
+        st.absorb(v)
+        return st
+
+    def step(self, n=1):
+        self._ck(self.L.irbc_step(self.h, n), "irbc_step")
+
+    def sync(self):
+        self._ck(self.L.irbc_sync(self.h), "irbc_sync")
+
+    def call(self, name, *args):
+        self._ck(getattr(self.L, "irbc_" + name)(self.h, *args), "irbc_" + name)
+
+    def observables(self):
+        out = np.zeros(16)
+        self._ck(self.L.irbc_observables(self.h, _p(out, D), 16), "irbc_observables")
+        return out
+
+    def velocity_profile(self, nbins):
+        out = np.zeros(nbins)
+        self._ck(self.L.irbc_velocity_profile(self.h, _p(out, D), nbins), "irbc_velocity_profile")
+        return out
+
+    def write_rbcdata(self, path, append=True):
+        self._ck(self.L.irbc_write_rbcdata(self.h, path.encode(), 1 if append else 0), "irbc_write_rbcdata")
+
+    def write_stl(self, path):
+        self._ck(self.L.irbc_write_stl(self.h, path.encode()), "irbc_write_stl")
+
+    def launch_count(self):
+        return int(self.L.irbc_launch_count(self.h))
+
+    def profile_begin(self):
+        self._ck(self.L.irbc_profile_begin(self.h), "irbc_profile_begin")
+
+    def profile_end(self):
+        """dict of CUDA-event times (ms) since profile_begin"""
+        out = np.zeros(8)
+        self._ck(self.L.irbc_profile_end(self.h, _p(out, D), 8), "irbc_profile_end")
+        return dict(total_ms=out[0], stream_ms=out[1], stream_launches=int(out[2]), collide_ms=out[3],
+                    collides=int(out[4]), membrane_ms=out[5], membrane_groups=int(out[6]),
+                    launches=int(out[7]))
+
+
+class PinnedArray:
+    """numpy view of page-locked host memory from irbc_host_alloc."""
+
+    def __init__(self, n, dtype):
+        dtype = np.dtype(dtype)
+        self.ptr = lib().irbc_host_alloc(max(1, n) * dtype.itemsize)
+        if not self.ptr:
+            raise IrbcError("irbc_host_alloc failed")
+        buf = (C.c_char * (max(1, n) * dtype.itemsize)).from_address(self.ptr)
+        self.array = np.frombuffer(buf, dtype=dtype, count=n)
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().irbc_host_free(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass

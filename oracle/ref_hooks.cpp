@@ -86,11 +86,14 @@ const double paraR_ = paraR;
 int irbc_ref_main(int argc, char* argv[]);
 void bond_dynamics();
 
-extern "C" void ref_rng_seed(uint64_t seed);
-extern "C" void ref_rng_set_uniform(uint32_t stream, uint64_t epoch);
-extern "C" void ref_rng_set_normal(uint32_t stream, uint64_t epoch);
-extern "C" uint64_t ref_rng_uniform_cursor();
-extern "C" uint64_t ref_rng_normal_cursor();
+// The draw-stream controls exist only in the replay builds (linked with
+// ref_replay_rng.cpp); the timing builds keep the reference's own RNG.
+extern "C" void ref_rng_seed(uint64_t seed) __attribute__((weak));
+extern "C" void ref_rng_set_uniform(uint32_t stream, uint64_t epoch) __attribute__((weak));
+extern "C" void ref_rng_set_normal(uint32_t stream, uint64_t epoch) __attribute__((weak));
+extern "C" uint64_t ref_rng_uniform_cursor() __attribute__((weak));
+extern "C" uint64_t ref_rng_normal_cursor() __attribute__((weak));
+#define RNG_CALL(f, ...) do { if (f) f(__VA_ARGS__); } while (0)
 
 typedef void (*ref_cb_t)(int64_t step);
 
@@ -129,7 +132,7 @@ void irbc_hook_TotalVA() {
   int64_t s = k - 1;
   if (g_nstep_times < (1 << 16)) g_step_time[g_nstep_times++] = now_s();
   // everything RanGen draws after this point in step s is bond_dynamics
-  ref_rng_set_uniform(ORC_STREAM_BOND, (uint64_t)s);
+  RNG_CALL(ref_rng_set_uniform, ORC_STREAM_BOND, (uint64_t)s);
   if (g_cb) g_cb(s);
   if (g_stop_step >= 0 && s >= g_stop_step) throw StopRun();
 }
@@ -138,8 +141,8 @@ void irbc_hook_CollisionStep() {
   // TotalVA has run once at set-up and once per finished step, so the step
   // in progress is g_calls - 1
   uint64_t s = (uint64_t)current_step();
-  ref_rng_set_uniform(ORC_STREAM_COLLIDE_U, s);
-  ref_rng_set_normal(ORC_STREAM_COLLIDE_N, s);
+  RNG_CALL(ref_rng_set_uniform, ORC_STREAM_COLLIDE_U, s);
+  RNG_CALL(ref_rng_set_normal, ORC_STREAM_COLLIDE_N, s);
   CollisionStep();
 }
 
@@ -190,9 +193,9 @@ extern "C" int ref_run(int argc, char** argv, int64_t stop_step, ref_cb_t cb, ui
   reset_globals();
   g_calls = 0; g_stop_step = stop_step; g_cb = cb; g_fast_init = fast_init;
   g_llist_calls = 0; g_nstep_times = 0;
-  ref_rng_seed(seed);
-  ref_rng_set_uniform(ORC_STREAM_INIT, 0);
-  ref_rng_set_normal(ORC_STREAM_COLLIDE_N, 0);
+  RNG_CALL(ref_rng_seed, seed);
+  RNG_CALL(ref_rng_set_uniform, ORC_STREAM_INIT, 0);
+  RNG_CALL(ref_rng_set_normal, ORC_STREAM_COLLIDE_N, 0);
   g_t0 = now_s();
   try {
     irbc_ref_main(argc, argv);
@@ -209,8 +212,8 @@ extern "C" int64_t ref_step_times(double* out, int64_t cap) {
 extern "C" int ref_llist_calls() { return g_llist_calls; }
 extern "C" void ref_set_threads(int n) { omp_set_num_threads(n); }
 extern "C" int ref_max_threads() { return omp_get_max_threads(); }
-extern "C" uint64_t ref_uniform_cursor() { return ref_rng_uniform_cursor(); }
-extern "C" uint64_t ref_normal_cursor() { return ref_rng_normal_cursor(); }
+extern "C" uint64_t ref_uniform_cursor() { return ref_rng_uniform_cursor ? ref_rng_uniform_cursor() : 0; }
+extern "C" uint64_t ref_normal_cursor() { return ref_rng_normal_cursor ? ref_rng_normal_cursor() : 0; }
 
 // ---- compiled-in parameters (define.h:35-73, maincode.cpp:347-348) -----------
 extern "C" void ref_get_params(orc_params* p) {
@@ -322,8 +325,8 @@ extern "C" int ref_set_state(const orc_view* v) {
 
 // ---- direct calls of the reference's functions (one thread) -----------------
 extern "C" void ref_call_collide(uint64_t epoch) {
-  ref_rng_set_uniform(ORC_STREAM_COLLIDE_U, epoch);
-  ref_rng_set_normal(ORC_STREAM_COLLIDE_N, epoch);
+  RNG_CALL(ref_rng_set_uniform, ORC_STREAM_COLLIDE_U, epoch);
+  RNG_CALL(ref_rng_set_normal, ORC_STREAM_COLLIDE_N, epoch);
   CollisionStep();
 }
 extern "C" void ref_call_llist() { llistupdate(); }
@@ -334,7 +337,7 @@ extern "C" double ref_call_reflection(int i) { return reflectionFed(i, 0.0); }
 extern "C" double ref_call_solve(double aa, double bb, double cc) { return Solve(aa, bb, cc); }
 extern "C" int ref_call_solvep3(double* x, double aa, double b, double c) { return SolveP3(x, aa, b, c); }
 extern "C" void ref_call_bond_dynamics(uint64_t epoch) {
-  ref_rng_set_uniform(ORC_STREAM_BOND, epoch);
+  RNG_CALL(ref_rng_set_uniform, ORC_STREAM_BOND, epoch);
   bond_dynamics();
 }
 extern "C" void ref_call_filewrite(const char* path) {
