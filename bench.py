@@ -1,0 +1,310 @@
+#!/usr/bin/env python3
+"""bench.py -- solvent particle-steps/s of the iRBC timestep on B200.
+
+Workload (the reference's large single-simulation configuration): box
+128 x 64 x 64 cells, 10 solvent particles per cell (5,242,880), SRD angle
+130 deg, dtcd 0.025 (12 streaming steps per collision), dtmd 0.002, moving
+wall 0.64 (shear 0.01), one 2562-vertex Evans-Fung discocyte of radius 4
+with 1000 knobs, kon 0.005, koff 0.015.  Synthetic data: positions and
+velocities from the seeded draw stream, the discocyte from
+irbc_b200/mesh.py.
+
+A "step" is one reference timestep (maincode.cpp:461-764): streaming with
+bounce-back of every particle, the membrane update, and every 12th step the
+collision.  `value` = Ns * steps * ranks / max-over-ranks device time of the
+timed steps (CUDA events on the library's stream).  The solvent state
+(~630 MB in FP64) is larger than L2 (126 MB), so no flush is needed between
+steps.  N > 1 GPUs run independent replicas (different seeds), no
+collective in the data path.
+
+`--impl reference` times the reference's own OpenMP code (oracle/_ref, the
+same box, Ns, mesh, angle and dt compiled into its define.h) on the host
+cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "irbc-code_b200"))
+
+METRIC = "MPCD solvent particle-steps/s (large single simulation, 128x64x64, 5.24M particles)"
+UNIT = "particle-steps/s"
+WORKLOAD = dict(workload="large single simulation: box 128x64x64, 5242880 solvent, 2562-vertex discocyte "
+                         "R=4, 1000 knobs, alpha 130 deg, dtcd 0.025, dtmd 0.002, walls 0.64",
+                Lx=128.0, Ly=64.0, Lz=64.0, Ns=5242880, alpha_deg=130.0, dtcd=0.025, dtmd=0.002, walls=0.64,
+                nknobs=1000, kon=0.005, koff=0.015)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_params(G, seed, precision):
+    import math
+    W = WORKLOAD
+    a = math.radians(W["alpha_deg"])
+    return G.default_params(Lx=W["Lx"], Ly=W["Ly"], Lz=W["Lz"], Ns=W["Ns"], cosalpha=math.cos(a),
+                            sinalpha=math.sin(a), dtcd=W["dtcd"], dtmd=W["dtmd"], walls=W["walls"],
+                            onrate=W["kon"], offrate=W["koff"], Nt=2562, seed=seed, precision=precision)
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def reduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(steps=12, warmup=1, variant="large_timing"):
+    """The reference's OpenMP code on this host's cores, bounded sample."""
+    cmd = [sys.executable, os.path.join(ROOT, "oracle", "ref_bench.py"), "--variant", variant,
+           "--steps", str(steps), "--warmup", str(warmup)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=1500)
+        line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
+        d = json.loads(line)
+        return d
+    except Exception as e:  # reported, never silently replaced
+        return {"error": "%s: %s" % (type(e).__name__, str(e)[:200])}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    steps = min(args.steps, 24)
+    warm = min(args.warmup, 1)
+    d = cpu_baseline(steps, warm)
+    if "error" in d:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU run failed: " + d["error"]}))
+        return
+    line = {
+        "impl": "reference", "metric": METRIC, "value": d["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * d["seconds"] / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism="host OpenMP, %d threads" % d["cores"]),
+        "cpu_baseline": {"value": d["value"], "unit": UNIT, "cores": d["cores"], "kind": "reference",
+                         "sample": "%d whole timesteps after %d warm-up of the reference's main loop "
+                                   "(oracle/_ref/large_timing, -O3 -fopenmp, its own Mersenne Twister); "
+                                   "set-up excluded" % (steps, warm)},
+        "e2e": {"value": d["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    world, rank, local = dist_setup()
+    import numpy as np
+    import irbc_b200 as G
+    from irbc_b200 import mesh
+    precision = G.FP32 if args.precision == "fp32" else G.FP64
+    p = make_params(G, seed=1234 + 7919 * rank, precision=precision)
+    p.device = local
+    sim = G.Simulation(p)
+    V, E, T = mesh.discocyte()
+    sim.init(V, E, T, WORKLOAD["nknobs"])
+    sim.step(args.warmup)
+    sim.sync()
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        sim.profile_begin()
+        sim.step(args.steps)
+        prof = sim.profile_end()
+    t_ms = reduce_max(prof["total_ms"], world)
+    ns = WORKLOAD["Ns"]
+    value = ns * args.steps * world / (t_ms * 1e-3)
+    # roofline of the streaming kernel (dominant): algorithmic bytes per launch
+    bpp = 76 if precision == G.FP64 else 36
+    stream_avg_ms = prof["stream_ms"] / max(1, prof["stream_launches"])
+    achieved = ns * bpp / (stream_avg_ms * 1e-3) / 1e9
+    peak, kind = peaks()
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "stream_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            tj = json.load(open(tfile))
+            traffic = tj.get("fp64" if precision == G.FP64 else "fp32")
+        except Exception:
+            traffic = None
+    # end to end through the C ABI with host buffers: the full state in from
+    # page-locked memory, every step the RBCdata record out, the final state out
+    e2e = None
+    if args.e2e:
+        e2e = run_e2e(G, sim, args.steps, world)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if precision == G.FP64 else "f32", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism="replicas x%d" % world if world > 1 else "single GPU",
+                       l2="state larger than L2 (no flush needed)"),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": "k_stream",
+                     "bytes_per_particle": bpp, "peak_kind": kind,
+                     "kernel_ms_avg": stream_avg_ms},
+        "phase_ms_per_step": {"stream": prof["stream_ms"] / args.steps,
+                              "collide": prof["collide_ms"] / args.steps,
+                              "membrane": prof["membrane_ms"] / args.steps},
+        "gpu_launches": prof["launches"],
+        "clocks": clocks.summary(),
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if rank == 0 and not args.no_cpu_baseline:
+        d = cpu_baseline(12, 1)
+        if "error" in d:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                                    "sample": "failed: " + d["error"]}
+        else:
+            line["cpu_baseline"] = {"value": d["value"], "unit": UNIT, "cores": d["cores"], "kind": "reference",
+                                    "sample": "12 whole timesteps (one collision) of the reference's main loop on "
+                                              "the same workload, after 1 warm-up step; set-up excluded"}
+    if rank == 0:
+        print(json.dumps(line))
+    sim.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_e2e(G, sim, steps, world):
+    """Same metric through the public API with host buffers: set_state of
+    the full state from page-locked memory, `steps` steps each followed by
+    the RBCdata record (vertex x,y,z,ix,iy,bondi) to host, then the full
+    state back.  Host wall clock with a device synchronize on both ends."""
+    import numpy as np
+    st = sim.get_state()
+    pinned = {}
+    for k, a in st.a.items():
+        pa = G.PinnedArray(a.size, a.dtype)
+        pa.array[:] = a
+        pinned[k] = pa
+        st.a[k] = pa.array
+    rec = G.State(1, sim.nv, sim.nlig, sim.ncell, solvent=False, llist=False)
+    h2d = sum(st.a[k].nbytes for k in st.a)
+    d2h_rec = sum(a.nbytes for a in rec.a.values())
+    sim.sync()
+    t0 = time.perf_counter()
+    sim.set_state(st)
+    for _ in range(steps):
+        sim.step(1)
+        v = rec.view()
+        # vertex record only: solvent and list pointers are left NULL
+        sim._ck(sim.L.irbc_get_state(sim.h, __import__("ctypes").byref(v)), "irbc_get_state")
+    out = sim.get_state()
+    sim.sync()
+    dt = time.perf_counter() - t0
+    d2h = d2h_rec * steps + sum(out.a[k].nbytes for k in out.a)
+    ns = WORKLOAD["Ns"]
+    return {"value": ns * steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d / steps),
+            "d2h_bytes_per_step": int(d2h / steps)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--warmup", type=int, default=12)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

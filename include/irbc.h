@@ -146,6 +146,18 @@ int irbc_pfdt(irbc_handle* h);                     /* pfdt, Src/memfuncs.cpp:443
 int irbc_forces(irbc_handle* h);                   /* force_calculate_dt, Src/memfuncs.cpp:214-441 */
 int irbc_bond_dynamics(irbc_handle* h, int64_t epoch); /* bond prep + bond_dynamics, maincode.cpp:668-725,16-54 */
 
+/* ---- standalone binning ------------------------------------------------------------
+ * Random-shift cell binning of CollisionStep (Src/solfuncs.cpp:139-147) for
+ * particles held in DEVICE memory: x, y, z[n] device arrays, shift (rx, ry,
+ * rz) in [0, 1).  Writes, all device arrays: cell[n] (the particle's cell
+ * index, cindex semantics), start[C+1] (exclusive scan of the per-cell
+ * counts, C = Lx*Ly*(Lz+1)) and order[n] (particle indices grouped by cell,
+ * ascending within a cell: the Cells[].sol lists).  Uses the box of p.
+ * Scratch memory is taken with cudaMalloc and released before returning. */
+int irbc_bin_particles(const irbc_params* p, const double* x, const double* y, const double* z,
+                       int64_t n, double rx, double ry, double rz, int32_t* cell, int32_t* start,
+                       int32_t* order);
+
 /* ---- output (formats of maincode.cpp:749-753 and Src/memfuncs.cpp:590-626) ---- */
 int irbc_write_rbcdata(irbc_handle* h, const char* path, int32_t append);
 int irbc_write_stl(irbc_handle* h, const char* path);

@@ -72,9 +72,7 @@ void dfree(T*& p) {
   p = nullptr;
 }
 
-void fill_devparams(irbc_handle* h) {
-  const irbc_params& P = h->P;
-  DevParams& d = h->dp;
+void fill_devparams_from(const irbc_params& P, DevParams& d) {
   d.a = P.a; d.Lx = P.Lx; d.Ly = P.Ly; d.Lz = P.Lz; d.dtcd = P.dtcd; d.navg = P.navg;
   d.Theta = P.Theta; d.walls = P.walls; d.mass = P.mass; d.cosalpha = P.cosalpha; d.sinalpha = P.sinalpha;
   d.kappasa = P.kappasa; d.kappad = P.kappad; d.kappav = P.kappav; d.kappab = P.kappab; d.pmass = P.pmass;
@@ -86,6 +84,8 @@ void fill_devparams(irbc_handle* h) {
   d.nz = (int)(P.Lz / P.a) + 1;
   d.ncell = (int64_t)d.nx * d.ny * d.nz;
 }
+
+void fill_devparams(irbc_handle* h) { fill_devparams_from(h->P, h->dp); }
 
 // ligand grid (maincode.cpp:77-93)
 void build_ligands(irbc_handle* h) {
@@ -983,6 +983,36 @@ extern "C" int irbc_velocity_profile(irbc_handle* h, double* out, int32_t nbins)
   CK(cudaStreamSynchronize(h->st));
   for (int k = 0; k < nbins; ++k) out[k] = buf[2 * k + 1] > 0 ? buf[2 * k] / buf[2 * k + 1] : 0.0;
   return 0;
+}
+
+// ---- standalone binning ------------------------------------------------------------
+namespace irbc {
+void bin_particles(const DevParams& p, const double* x, const double* y, const double* z, int64_t n,
+                   double rx, double ry, double rz, int* cell, int* start, int* order, int* cnt, int* slot,
+                   int* part, int* totals, cudaStream_t st);
+}
+
+extern "C" int irbc_bin_particles(const irbc_params* p, const double* x, const double* y, const double* z,
+                                  int64_t n, double rx, double ry, double rz, int32_t* cell, int32_t* start,
+                                  int32_t* order) {
+  if (!p || n < 0 || (n > 0 && (!x || !y || !z || !cell || !order)) || !start) return IRBC_ERR_ARG;
+  if (p->a != 1.0 || p->Lx <= 0 || p->Ly <= 0 || p->Lz <= 0 || n >= (1LL << 31)) return IRBC_ERR_ARG;
+  if (!(rx >= 0 && rx < 1 && ry >= 0 && ry < 1 && rz >= 0 && rz < 1)) return IRBC_ERR_ARG;
+  DevParams d{};
+  fill_devparams_from(*p, d);
+  int *cnt = nullptr, *slot = nullptr, *part = nullptr, *totals = nullptr;
+  int64_t nb = scan_part_blocks(d.ncell);
+  cudaError_t e = dalloc(&cnt, d.ncell);
+  if (e == cudaSuccess) e = dalloc(&slot, n);
+  if (e == cudaSuccess) e = dalloc(&part, 3 * nb + 3);
+  if (e == cudaSuccess) e = dalloc(&totals, 4);
+  if (e == cudaSuccess) {
+    bin_particles(d, x, y, z, n, rx, ry, rz, cell, start, order, cnt, slot, part, totals, 0);
+    g_launches += 6;
+    e = cudaStreamSynchronize(0);
+  }
+  dfree(cnt); dfree(slot); dfree(part); dfree(totals);
+  return e == cudaSuccess ? 0 : IRBC_ERR_CUDA;
 }
 
 // ---- profiling window and host buffers ------------------------------------------------

@@ -112,6 +112,8 @@ def lib():
     L.irbc_host_alloc.restype = C.c_void_p
     L.irbc_host_alloc.argtypes = [C.c_size_t]
     L.irbc_host_free.argtypes = [C.c_void_p]
+    L.irbc_bin_particles.argtypes = [C.POINTER(Params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                     C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = L
     return L
 

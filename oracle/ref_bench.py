@@ -36,7 +36,7 @@ def main():
     ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--threads", type=int, default=0)
-    ap.add_argument("--nknobs", type=int, default=1000)
+    ap.add_argument("--nknobs", type=int, default=0, help="default: 500 on the 600-vertex mesh, 1000 otherwise")
     ap.add_argument("--onrate", type=float, default=0.005)
     ap.add_argument("--offrate", type=float, default=0.015)
     a = ap.parse_args()
@@ -46,6 +46,9 @@ def main():
     from irbc_b200 import mesh
     R = O.Reference(a.variant, threads=threads)
     wd = tempfile.mkdtemp(prefix="irbc_refbench_")
+    nknobs = a.nknobs or (500 if R.p.Nt == 600 else 1000)
+    if nknobs > R.p.Nt:
+        raise SystemExit("the reference's knob loop never ends with more knobs than vertices")
     if R.p.Nt == 600:
         vf, ef, tf = O.troph_files()
     else:
@@ -55,7 +58,7 @@ def main():
         vf, ef, tf = mesh.write_reference_files(wd, V, E, T)
     t0 = time.perf_counter()
     stop = a.warmup + a.steps
-    R.run(vf, ef, tf, a.nknobs, stop, seed=int(time.time()), onrate=a.onrate, offrate=a.offrate,
+    R.run(vf, ef, tf, nknobs, stop, seed=int(time.time()), onrate=a.onrate, offrate=a.offrate,
           fast_init=1, workdir=wd)
     wall = time.perf_counter() - t0
     ts = R.step_times()

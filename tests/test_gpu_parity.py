@@ -114,3 +114,49 @@ def test_full_size_config1_init_and_steps():
     sim.step(12)
     orc.step(12)
     assert H.compare(sim.get_state(), orc.get_state(), RTOL) == {}
+
+
+def _np_cells(op, x, y, z, r):
+    """cindex cell of each particle in the shifted grid (Src/solfuncs.cpp:141-144)."""
+    def bb(v, L):
+        v = v.copy()
+        while (v > L).any():
+            v[v > L] -= L
+        while (v < 0).any():
+            v[v < 0] += L
+        return v
+    nx, ny, nz = int(op.Lx), int(op.Ly), int(op.Lz) + 1
+    fx = np.floor(bb(x - r[0], op.Lx)).astype(np.int64)
+    fy = np.floor(bb(y - r[1], op.Ly)).astype(np.int64)
+    fz = np.floor(z - r[2] + 1.0).astype(np.int64)
+    ok = (fx >= 0) & (fx < nx) & (fy >= 0) & (fy < ny) & (fz >= 0) & (fz < nz)
+    return np.where(ok, (fx * ny + fy) * nz + fz, 0)
+
+
+def test_bin_particles_standalone():
+    """irbc_bin_particles on device arrays: cells, counting-sort starts and
+    the per-cell particle order (ascending index) exactly."""
+    import ctypes as C
+    import torch
+    import irbc_b200 as G
+    op = O.default_params(Ns=200000)
+    rng = np.random.default_rng(4)
+    n = 200000
+    pos = np.stack([rng.uniform(0, op.Lx, n), rng.uniform(0, op.Ly, n), rng.uniform(0, op.Lz, n)])
+    pos[0, :5] = [0.0, op.Lx, 59.99999999, 1e-300, 30.0]   # edges: x == Lx maps to cell 0
+    r = (0.25, 0.5, 0.999)
+    dev = [torch.tensor(pos[k], dtype=torch.float64, device="cuda") for k in range(3)]
+    p = H.to_irbc_params(op, 1)
+    ncell = int(op.Lx) * int(op.Ly) * (int(op.Lz) + 1)
+    cell = torch.zeros(n, dtype=torch.int32, device="cuda")
+    start = torch.zeros(ncell + 1, dtype=torch.int32, device="cuda")
+    order = torch.zeros(n, dtype=torch.int32, device="cuda")
+    L = G.lib()
+    rc = L.irbc_bin_particles(C.byref(p), dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr(), n,
+                              r[0], r[1], r[2], cell.data_ptr(), start.data_ptr(), order.data_ptr())
+    assert rc == 0
+    want = _np_cells(op, pos[0], pos[1], pos[2], r)
+    np.testing.assert_array_equal(cell.cpu().numpy(), want)
+    counts = np.bincount(want, minlength=ncell)
+    np.testing.assert_array_equal(start.cpu().numpy(), np.concatenate([[0], np.cumsum(counts)]))
+    np.testing.assert_array_equal(order.cpu().numpy(), np.argsort(want, kind="stable"))
