@@ -158,6 +158,22 @@ int irbc_bin_particles(const irbc_params* p, const double* x, const double* y, c
                        int64_t n, double rx, double ry, double rz, int32_t* cell, int32_t* start,
                        int32_t* order);
 
+/* No counterpart in the reference.  The binning of irbc_bin_particles for
+ * callers that cannot allocate device memory while they run (code inside an
+ * allocator callback or memory-pool hook, threads that must not take the
+ * driver's allocation lock, embedders with a fixed device-memory budget).
+ * Same arguments and results; allocates nothing.  Its scratch is a fixed
+ * static device array (4 MiB plus 12 KiB) that every GPU loading the library
+ * keeps until the process exits, so boxes are limited to 1,048,576 cells
+ * (Lx*Ly*(Lz+1)); larger boxes return IRBC_ERR_CAPACITY.  The first call on
+ * a device looks up the array's device address; make that first call before
+ * any stream capture.  All calls share the one array, so calls that overlap
+ * on the GPU (other host threads, other streams) race; this one runs on the
+ * legacy default stream and returns after it has finished. */
+int irbc_bin_particles_noalloc(const irbc_params* p, const double* x, const double* y, const double* z,
+                               int64_t n, double rx, double ry, double rz, int32_t* cell, int32_t* start,
+                               int32_t* order);
+
 /* ---- output (formats of maincode.cpp:749-753 and Src/memfuncs.cpp:590-626) ---- */
 int irbc_write_rbcdata(irbc_handle* h, const char* path, int32_t append);
 int irbc_write_stl(irbc_handle* h, const char* path);

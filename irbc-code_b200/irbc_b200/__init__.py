@@ -114,6 +114,7 @@ def lib():
     L.irbc_host_free.argtypes = [C.c_void_p]
     L.irbc_bin_particles.argtypes = [C.POINTER(Params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                      C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.irbc_bin_particles_noalloc.argtypes = L.irbc_bin_particles.argtypes
     _lib = L
     return L
 
