@@ -15,8 +15,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-O2",
          "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["kernels.cu", "binning.cu", "binning_noalloc.cu", "api.cu"]
-HEADERS = ["common.cuh", "sim.h"]
+SOURCES = ["kernels.cu", "fast.cu", "binning.cu", "binning_noalloc.cu", "api.cu"]
+HEADERS = ["common.cuh", "sim.h", "fast.h"]
 
 
 def _newer(target, deps):

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "fast.h"
 #include "irbc.h"
 #include "sim.h"
 
@@ -26,7 +27,12 @@ struct irbc_handle {
   Solvent s;
   Cells c;
   Membrane m;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr;   // solvent kernels; every public call orders on it
+  cudaStream_t st2 = nullptr;  // membrane kernels, run beside the solvent ones
+  FastBufs fb;
+  int snap_buf = 0;            // which snapshot the next streaming step reads
+  bool snap_ready = false;     // snapshot/triangle prep of the next step done
+  cudaEvent_t ev_snap = nullptr, ev_mem = nullptr, ev_coll = nullptr, ev_str[2] = {nullptr, nullptr};
   std::string err;
   bool have_mesh = false;
   int64_t step = 0;
@@ -255,11 +261,51 @@ int down(irbc_handle* h, T* v, const T* d, int64_t n) {
   return 0;
 }
 
+void free_fast(FastBufs& f) {
+  for (int b = 0; b < 2; ++b) {
+    for (double** q : {&f.snap[b].x, &f.snap[b].y, &f.snap[b].z, &f.snap[b].vx, &f.snap[b].vy, &f.snap[b].vz})
+      dfree(*q);
+    dfree(f.pre[b]);
+  }
+  dfree(f.slot); dfree(f.gstart); dfree(f.gidx);
+}
+
+// per-vertex force slots in the order force_calculate_dt adds the terms:
+// slots 4i..4i+3 of edge i (l1 WLC, l1 POW, l2 WLC, l2 POW), 9 per triangle
+// after 4E (alpha, alphad per corner, then the three volume terms), 4 per
+// dihedral after 4E+9T (l1, l4, l2, l3)
+void build_gather(const HostMesh& M, const std::vector<int>& start, const std::vector<int>& inc,
+                  std::vector<int>& gstart, std::vector<int>& gidx) {
+  const int base_t = 4 * M.ne, base_d = 4 * M.ne + 9 * M.nt;
+  gstart.assign(M.nv + 1, 0);
+  gidx.clear();
+  for (int v = 0; v < M.nv; ++v) {
+    gstart[v] = (int)gidx.size();
+    for (int q = start[v]; q < start[v + 1]; ++q) {
+      int e = inc[q];
+      int kind = (e >> 30) & 3, role = (e >> 27) & 7, item = e & ((1 << 27) - 1);
+      if (kind == 0) {
+        gidx.push_back(4 * item + 2 * role);
+        gidx.push_back(4 * item + 2 * role + 1);
+      } else if (kind == 1) {
+        gidx.push_back(base_t + 9 * item + 2 * role);
+        gidx.push_back(base_t + 9 * item + 2 * role + 1);
+        gidx.push_back(base_t + 9 * item + 6 + role);
+      } else {
+        gidx.push_back(base_d + 4 * item + role);
+      }
+    }
+  }
+  gstart[M.nv] = (int)gidx.size();
+}
+
 // allocates the membrane and uploads the topology
 int upload_mesh(irbc_handle* h, const HostMesh& M) {
   Membrane& m = h->m;
   if (M.nv > 8192) return fail(h, IRBC_ERR_ARG, "at most 8192 membrane vertices");
   free_membrane(m);
+  free_fast(h->fb);
+  h->snap_ready = false;
   m.nv = M.nv; m.ne = M.ne; m.nt = M.nt;
   for (double** p : {&m.x, &m.y, &m.z, &m.vx, &m.vy, &m.vz, &m.fx, &m.fy, &m.fz, &m.poff, &m.pon})
     CK(dalloc(p, M.nv));
@@ -276,6 +322,21 @@ int upload_mesh(irbc_handle* h, const HostMesh& M) {
   CK(dalloc(&m.inc_start, M.nv + 1));
   CK(dalloc(&m.inc, (int64_t)inc.size()));
   if (up(h, m.inc_start, start) || up(h, m.inc, inc)) return IRBC_ERR_CUDA;
+  {
+    FastBufs& f = h->fb;
+    for (int b = 0; b < 2; ++b) {
+      for (double** q : {&f.snap[b].x, &f.snap[b].y, &f.snap[b].z, &f.snap[b].vx, &f.snap[b].vy, &f.snap[b].vz})
+        CK(dalloc(q, M.nv));
+      CK(dalloc(&f.pre[b], M.nt));
+      f.snap[b].t1 = m.t1; f.snap[b].t2 = m.t2; f.snap[b].t3 = m.t3;
+    }
+    std::vector<int> gstart, gidx;
+    build_gather(M, start, inc, gstart, gidx);
+    CK(dalloc(&f.slot, 3 * (int64_t)(8 * M.ne + 9 * M.nt)));
+    CK(dalloc(&f.gstart, M.nv + 1));
+    CK(dalloc(&f.gidx, (int64_t)gidx.size()));
+    if (up(h, f.gstart, gstart) || up(h, f.gidx, gidx)) return IRBC_ERR_CUDA;
+  }
   if (up(h, m.e1, M.e1) || up(h, m.e2, M.e2) || up(h, m.es1, M.es1) || up(h, m.es2, M.es2) ||
       up(h, m.iedge, M.iedge) || up(h, m.l0, M.l0) || up(h, m.kappap, M.kappap) || up(h, m.t1, M.t1) ||
       up(h, m.t2, M.t2) || up(h, m.t3, M.t3) || up(h, m.tarea, M.tarea))
@@ -306,14 +367,15 @@ cudaEvent_t next_event(irbc_handle* h) {
 struct ProfScope {
   irbc_handle* h;
   size_t idx;
-  ProfScope(irbc_handle* hh, int cat) : h(hh), idx(0) {
+  cudaStream_t st;
+  ProfScope(irbc_handle* hh, int cat, cudaStream_t s = nullptr) : h(hh), idx(0), st(s ? s : hh->st) {
     if (!h->prof) return;
     idx = h->ev_used;
-    cudaEventRecord(next_event(h), h->st);
+    cudaEventRecord(next_event(h), st);
     h->ev_marks.push_back({cat, idx});
   }
   ~ProfScope() {
-    if (h->prof) cudaEventRecord(next_event(h), h->st);
+    if (h->prof) cudaEventRecord(next_event(h), st);
   }
 };
 
@@ -359,6 +421,18 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   cudaError_t e = cudaSetDevice(p->device);
   if (e != cudaSuccess) { delete h; return IRBC_ERR_CUDA; }
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) { delete h; return IRBC_ERR_CUDA; }
+  {
+    // the membrane chain is latency bound: give its stream the higher priority
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (cudaStreamCreateWithPriority(&h->st2, cudaStreamNonBlocking, hi) != cudaSuccess) {
+      cudaStreamDestroy(h->st);
+      delete h;
+      return IRBC_ERR_CUDA;
+    }
+    for (cudaEvent_t* e : {&h->ev_snap, &h->ev_mem, &h->ev_coll, &h->ev_str[0], &h->ev_str[1]})
+      cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+  }
   fill_devparams(h);
   build_ligands(h);
   h->csteps = (int)(p->dtcd / p->dtmd);
@@ -388,6 +462,8 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   A(dalloc(&h->m.ylig, h->dp.nlig));
   A(dalloc(&h->m.sc, 1));
   A(dalloc(&h->obs, 64 + 4096));
+  A(dalloc(&h->fb.queue, s.n));
+  A(dalloc(&h->fb.qn, 4));
   if (rc) { irbc_destroy(h); return rc; }
   cudaMemsetAsync(c.lstart, 0, sizeof(int) * (c.n + 1), h->st);
   cudaMemsetAsync(h->m.ligi, 0, sizeof(int) * h->dp.nlig, h->st);
@@ -406,6 +482,12 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   if (!h) return;
   cudaSetDevice(h->P.device);
   if (h->st) cudaStreamSynchronize(h->st);
+  if (h->st2) cudaStreamSynchronize(h->st2);
+  free_fast(h->fb);
+  dfree(h->fb.queue); dfree(h->fb.qn);
+  for (cudaEvent_t e : {h->ev_snap, h->ev_mem, h->ev_coll, h->ev_str[0], h->ev_str[1]})
+    if (e) cudaEventDestroy(e);
+  if (h->st2) cudaStreamDestroy(h->st2);
   Solvent& s = h->s;
   Cells& c = h->c;
   for (double** q : {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.x2, &s.y2, &s.z2, &s.vx2, &s.vy2, &s.vz2})
@@ -792,9 +874,11 @@ extern "C" int irbc_collide(irbc_handle* h, int64_t epoch) {
   return 0;
 }
 extern "C" int irbc_stream(irbc_handle* h) {
-  if (!h) return IRBC_ERR_ARG;
-  launch_stream(h->dp, h->s, h->c, h->m, h->st);
-  g_launches += 1;
+  if (!h || !h->have_mesh) return IRBC_ERR_ARG;
+  fast_snap_prep(h->dp, h->m, h->fb, 0, h->st);
+  fast_stream(h->dp, h->s, h->c, h->fb, 0, h->st);
+  h->snap_ready = false;
+  g_launches += 4;
   CK(cudaGetLastError());
   return 0;
 }
@@ -842,10 +926,11 @@ extern "C" int irbc_step_part1(irbc_handle* h) {
     g_launches += 10;
     h->colsteps = 0;
   }
+  const int buf = (int)(s & 1);
   {
     ProfScope ps(h, PROF_MEMBRANE);
-    launch_half_kick(h->dp, h->m, h->st);
-    g_launches += 1;
+    fast_kick_prep(h->dp, h->m, h->fb, buf, h->st);
+    g_launches += 2;
   }
   if (h->upd == h->uplist) {
     int rc = do_llist(h);
@@ -854,14 +939,14 @@ extern "C" int irbc_step_part1(irbc_handle* h) {
   }
   {
     ProfScope ps(h, PROF_STREAM);
-    launch_stream(h->dp, h->s, h->c, h->m, h->st);
+    fast_stream(h->dp, h->s, h->c, h->fb, buf, h->st);
   }
   {
     ProfScope ps(h, PROF_MEMBRANE);
-    launch_drift(h->dp, h->m, h->st);
-    launch_total_va(h->dp, h->m, h->st);
+    fast_drift_va(h->dp, h->m, h->st);
   }
-  g_launches += 4;
+  g_launches += 3;
+  h->snap_ready = false;
   CK(cudaGetLastError());
   return 0;
 }
@@ -873,26 +958,91 @@ extern "C" int irbc_step_part2(irbc_handle* h) {
   const int64_t s = h->step;
   {
     ProfScope ps(h, PROF_MEMBRANE);
-    launch_pfdt_forces(h->dp, h->m, 1, 1, 1, h->st);
-    launch_bonds(h->dp, h->m, (uint64_t)s, h->st);
-    launch_kick2(h->dp, h->m, h->st);
+    fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)s, 0, (int)((s + 1) & 1), h->st);
   }
-  g_launches += 5;
+  g_launches += 3;
   if (h->filecc == h->P.out_every) { h->filec += 1; h->filecc = 0; }
   h->step = s + 1;
   CK(cudaGetLastError());
   return 0;
 }
 
+// n timesteps with the membrane chain on its own stream: step s streams the
+// solvent (h->st) while the membrane drifts, computes forces and bonds for s
+// and prepares the snapshot of s+1 (h->st2).  Collisions, llist updates and
+// the snapshot buffers (two, by step parity) are ordered by events.  The
+// result equals n calls of part 1 + part 2.
 extern "C" int irbc_step(irbc_handle* h, int64_t n) {
   if (!h || n < 0) return IRBC_ERR_ARG;
+  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
   cudaSetDevice(h->P.device);
+  const irbc_params& p = h->P;
+  cudaStream_t ms = h->st, ss = h->st2;
+  // the side stream starts after everything already queued on the main one
+  CK(cudaEventRecord(h->ev_coll, ms));
+  CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
   for (int64_t k = 0; k < n; ++k) {
-    int rc = irbc_step_part1(h);
-    if (rc) return rc;
-    rc = irbc_step_part2(h);
-    if (rc) return rc;
+    const int64_t s = h->step;
+    h->dp.wallspeed = (s < p.warm_steps) ? p.warm_speed : p.walls;
+    h->colsteps += 1; h->bbi += 1; h->upd += 1;
+    if (s > 0) h->filecc += 1;
+    const int buf = (int)(s & 1);
+    if (h->colsteps == h->csteps) {
+      CK(cudaStreamWaitEvent(ms, h->ev_mem, 0));
+      {
+        ProfScope ps(h, PROF_COLLIDE, ms);
+        launch_collide(h->dp, h->s, h->c, h->m, (uint64_t)s, ms);
+      }
+      g_launches += 10;
+      h->colsteps = 0;
+      CK(cudaEventRecord(h->ev_coll, ms));
+      CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
+      h->snap_ready = false;
+    }
+    if (!h->snap_ready) {
+      CK(cudaStreamWaitEvent(ss, h->ev_str[buf], 0));
+      ProfScope ps(h, PROF_MEMBRANE, ss);
+      fast_kick_prep(h->dp, h->m, h->fb, buf, ss);
+      g_launches += 2;
+    }
+    if (h->upd == h->uplist) {
+      // positions of step s are final once the side stream reaches here;
+      // the side stream's drift of step s waits for the update
+      CK(cudaEventRecord(h->ev_snap, ss));
+      CK(cudaStreamWaitEvent(ms, h->ev_snap, 0));
+      int rc = do_llist(h);
+      if (rc) return rc;
+      h->upd = 0;
+      CK(cudaEventRecord(h->ev_coll, ms));
+      CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
+    }
+    CK(cudaEventRecord(h->ev_snap, ss));
+    CK(cudaStreamWaitEvent(ms, h->ev_snap, 0));
+    {
+      ProfScope ps(h, PROF_STREAM, ms);
+      fast_stream(h->dp, h->s, h->c, h->fb, buf, ms);
+    }
+    g_launches += 2;
+    CK(cudaEventRecord(h->ev_str[buf], ms));
+    // the next step's snapshot goes to the other buffer, read by the
+    // previous step's streaming
+    const bool last = (k == n - 1);
+    const bool next_collides = (h->colsteps + 1 == h->csteps);
+    const int next_kick = (!last && !next_collides) ? 1 : 0;
+    CK(cudaStreamWaitEvent(ss, h->ev_str[buf ^ 1], 0));
+    {
+      ProfScope ps(h, PROF_MEMBRANE, ss);
+      fast_drift_va(h->dp, h->m, ss);
+      fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)s, next_kick, buf ^ 1, ss);
+    }
+    g_launches += 4;
+    CK(cudaEventRecord(h->ev_mem, ss));
+    h->snap_ready = next_kick != 0;
+    if (h->filecc == p.out_every) { h->filec += 1; h->filecc = 0; }
+    h->step = s + 1;
   }
+  CK(cudaStreamWaitEvent(ms, h->ev_mem, 0));
+  CK(cudaGetLastError());
   return 0;
 }
 

@@ -89,4 +89,55 @@ __device__ __forceinline__ void cp(const R A[3], const R B[3], R C[3]) {
   C[2] = (A[0] * B[1]) - (B[0] * A[1]);
 }
 
+// SolveP3 (Src/poly34.cpp:26-55): trigonometric (three real roots) or
+// Cardano (one) form, then the root selection of Solve
+// (Src/solfuncs.cpp:369-396): the smallest root in [0, dtmd], else the next.
+__device__ __forceinline__ double solve_p3_tt(double aa, double b, double c, double dtmd) {
+  // SolveP3 (Src/poly34.cpp:26-55) + root selection of Solve (Src/solfuncs.cpp:369-396)
+  const double TwoPi = 6.28318530717958648, eps = 1e-14;
+  double x[3];
+  int nroot;
+  double a2 = aa * aa;
+  double q = (a2 - 3 * b) / 9;
+  double r = (aa * (2 * a2 - 9 * b) + 27 * c) / 54;
+  double r2 = r * r;
+  double q3 = q * q * q;
+  if (r2 < q3) {
+    double t = r / sqrt(q3);
+    if (t < -1) t = -1;
+    if (t > 1) t = 1;
+    t = acos(t);
+    aa /= 3; q = -2 * sqrt(q);
+    x[0] = q * cos(t / 3) - aa;
+    x[1] = q * cos((t + TwoPi) / 3) - aa;
+    x[2] = q * cos((t - TwoPi) / 3) - aa;
+    nroot = 3;
+  } else {
+    double A = -pow(fabs(r) + sqrt(r2 - q3), 1. / 3);
+    if (r < 0) A = -A;
+    double B = (A == 0) ? 0 : q / A;
+    aa /= 3;
+    x[0] = (A + B) - aa;
+    x[1] = -0.5 * (A + B) - aa;
+    x[2] = 0.5 * sqrt(3.) * (A - B);
+    if (fabs(x[2]) < eps) { x[2] = x[1]; nroot = 2; } else nroot = 1;
+  }
+  double tt;
+  if (nroot == 3 || nroot == 2) {
+    // sort three values ascending (std::sort on 3 doubles without NaN)
+    double u0 = x[0], u1 = x[1], u2 = x[2], t;
+    if (u1 < u0) { t = u0; u0 = u1; u1 = t; }
+    if (u2 < u1) { t = u1; u1 = u2; u2 = t; }
+    if (u1 < u0) { t = u0; u0 = u1; u1 = t; }
+    tt = u0;
+    if ((tt < 0) || (tt > dtmd)) {
+      tt = u1;
+      if ((tt < 0) || (tt > dtmd)) tt = u2;
+    }
+  } else {
+    tt = x[0];
+  }
+  return tt;
+}
+
 }  // namespace irbc

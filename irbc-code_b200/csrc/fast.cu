@@ -1,0 +1,750 @@
+// fast.cu -- the production FP64 step: streaming that hands particles with
+// long cell lists to a warp each, and the membrane update as four kernels
+// (drift + TotalVA in one CTA, per-item force terms, an ordered per-vertex
+// gather, and a one-CTA tail with the serial bond and parasite work) that
+// run on a side stream beside the solvent kernels.
+//
+// Results equal the one-kernel-per-phase path (kernels.cu) bit for bit.
+#include <cstdio>
+#include "fast.h"
+
+namespace irbc {
+
+static inline unsigned nb(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+#define UXm(v) (m.x[v] + m.ix[v] * p.Lx)
+#define UYm(v) (m.y[v] + m.iy[v] * p.Ly)
+
+// ======================================================== triangle prep ===
+// For the streaming step: each triangle's corners at t (A1,B1,C1, no image
+// shift) and at t+dtmd, and the normals X = (B1-A1)x(C1-A1), Xdt likewise,
+// as reflectionFed computes them (Src/solfuncs.cpp:457-509).  Also a copy of
+// the vertex positions and velocities the streaming kernels read, so the
+// membrane may move on while they run.
+__device__ void tri_prep_one(const DevParams& p, const Membrane& m, int j, const double* vx, const double* vy,
+                             const double* vz, TriPre* out) {
+  int p1 = m.t1[j], p2 = m.t2[j], p3 = m.t3[j];
+  const double rstep = 0.0, dtmd = p.dtmd, Lx = p.Lx, Ly = p.Ly;
+  const int z0 = 0;
+  double v1x = (m.x[p1] + z0 * Lx) + vx[p1] * rstep, v1y = (m.y[p1] + z0 * Ly) + vy[p1] * rstep,
+         v1z = m.z[p1] + vz[p1] * rstep;
+  double v2x = (m.x[p2] + z0 * Lx) + vx[p2] * rstep, v2y = (m.y[p2] + z0 * Ly) + vy[p2] * rstep,
+         v2z = m.z[p2] + vz[p2] * rstep;
+  double v3x = (m.x[p3] + z0 * Lx) + vx[p3] * rstep, v3y = (m.y[p3] + z0 * Ly) + vy[p3] * rstep,
+         v3z = m.z[p3] + vz[p3] * rstep;
+  double w1x = v1x + vx[p1] * (dtmd - rstep), w1y = v1y + vy[p1] * (dtmd - rstep), w1z = v1z + vz[p1] * (dtmd - rstep);
+  double w2x = v2x + vx[p2] * (dtmd - rstep), w2y = v2y + vy[p2] * (dtmd - rstep), w2z = v2z + vz[p2] * (dtmd - rstep);
+  double w3x = v3x + vx[p3] * (dtmd - rstep), w3y = v3y + vy[p3] * (dtmd - rstep), w3z = v3z + vz[p3] * (dtmd - rstep);
+  double t0[3], t1v[3], X[3], Xdt[3];
+  t0[0] = v2x - v1x; t0[1] = v2y - v1y; t0[2] = v2z - v1z;
+  t1v[0] = v3x - v1x; t1v[1] = v3y - v1y; t1v[2] = v3z - v1z;
+  cp(t0, t1v, X);
+  t0[0] = w2x - w1x; t0[1] = w2y - w1y; t0[2] = w2z - w1z;
+  t1v[0] = w3x - w1x; t1v[1] = w3y - w1y; t1v[2] = w3z - w1z;
+  cp(t0, t1v, Xdt);
+  TriPre q;
+  q.X[0] = X[0]; q.X[1] = X[1]; q.X[2] = X[2];
+  q.Xdt[0] = Xdt[0]; q.Xdt[1] = Xdt[1]; q.Xdt[2] = Xdt[2];
+  q.A1[0] = v1x; q.A1[1] = v1y; q.A1[2] = v1z;
+  q.A2[0] = w1x; q.A2[1] = w1y; q.A2[2] = w1z;
+  out[j] = q;
+}
+
+// ================================================================ stream =====
+// reflectionFed's per-triangle test and hit, reading the vertex snapshot.
+// Returns true if the triangle was hit (state updated).  `pre` gives the
+// precomputed normals when the particle is outside the periodic stencil
+// bands (3a from each side wall), where reflectionFed applies no shift.
+__device__ __forceinline__ bool tri_visit(const DevParams& p, const Snap& sn, const TriPre* __restrict__ pre, int jj,
+                                          double& X_, double& Y_, double& Z_, double& VX, double& VY, double& VZ,
+                                          int indio, double& fulldt, bool use_pre) {
+  const double rstep = 0.0, dtmd = p.dtmd, a = p.a, Lx = p.Lx, Ly = p.Ly;
+  int flg = 0;
+  const double solvx = X_ + 0 * Lx, solvy = Y_ + 0 * Ly, solvz = Z_;
+  double bt, bdt;
+  double v1x, v1y, v1z, v2x, v2y, v2z, v3x, v3y, v3z;
+  int p1 = sn.t1[jj], p2 = sn.t2[jj], p3 = sn.t3[jj];
+  if (use_pre) {
+    const TriPre& q = pre[jj];
+    double PSt0 = solvx - q.A1[0], PSt1 = solvy - q.A1[1], PSt2 = solvz - q.A1[2];
+    double PD0 = (solvx + VX * (dtmd - rstep)) - q.A2[0];
+    double PD1 = (solvy + VY * (dtmd - rstep)) - q.A2[1];
+    double PD2 = (solvz + VZ * (dtmd - rstep)) - q.A2[2];
+    bt = q.X[0] * PSt0 + q.X[1] * PSt1 + q.X[2] * PSt2;
+    bdt = q.Xdt[0] * PD0 + q.Xdt[1] * PD1 + q.Xdt[2] * PD2;
+    if ((indio == 1) && (bt < 0)) flg = 1;
+    if ((indio == 0) && (bt > 0)) flg = 1;
+    if (!((bt * bdt <= 0) && (flg == 0))) return false;
+    v1x = q.A1[0]; v1y = q.A1[1]; v1z = q.A1[2];
+    v2x = (sn.x[p2] + 0 * Lx) + sn.vx[p2] * rstep; v2y = (sn.y[p2] + 0 * Ly) + sn.vy[p2] * rstep;
+    v2z = sn.z[p2] + sn.vz[p2] * rstep;
+    v3x = (sn.x[p3] + 0 * Lx) + sn.vx[p3] * rstep; v3y = (sn.y[p3] + 0 * Ly) + sn.vy[p3] * rstep;
+    v3z = sn.z[p3] + sn.vz[p3] * rstep;
+  } else {
+    v1x = (sn.x[p1] + 0 * Lx) + sn.vx[p1] * rstep; v1y = (sn.y[p1] + 0 * Ly) + sn.vy[p1] * rstep;
+    v1z = sn.z[p1] + sn.vz[p1] * rstep;
+    v2x = (sn.x[p2] + 0 * Lx) + sn.vx[p2] * rstep; v2y = (sn.y[p2] + 0 * Ly) + sn.vy[p2] * rstep;
+    v2z = sn.z[p2] + sn.vz[p2] * rstep;
+    v3x = (sn.x[p3] + 0 * Lx) + sn.vx[p3] * rstep; v3y = (sn.y[p3] + 0 * Ly) + sn.vy[p3] * rstep;
+    v3z = sn.z[p3] + sn.vz[p3] * rstep;
+    double rstencilx = Lx - (3.0 * a), lstencilx = 3.0 * a, rstencily = Ly - (3.0 * a), lstencily = 3.0 * a;
+    if (solvx < lstencilx) {
+      v1x -= (v1x > rstencilx) ? Lx : 0; v2x -= (v2x > rstencilx) ? Lx : 0; v3x -= (v3x > rstencilx) ? Lx : 0;
+    } else if (solvx > rstencilx) {
+      v1x += (v1x < lstencilx) ? Lx : 0; v2x += (v2x < lstencilx) ? Lx : 0; v3x += (v3x < lstencilx) ? Lx : 0;
+    }
+    if (solvy < lstencily) {
+      v1y -= (v1y > rstencily) ? Ly : 0; v2y -= (v2y > rstencily) ? Ly : 0; v3y -= (v3y > rstencily) ? Ly : 0;
+    } else if (solvy > rstencily) {
+      v1y += (v1y < lstencily) ? Ly : 0; v2y += (v2y < lstencily) ? Ly : 0; v3y += (v3y < lstencily) ? Ly : 0;
+    }
+    double w1x = v1x + sn.vx[p1] * (dtmd - rstep), w1y = v1y + sn.vy[p1] * (dtmd - rstep), w1z = v1z + sn.vz[p1] * (dtmd - rstep);
+    double w2x = v2x + sn.vx[p2] * (dtmd - rstep), w2y = v2y + sn.vy[p2] * (dtmd - rstep), w2z = v2z + sn.vz[p2] * (dtmd - rstep);
+    double w3x = v3x + sn.vx[p3] * (dtmd - rstep), w3y = v3y + sn.vy[p3] * (dtmd - rstep), w3z = v3z + sn.vz[p3] * (dtmd - rstep);
+    double X[3], Xdt[3], t0[3], t1v[3];
+    t0[0] = v2x - v1x; t0[1] = v2y - v1y; t0[2] = v2z - v1z;
+    t1v[0] = v3x - v1x; t1v[1] = v3y - v1y; t1v[2] = v3z - v1z;
+    cp(t0, t1v, X);
+    t0[0] = w2x - w1x; t0[1] = w2y - w1y; t0[2] = w2z - w1z;
+    t1v[0] = w3x - w1x; t1v[1] = w3y - w1y; t1v[2] = w3z - w1z;
+    cp(t0, t1v, Xdt);
+    double PSt0 = solvx - v1x, PSt1 = solvy - v1y, PSt2 = solvz - v1z;
+    double PD0 = (solvx + VX * (dtmd - rstep)) - w1x;
+    double PD1 = (solvy + VY * (dtmd - rstep)) - w1y;
+    double PD2 = (solvz + VZ * (dtmd - rstep)) - w1z;
+    bt = X[0] * PSt0 + X[1] * PSt1 + X[2] * PSt2;
+    bdt = Xdt[0] * PD0 + Xdt[1] * PD1 + Xdt[2] * PD2;
+    if ((indio == 1) && (bt < 0)) flg = 1;
+    if ((indio == 0) && (bt > 0)) flg = 1;
+    if (!((bt * bdt <= 0) && (flg == 0))) return false;
+  }
+  // crossing candidate: contact time from the cubic, barycentric test (:526-594)
+  const double mvx1 = sn.vx[p1], mvy1 = sn.vy[p1], mvz1 = sn.vz[p1];
+  const double mvx2 = sn.vx[p2], mvy2 = sn.vy[p2], mvz2 = sn.vz[p2];
+  const double mvx3 = sn.vx[p3], mvy3 = sn.vy[p3], mvz3 = sn.vz[p3];
+  double a10[3], a20[3], d1[3], d2[3], a1v[3], a2v[3], b1[3], b2[3], b3[3], d11[3], d22[3];
+  a10[0] = v2x - v1x; a10[1] = v2y - v1y; a10[2] = v2z - v1z;
+  a20[0] = v3x - v1x; a20[1] = v3y - v1y; a20[2] = v3z - v1z;
+  d1[0] = mvx2 - mvx1; d1[1] = mvy2 - mvy1; d1[2] = mvz2 - mvz1;
+  d2[0] = mvx3 - mvx1; d2[1] = mvy3 - mvy1; d2[2] = mvz3 - mvz1;
+  a1v[0] = solvx - v1x; a1v[1] = solvy - v1y; a1v[2] = solvz - v1z;
+  a2v[0] = VX - mvx1; a2v[1] = VY - mvy1; a2v[2] = VZ - mvz1;
+  cp(a10, a20, b1);
+  cp(a10, d2, d11);
+  cp(d1, a20, d22);
+  cp(d1, d2, b3);
+  for (int k = 0; k < 3; ++k) b2[k] = d11[k] + d22[k];
+  double a2b3 = a2v[0] * b3[0] + a2v[1] * b3[1] + a2v[2] * b3[2];
+  double a1b3 = a1v[0] * b3[0] + a1v[1] * b3[1] + a1v[2] * b3[2];
+  double a2b2 = a2v[0] * b2[0] + a2v[1] * b2[1] + a2v[2] * b2[2];
+  double a1b2 = a1v[0] * b2[0] + a1v[1] * b2[1] + a1v[2] * b2[2];
+  double a2b1 = a2v[0] * b1[0] + a2v[1] * b1[1] + a2v[2] * b1[2];
+  double a1b1 = a1v[0] * b1[0] + a1v[1] * b1[1] + a1v[2] * b1[2];
+  double tt = solve_p3_tt((a1b3 + a2b2) / a2b3, (a1b2 + a2b1) / a2b3, a1b1 / a2b3, dtmd);
+  double PS2[3], pd[3];
+  PS2[0] = (solvx + VX * tt) - (v1x + mvx1 * tt);
+  PS2[1] = (solvy + VY * tt) - (v1y + mvy1 * tt);
+  PS2[2] = (solvz + VZ * tt) - (v1z + mvz1 * tt);
+  pd[0] = (solvx + VX * tt); pd[1] = (solvy + VY * tt); pd[2] = (solvz + VZ * tt);
+  a10[0] = (v2x + mvx2 * tt) - (v1x + mvx1 * tt);
+  a10[1] = (v2y + mvy2 * tt) - (v1y + mvy1 * tt);
+  a10[2] = (v2z + mvz2 * tt) - (v1z + mvz1 * tt);
+  a20[0] = (v3x + mvx3 * tt) - (v1x + mvx1 * tt);
+  a20[1] = (v3y + mvy3 * tt) - (v1y + mvy1 * tt);
+  a20[2] = (v3z + mvz3 * tt) - (v1z + mvz1 * tt);
+  double pa1 = PS2[0] * a10[0] + PS2[1] * a10[1] + PS2[2] * a10[2];
+  double pa2 = PS2[0] * a20[0] + PS2[1] * a20[1] + PS2[2] * a20[2];
+  double a1a2 = a10[0] * a20[0] + a10[1] * a20[1] + a10[2] * a20[2];
+  double a12 = a10[0] * a10[0] + a10[1] * a10[1] + a10[2] * a10[2];
+  double a22 = a20[0] * a20[0] + a20[1] * a20[1] + a20[2] * a20[2];
+  double den = (a12 * a22) - (a1a2 * a1a2);
+  double eta = ((pa1 * a22) - (pa2 * a1a2)) / den;
+  double zeta = ((pa2 * a12) - (pa1 * a1a2)) / den;
+  if ((eta >= 0) && (zeta >= 0) && (eta + zeta <= 1) && (tt < (dtmd - rstep))) {
+    fulldt += tt;
+    double vd0 = (1.0 - eta - zeta) * mvx1 + eta * mvx2 + zeta * mvx3;
+    double vd1 = (1.0 - eta - zeta) * mvy1 + eta * mvy2 + zeta * mvy3;
+    double vd2 = (1.0 - eta - zeta) * mvz1 + eta * mvz2 + zeta * mvz3;
+    VX = 2.0 * vd0 - VX; VY = 2.0 * vd1 - VY; VZ = 2.0 * vd2 - VZ;
+    X_ = pd[0]; Y_ = pd[1]; Z_ = pd[2];
+    return true;
+  }
+  return false;
+}
+
+// free flight, walls and wrap after the membrane (maincode.cpp:516-560)
+__device__ __forceinline__ void finish_stream(const DevParams& p, double fullts, double& X, double& Y, double& Z,
+                                              double& VX, double& VY, double& VZ) {
+  const double dtmd = p.dtmd;
+  X += VX * (dtmd - fullts);
+  Y += VY * (dtmd - fullts);
+  Z += VZ * (dtmd - fullts);
+  const double ul = p.Lz, ll = 0;
+  if (Z > ul || Z < ll) {
+    double A[3], B[3];
+    const double wall = Z > ul ? ul : ll;
+    A[0] = X - VX * (dtmd - fullts); A[1] = Y - VY * (dtmd - fullts); A[2] = Z - VZ * (dtmd - fullts);
+    double sp = (wall - A[2]) / (Z - A[2]);
+    B[0] = A[0] + sp * (X - A[0]); B[1] = A[1] + sp * (Y - A[1]); B[2] = A[2] + sp * (Z - A[2]);
+    double dist = sqrt(((B[0] - A[0]) * (B[0] - A[0])) + ((B[1] - A[1]) * (B[1] - A[1])) + ((B[2] - A[2]) * (B[2] - A[2])));
+    double dtt = dist / sqrt((VX * VX) + (VY * VY) + (VZ * VZ));
+    if (Z > ul) { VX = p.wallspeed; VY = 0; VZ = 0; }
+    else { VX *= -1.0; VY *= -1.0; VZ *= -1.0; }
+    X = B[0] + VX * ((dtmd - fullts) - dtt);
+    Y = B[1] + VY * ((dtmd - fullts) - dtt);
+    Z = B[2] + VZ * ((dtmd - fullts) - dtt);
+  }
+  X = bbound(X, p.Lx);
+  Y = bbound(Y, p.Ly);
+}
+
+__device__ __forceinline__ bool in_stencil(const DevParams& p, double x, double y) {
+  return (x < 3.0 * p.a) || (x > p.Lx - (3.0 * p.a)) || (y < 3.0 * p.a) || (y > p.Ly - (3.0 * p.a));
+}
+
+// one thread per particle: free flight, walls and wrap for particles whose
+// cell has no triangles; the others are queued for k_stream_heavy and left
+// untouched here
+__global__ void __launch_bounds__(256) k_stream_fast(DevParams p, Solvent s, const int* __restrict__ lstart,
+                                                     const int* __restrict__ lidx, Snap sn,
+                                                     const TriPre* __restrict__ pre, int* queue, int* qn) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  double X = s.x[i], Y = s.y[i], Z = s.z[i];
+  double VX = s.vx[i], VY = s.vy[i], VZ = s.vz[i];
+  const double VX0 = VX, VY0 = VY, VZ0 = VZ;
+  int fx = (int)floor(bbound(X, p.Lx));
+  int fy = (int)floor(bbound(Y, p.Ly));
+  int fz = (int)floor(Z + 1.0);
+  int pid = cell_of(p, fx, fy, fz);
+  const int l0 = __ldg(lstart + pid), l1 = __ldg(lstart + pid + 1);
+  (void)sn; (void)pre; (void)lidx;
+  if (l1 > l0) {
+    // near the membrane: a warp of k_stream_heavy takes this particle
+    unsigned m = __activemask();
+    int leader = __ffs(m) - 1;
+    int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(qn, __popc(m));
+    base = __shfl_sync(m, base, leader);
+    queue[base + __popc(m & ((1u << lane) - 1))] = (int)i;
+    return;
+  }
+  finish_stream(p, 0.0, X, Y, Z, VX, VY, VZ);
+  s.x[i] = X; s.y[i] = Y; s.z[i] = Z;
+  if (VX != VX0 || VY != VY0 || VZ != VZ0 || VX0 != VX0) { s.vx[i] = VX; s.vy[i] = VY; s.vz[i] = VZ; }
+}
+
+// one warp per queued particle: lanes test 32 triangles of the list at a
+// time against the current particle state; the first candidate (lowest list
+// position) is resolved, and testing resumes after it with the updated
+// state -- the same sequence of states as the sequential loop.
+// the triangle walk of reflectionFed for one particle, by a whole warp:
+// lanes test 32 list entries at a time on copies of the particle state;
+// the first entry that would hit (lowest list position) is applied on every
+// lane and testing resumes after it with the updated state
+__device__ __forceinline__ void stream_heavy_walk(const DevParams& p, const Snap& sn, const TriPre* __restrict__ pre,
+                                                  const int* __restrict__ lidx, int l0, int l1, int lane, int indio,
+                                                  double& X, double& Y, double& Z, double& VX, double& VY,
+                                                  double& VZ, double& fulldt) {
+  int cur = l0;
+  while (cur < l1) {
+    bool found = false;
+    const int j = cur + lane;
+    if (j < l1) {
+      double x = X, y = Y, z = Z, vx = VX, vy = VY, vz = VZ, fd = 0.0;
+      found = tri_visit(p, sn, pre, lidx[j], x, y, z, vx, vy, vz, indio, fd, !in_stencil(p, X, Y));
+    }
+    unsigned ball = __ballot_sync(0xffffffffu, found);
+    if (ball == 0) { cur += 32; continue; }
+    int first = __ffs(ball) - 1;
+    int jj = lidx[cur + first];
+    tri_visit(p, sn, pre, jj, X, Y, Z, VX, VY, VZ, indio, fulldt, !in_stencil(p, X, Y));
+    cur += first + 1;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_stream_heavy(DevParams p, Solvent s, const int* __restrict__ lstart,
+                                                      const int* __restrict__ lidx, Snap sn,
+                                                      const TriPre* __restrict__ pre, const int* queue,
+                                                      const int* qn) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int nq = *qn;
+  for (int64_t q = w; q < nq; q += nw) {
+    const int64_t i = queue[q];
+    double X = s.x[i], Y = s.y[i], Z = s.z[i];
+    double VX = s.vx[i], VY = s.vy[i], VZ = s.vz[i];
+    const double VX0 = VX, VY0 = VY, VZ0 = VZ;
+    const int indio = s.indio[i];
+    int fx = (int)floor(bbound(X, p.Lx));
+    int fy = (int)floor(bbound(Y, p.Ly));
+    int fz = (int)floor(Z + 1.0);
+    int pid = cell_of(p, fx, fy, fz);
+    const int l0 = lstart[pid], l1 = lstart[pid + 1];
+    double fulldt = 0.0;
+    stream_heavy_walk(p, sn, pre, lidx, l0, l1, lane, indio, X, Y, Z, VX, VY, VZ, fulldt);
+    if (lane == 0) {
+      finish_stream(p, fulldt, X, Y, Z, VX, VY, VZ);
+      s.x[i] = X; s.y[i] = Y; s.z[i] = Z;
+      if (VX != VX0 || VY != VY0 || VZ != VZ0 || VX0 != VX0) { s.vx[i] = VX; s.vy[i] = VY; s.vz[i] = VZ; }
+    }
+  }
+}
+
+// ========================================================= membrane step ====
+// drift (maincode.cpp:566-598) then TotalVA (Src/memfuncs.cpp:161-190), one CTA
+__global__ void __launch_bounds__(1024) k_drift_va(DevParams p, Membrane m) {
+  for (int i = threadIdx.x; i < p.nv; i += blockDim.x) {
+    double x = m.x[i], y = m.y[i], z = m.z[i];
+    x += (m.vx[i] * p.dtmd);
+    y += (m.vy[i] * p.dtmd);
+    z += (m.vz[i] * p.dtmd);
+    if (x > p.Lx) { x -= p.Lx; m.ix[i] += 1; }
+    if (x < 0) { x += p.Lx; m.ix[i] -= 1; }
+    if (y > p.Ly) { y -= p.Ly; m.iy[i] += 1; }
+    if (y < 0) { y += p.Ly; m.iy[i] -= 1; }
+    m.x[i] = x; m.y[i] = y; m.z[i] = z;
+  }
+  if (threadIdx.x == 0) {
+    MemScalars* sc = m.sc;
+    for (int k = 0; k < 3; ++k)
+      sc->para[k] += (sc->paraV[k] * p.dtmd) + (sc->paraft[k] * p.dtmd * p.dtmd / (2.0 * p.PRmass));
+    if (sc->para[0] > p.Lx) { sc->para[0] -= p.Lx; sc->paradx += 1; }
+    else if (sc->para[0] < 0) { sc->para[0] += p.Lx; sc->paradx -= 1; }
+    if (sc->para[1] > p.Ly) { sc->para[1] -= p.Ly; sc->parady += 1; }
+    else if (sc->para[1] < 0) { sc->para[1] += p.Ly; sc->parady -= 1; }
+  }
+  __syncthreads();
+  // per-triangle terms in parallel; the two sums left to right in triangle
+  // order, as the reference's one-thread reduction forms them: the area
+  // constraint multiplies the rounding drift of Sarea by kappasa/Sarea0
+  for (int i = threadIdx.x; i < p.nt; i += blockDim.x) {
+    int l1 = m.t1[i], l2 = m.t2[i], l3 = m.t3[i];
+    double A[3], B[3], eta[3], Cn[3];
+    A[0] = UXm(l2) - UXm(l1); A[1] = UYm(l2) - UYm(l1); A[2] = m.z[l2] - m.z[l1];
+    B[0] = UXm(l3) - UXm(l1); B[1] = UYm(l3) - UYm(l1); B[2] = m.z[l3] - m.z[l1];
+    cp(A, B, eta);
+    m.area[i] = 0.5 * sqrt(eta[0] * eta[0] + eta[1] * eta[1] + eta[2] * eta[2]);
+    Cn[0] = (UXm(l1) + UXm(l2) + UXm(l3)) / 3.0;
+    Cn[1] = (UYm(l1) + UYm(l2) + UYm(l3)) / 3.0;
+    Cn[2] = (m.z[l1] + m.z[l2] + m.z[l3]) / 3.0;
+    m.vol[i] = (1.0 / 6.0) * ((eta[0] * Cn[0]) + (eta[1] * Cn[1]) + (eta[2] * Cn[2]));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+#pragma unroll 8
+    for (int i = 0; i < p.nt; ++i) t += m.area[i];
+    m.sc->Sarea = t;
+  } else if (threadIdx.x == 32) {
+    double t = 0.0;
+#pragma unroll 8
+    for (int i = 0; i < p.nt; ++i) t += m.vol[i];
+    m.sc->Volume = t;
+  }
+}
+
+// force terms of every edge (WLC + POW), triangle (local/global area and
+// volume) and bending dihedral, stored per term in slots so the per-vertex
+// gather can add them in the reference's order (Src/memfuncs.cpp:233-427)
+__global__ void __launch_bounds__(256) k_force_items(DevParams p, Membrane m, double* __restrict__ slot) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const MemScalars* sc = m.sc;
+  if (t < p.ne) {
+    int i = t;
+    int l1 = m.e1[i], l2 = m.e2[i];
+    double l0 = m.l0[i];
+    double A[3];
+    A[0] = UXm(l1) - UXm(l2); A[1] = UYm(l1) - UYm(l2); A[2] = m.z[l1] - m.z[l2];
+    double aa = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+    A[0] /= aa; A[1] /= aa; A[2] /= aa;
+    double xx = aa / (2.5 * l0);
+    double xxx = 1.0 / (4.0 * (1.0 - xx) * (1.0 - xx));
+    const double kp = m.kappap[i];
+    double* S = slot + (int64_t)12 * i;
+    for (int k = 0; k < 3; ++k) {
+      S[0 + k] = (-1.0 / (p.elap)) * (xxx - 0.25 + xx) * A[k];
+      S[3 + k] = kp * A[k] / (aa * aa);
+      S[6 + k] = (1.0 / (p.elap)) * (xxx - 0.25 + xx) * A[k];
+      S[9 + k] = -kp * A[k] / (aa * aa);
+    }
+    return;
+  }
+  t -= p.ne;
+  if (t < p.nt) {
+    int i = t;
+    int l1 = m.t1[i], l2 = m.t2[i], l3 = m.t3[i];
+    const double Sarea = sc->Sarea, Volume = sc->Volume;
+    double beta = -p.kappasa * (Sarea - p.Sarea0) / p.Sarea0;
+    double betav = -p.kappav * (Volume - p.Volume0) / (p.Volume0);
+    double A0[3], B0[3], e0[3];
+    A0[0] = UXm(l2) - UXm(l1); A0[1] = UYm(l2) - UYm(l1); A0[2] = m.z[l2] - m.z[l1];
+    B0[0] = UXm(l3) - UXm(l1); B0[1] = UYm(l3) - UYm(l1); B0[2] = m.z[l3] - m.z[l1];
+    cp(A0, B0, e0);
+    double area = 0.5 * sqrt(e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2]);
+    double alpha = beta / (4.0 * area);
+    double alphad = -p.kappad * (area - m.tarea[i]) / (4.0 * m.tarea[i] * area);
+    double A21[3], A13[3], A32[3], eta[3], C[3], B[3];
+    A21[0] = UXm(l2) - UXm(l1); A21[1] = UYm(l2) - UYm(l1); A21[2] = m.z[l2] - m.z[l1];
+    A13[0] = UXm(l1) - UXm(l3); A13[1] = UYm(l1) - UYm(l3); A13[2] = m.z[l1] - m.z[l3];
+    A32[0] = UXm(l3) - UXm(l2); A32[1] = UYm(l3) - UYm(l2); A32[2] = m.z[l3] - m.z[l2];
+    cp(A13, A21, eta);
+    B[0] = (UXm(l1) + UXm(l2) + UXm(l3)) / 3.0;
+    B[1] = (UYm(l1) + UYm(l2) + UYm(l3)) / 3.0;
+    B[2] = (m.z[l1] + m.z[l2] + m.z[l3]) / 3.0;
+    double* S = slot + (int64_t)12 * p.ne + (int64_t)27 * i;
+    const double* sides[3] = {A32, A13, A21};
+    for (int c = 0; c < 3; ++c) {
+      cp(eta, sides[c], C);
+      for (int k = 0; k < 3; ++k) { S[6 * c + k] = alpha * C[k]; S[6 * c + 3 + k] = alphad * C[k]; }
+      cp(B, sides[c], C);
+      for (int k = 0; k < 3; ++k) S[18 + 3 * c + k] = betav * ((eta[k] / 3.0) + C[k]) / 6.0;
+    }
+    return;
+  }
+  t -= p.nt;
+  if (t < p.ne) {
+    int i = t;
+    int l2, l3;
+    if (m.iedge[i] == -1) { l3 = m.e1[i]; l2 = m.e2[i]; } else { l2 = m.e1[i]; l3 = m.e2[i]; }
+    int l1 = m.es1[i], l4 = m.es2[i];
+    double a21[3], a31[3], a24[3], a34[3], a32[3], t1[3], t2[3], eta[3], zeta[3], C[3], D[3], E[3], F[3];
+    a21[0] = UXm(l2) - UXm(l1); a21[1] = UYm(l2) - UYm(l1); a21[2] = m.z[l2] - m.z[l1];
+    a31[0] = UXm(l3) - UXm(l1); a31[1] = UYm(l3) - UYm(l1); a31[2] = m.z[l3] - m.z[l1];
+    a24[0] = UXm(l2) - UXm(l4); a24[1] = UYm(l2) - UYm(l4); a24[2] = m.z[l2] - m.z[l4];
+    a34[0] = UXm(l3) - UXm(l4); a34[1] = UYm(l3) - UYm(l4); a34[2] = m.z[l3] - m.z[l4];
+    a32[0] = UXm(l3) - UXm(l2); a32[1] = UYm(l3) - UYm(l2); a32[2] = m.z[l3] - m.z[l2];
+    t1[0] = (UXm(l1) + UXm(l2) + UXm(l3)) / 3.0;
+    t1[1] = (UYm(l1) + UYm(l2) + UYm(l3)) / 3.0;
+    t1[2] = (m.z[l1] + m.z[l2] + m.z[l3]) / 3.0;
+    t2[0] = (UXm(l4) + UXm(l2) + UXm(l3)) / 3.0;
+    t2[1] = (UYm(l4) + UYm(l2) + UYm(l3)) / 3.0;
+    t2[2] = (m.z[l4] + m.z[l2] + m.z[l3]) / 3.0;
+    cp(a21, a31, eta);
+    cp(a34, a24, zeta);
+    double etam = sqrt(eta[0] * eta[0] + eta[1] * eta[1] + eta[2] * eta[2]);
+    double zetam = sqrt(zeta[0] * zeta[0] + zeta[1] * zeta[1] + zeta[2] * zeta[2]);
+    double costh = (eta[0] * zeta[0] + eta[1] * zeta[1] + eta[2] * zeta[2]) / (etam * zetam);
+    if (costh > 1.0) costh = 1.0;
+    if (costh < -1.0) costh = -1.0;
+    if (costh == 1.0) costh -= 0.0005;
+    if (costh == -1.0) costh += 0.0005;
+    double sinth = sqrt(1.0 - costh * costh);
+    double tt0 = t1[0] - t2[0];
+    double tt1 = t1[1] - t2[1];
+    double factor = (((eta[0] - zeta[0]) * tt0) + ((eta[1] - zeta[1]) * tt1) + ((eta[2] - zeta[2]) * (t1[2] - t2[2])));
+    double fact = (factor >= 0.0) ? 1.0 : -1.0;
+    sinth = fact * sinth;
+    double betab = p.kappab * (sinth * p.cth0 - costh * p.sth0) / sinth;
+    double b11 = -(betab * costh) / (etam * etam);
+    double b22 = -(betab * costh) / (zetam * zetam);
+    double b12 = betab / (etam * zetam);
+    double* S = slot + (int64_t)12 * p.ne + (int64_t)27 * p.nt + (int64_t)12 * i;
+    cp(eta, a32, C);
+    cp(zeta, a32, D);
+    for (int k = 0; k < 3; ++k) { S[k] = b11 * C[k] + b12 * D[k]; S[3 + k] = -b12 * C[k] - b22 * D[k]; }
+    cp(eta, a31, C); cp(zeta, a31, D); cp(eta, a34, E); cp(zeta, a34, F);
+    for (int k = 0; k < 3; ++k) S[6 + k] = -b11 * C[k] + b12 * (E[k] - D[k]) + b22 * F[k];
+    cp(eta, a21, C); cp(zeta, a21, D); cp(eta, a24, E); cp(zeta, a24, F);
+    for (int k = 0; k < 3; ++k) S[9 + k] = b11 * C[k] + b12 * (-E[k] + D[k]) - b22 * F[k];
+  }
+}
+
+__device__ __forceinline__ bool wca_f(const DevParams& p, const Membrane& m, const MemScalars* sc, int i, double X[3]) {
+  double cutoff = p.paraR, epsilon = 0.1, sigma = 0.890898718 * cutoff;
+  double A[3];
+  A[0] = (sc->para[0] + sc->paradx * p.Lx) - (m.x[i] + m.ix[i] * p.Lx);
+  A[1] = (sc->para[1] + sc->parady * p.Ly) - (m.y[i] + m.iy[i] * p.Ly);
+  A[2] = sc->para[2] - m.z[i];
+  double aa = A[0] * A[0] + A[1] * A[1] + A[2] * A[2];
+  if (aa <= cutoff * cutoff) {
+    double ex = (sigma * sigma * sigma * sigma * sigma * sigma) / (aa * aa * aa);
+    X[0] = (24.0 * epsilon / aa) * ((2.0 * ex * ex) - ex) * A[0];
+    X[1] = (24.0 * epsilon / aa) * ((2.0 * ex * ex) - ex) * A[1];
+    X[2] = (24.0 * epsilon / aa) * ((2.0 * ex * ex) - ex) * A[2];
+    return true;
+  }
+  return false;
+}
+
+// per vertex, in the order of maincode.cpp:603-665: pfdt's -X, the sum of
+// the force slots (reference order), gravity, bond spring, wall repulsion
+__global__ void __launch_bounds__(128) k_force_gather(DevParams p, Membrane m, const double* __restrict__ slot,
+                                                      const int* __restrict__ gstart, const int* __restrict__ gidx) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nv) return;
+  const MemScalars* sc = m.sc;
+  double f[3] = {m.fx[i], m.fy[i], m.fz[i]};
+  double X[3];
+  if (wca_f(p, m, sc, i, X)) { f[0] -= X[0]; f[1] -= X[1]; f[2] -= X[2]; }
+  double ff[3] = {0.0, 0.0, 0.0};
+  for (int q = gstart[i]; q < gstart[i + 1]; ++q) {
+    const double* S = slot + 3 * (int64_t)gidx[q];
+    ff[0] += S[0]; ff[1] += S[1]; ff[2] += S[2];
+  }
+  f[0] += ff[0]; f[1] += ff[1]; f[2] += ff[2];
+  f[2] += -p.Fg / (double)p.nv;
+  if (m.bondi[i] == 1) {
+    int jj = m.bondl[i];
+    double A[3];
+    A[0] = m.x[i] - m.xlig[jj];
+    A[1] = m.y[i] - m.ylig[jj];
+    A[2] = m.z[i];
+    A[0] -= p.Lx * round(A[0] / p.Lx);
+    A[1] -= p.Ly * round(A[1] / p.Ly);
+    double aa = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+    A[0] /= aa; A[1] /= aa; A[2] /= aa;
+    if (aa > p.el0) {
+      f[0] += -p.ks * (aa - p.el0) * A[0];
+      f[1] += -p.ks * (aa - p.el0) * A[1];
+      f[2] += -p.ks * (aa - p.el0) * A[2];
+    }
+  }
+  double cc = m.z[i];
+  if (cc < 0.5) f[2] += 300.0 * exp(-50.0 * cc);
+  cc = p.Lz - m.z[i];
+  if (cc < 0.5) f[2] -= 300.0 * exp(-50.0 * cc);
+  m.fx[i] = f[0]; m.fy[i] = f[1]; m.fz[i] = f[2];
+}
+
+__device__ __forceinline__ bool in_liglist_f(const DevParams& p, int cell, double xl, double yl) {
+  int k = cell % p.nz, j = (cell / p.nz) % p.ny, i = cell / (p.nz * p.ny);
+  double zmax = -1.0 + (double)k * p.a + p.a;
+  if (!(zmax <= 2.0)) return false;
+  double xmin = (double)i * p.a, xmax = (double)i * p.a + p.a;
+  double ymin = (double)j * p.a, ymax = (double)j * p.a + p.a;
+  double A0 = fabs(((xmin + xmax) * 0.5) - xl);
+  double A1 = fabs(((ymin + ymax) * 0.5) - yl);
+  A0 -= p.Lx * round(A0 / p.Lx);
+  A1 -= p.Ly * round(A1 / p.Ly);
+  return (A0 < 1.5) && (A1 < 1.5);
+}
+
+// One CTA: bond preparation (maincode.cpp:668-723), second half-kick
+// (:727-733), pfdt's parasite sum in vertex order (Src/memfuncs.cpp:469-482),
+// bond_dynamics (:16-54) over the compacted, ordered list of bonded or
+// eligible vertices with its uniforms drawn in parallel, the parasite kick
+// (:736-744), and, when the next step has no collision, the next step's
+// half-kick (:487-496) with the snapshot and triangle prep for its
+// streaming.  Each thread owns a contiguous run of vertices so that a block
+// scan of per-thread counts keeps vertex order in the compacted lists.
+constexpr int kTailT = 1024, kTailList = 1024, kTailDraws = 2048;
+__global__ void __launch_bounds__(kTailT) k_mem_tail(DevParams p, Membrane m, uint64_t epoch, int next_kick,
+                                                    TriPre* pre, Snap sn) {
+  __shared__ int s_a[kTailT], s_w[kTailT], s_d[kTailT];
+  __shared__ int s_list[kTailList], s_wlist[kTailList], s_doff[kTailList];
+  __shared__ double s_u[kTailDraws];
+  __shared__ int s_tot[3];
+  const int T = blockDim.x, tid = threadIdx.x;
+  MemScalars* sc = m.sc;
+  const int chunk = (p.nv + T - 1) / T;
+  const int v0 = min(tid * chunk, p.nv), v1 = min(v0 + chunk, p.nv);
+  int na = 0, nw = 0, nd = 0;
+  for (int ii = v0; ii < v1; ++ii) {
+    double A[3], B[3];
+    if (m.bondi[ii] == 1) {
+      int p1modx = m.ix[ii], p1mody = m.iy[ii], jj = m.bondl[ii];
+      A[0] = (m.x[ii] + p1modx * p.Lx) - (m.xlig[jj] + p1modx * p.Lx);
+      A[1] = (m.y[ii] + p1mody * p.Ly) - (m.ylig[jj] + p1mody * p.Ly);
+      A[2] = m.z[ii] - 0.0;
+      double xx = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+      if (xx > p.el0) {
+        B[0] = -p.ks * (xx - p.el0) * A[0] / xx;
+        B[1] = -p.ks * (xx - p.el0) * A[1] / xx;
+        B[2] = -p.ks * (xx - p.el0) * A[2] / xx;
+      } else {
+        B[0] = B[1] = B[2] = 0.0;
+      }
+      double bb = sqrt(B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+      double koff = p.offrate * exp(bb / p.FD);
+      m.poff[ii] = 1.0 - exp(-koff * p.dtmd);
+      na += 1; nd += 1;
+    } else if ((m.z[ii] < p.dthr) && (m.bondi[ii] == 0) && (m.knob[ii] == 1)) {
+      const int pid = m.pid[ii];
+      m.pon[ii] = 1.0 - exp(-p.onrate * p.dtmd);
+      int n = 0;
+      double* pd = m.pair_d + (int64_t)ii * kMaxPairs;
+      int* pj = m.pair_j + (int64_t)ii * kMaxPairs;
+      const int p1modx = m.ix[ii], p1mody = m.iy[ii];
+      const double vx = m.x[ii], vy = m.y[ii];
+      int gx0 = max((int)floor((vx - p.dthr) / 0.5) - 1, 0), gx1 = min((int)floor((vx + p.dthr) / 0.5) + 1, p.nligx - 1);
+      int gy0 = max((int)floor((vy - p.dthr) / 0.5) - 1, 0), gy1 = min((int)floor((vy + p.dthr) / 0.5) + 1, p.nligy - 1);
+      for (int gx = gx0; gx <= gx1; ++gx) {
+        for (int gy = gy0; gy <= gy1; ++gy) {
+          int j = gx * p.nligy + gy;
+          double xl = m.xlig[j], yl = m.ylig[j];
+          if (!in_liglist_f(p, pid, xl, yl)) continue;
+          A[0] = (vx + p1modx * p.Lx) - (xl + p1modx * p.Lx);
+          A[1] = (vy + p1mody * p.Ly) - (yl + p1mody * p.Ly);
+          A[2] = m.z[ii] - 0.0;
+          double aaa = (A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+          if (aaa <= p.dthr * p.dthr && n < kMaxPairs) {
+            int r = n++;
+            while (r > 0 && (pd[r - 1] > aaa || (pd[r - 1] == aaa && pj[r - 1] > j))) { pd[r] = pd[r - 1]; pj[r] = pj[r - 1]; --r; }
+            pd[r] = aaa; pj[r] = j;
+          }
+        }
+      }
+      m.npair[ii] = n;
+      na += 1; nd += n;
+    }
+    double X[3];
+    nw += wca_f(p, m, sc, ii, X) ? 1 : 0;
+    m.vx[ii] += (m.fx[ii] * p.dtmd / (2.0 * p.pmass));
+    m.vy[ii] += (m.fy[ii] * p.dtmd / (2.0 * p.pmass));
+    m.vz[ii] += (m.fz[ii] * p.dtmd / (2.0 * p.pmass));
+  }
+  s_a[tid] = na; s_w[tid] = nw; s_d[tid] = nd;
+  __syncthreads();
+  // exclusive scans of the three per-thread counts, one warp per array
+  if (tid < 96) {
+    int* arr = tid < 32 ? s_a : (tid < 64 ? s_w : s_d);
+    const int lane = tid & 31;
+    int carry = 0;
+    for (int base = 0; base < T; base += 32) {
+      int x = arr[base + lane], v = x;
+      for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += y; }
+      arr[base + lane] = carry + v - x;
+      carry += __shfl_sync(0xffffffffu, v, 31);
+    }
+    if (lane == 0) s_tot[tid >> 5] = carry;
+  }
+  __syncthreads();
+  const bool fits = s_tot[0] <= kTailList && s_tot[1] <= kTailList && s_tot[2] <= kTailDraws;
+  if (fits) {
+    int oa = s_a[tid], ow = s_w[tid], od = s_d[tid];
+    for (int ii = v0; ii < v1; ++ii) {
+      const bool bonded = m.bondi[ii] == 1;
+      const bool elig = !bonded && (m.z[ii] < p.dthr) && (m.knob[ii] == 1);
+      if (bonded || elig) {
+        s_list[oa] = ii;
+        s_doff[oa] = od;
+        int n = bonded ? 1 : m.npair[ii];
+        for (int r = 0; r < n; ++r) s_u[od + r] = draw_uniform(p.seed, STREAM_BOND, epoch, (uint64_t)(od + r));
+        oa += 1; od += n;
+      }
+      double X[3];
+      if (wca_f(p, m, sc, ii, X)) s_wlist[ow++] = ii;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int na_t = s_tot[0], nw_t = s_tot[1];
+    double fx = 0, fy = 0, fz = 0;
+    if (fits) {
+      for (int q = 0; q < nw_t; ++q) {
+        double X[3];
+        wca_f(p, m, sc, s_wlist[q], X);
+        fx += X[0]; fy += X[1]; fz += X[2];
+      }
+    } else {
+      for (int ii = 0; ii < p.nv; ++ii) {
+        double X[3];
+        if (wca_f(p, m, sc, ii, X)) { fx += X[0]; fy += X[1]; fz += X[2]; }
+      }
+    }
+    sc->parafdt[0] += fx; sc->parafdt[1] += fy; sc->parafdt[2] += fz;
+    uint64_t k = 0;
+    const int nlist = fits ? na_t : p.nv;
+    for (int q = 0; q < nlist; ++q) {
+      const int ii = fits ? s_list[q] : q;
+      if (m.bondi[ii] == 1) {
+        double randoff = fits ? s_u[k] : draw_uniform(p.seed, STREAM_BOND, epoch, k);
+        ++k;
+        int jj = m.bondl[ii];
+        if (m.poff[ii] > randoff) { m.bondi[ii] = 0; m.bondl[ii] = p.randno; m.ligi[jj] = 0; }
+      } else if ((m.z[ii] < p.dthr) && (m.bondi[ii] == 0) && (m.knob[ii] == 1)) {
+        const int n = m.npair[ii];
+        for (int r = 0; r < n; ++r) {
+          int j = m.pair_j[(int64_t)ii * kMaxPairs + r];
+          double pon = m.pon[ii];
+          double randon = fits ? s_u[k] : draw_uniform(p.seed, STREAM_BOND, epoch, k);
+          ++k;
+          if ((pon > randon) && (m.ligi[j] == 0)) { m.ligi[j] = 1; m.bondi[ii] = 1; m.bondl[ii] = j; }
+        }
+      }
+    }
+    for (int c = 0; c < 3; ++c) sc->paraV[c] += ((sc->paraft[c] + sc->parafdt[c]) * p.dtmd / (2.0 * p.PRmass));
+    for (int c = 0; c < 3; ++c) { sc->paraft[c] = sc->parafdt[c]; sc->parafdt[c] = 0.0; }
+  }
+  if (!next_kick) return;
+  __syncthreads();
+  for (int i = tid; i < p.nv; i += T) {
+    double vx = m.vx[i] + (m.fx[i] * p.dtmd / (2.0 * p.pmass));
+    double vy = m.vy[i] + (m.fy[i] * p.dtmd / (2.0 * p.pmass));
+    double vz = m.vz[i] + (m.fz[i] * p.dtmd / (2.0 * p.pmass));
+    m.vx[i] = vx; m.vy[i] = vy; m.vz[i] = vz;
+    m.fx[i] = 0.0; m.fy[i] = 0.0; m.fz[i] = 0.0;
+    sn.x[i] = m.x[i]; sn.y[i] = m.y[i]; sn.z[i] = m.z[i];
+    sn.vx[i] = vx; sn.vy[i] = vy; sn.vz[i] = vz;
+  }
+  __syncthreads();
+  for (int j = tid; j < p.nt; j += T) tri_prep_one(p, m, j, m.vx, m.vy, m.vz, pre);
+}
+
+// half-kick + snapshot + triangle prep as separate launches (after a
+// collision, or at the first step)
+__global__ void k_kick_snap(DevParams p, Membrane m, Snap sn) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nv) return;
+  double vx = m.vx[i] + (m.fx[i] * p.dtmd / (2.0 * p.pmass));
+  double vy = m.vy[i] + (m.fy[i] * p.dtmd / (2.0 * p.pmass));
+  double vz = m.vz[i] + (m.fz[i] * p.dtmd / (2.0 * p.pmass));
+  m.vx[i] = vx; m.vy[i] = vy; m.vz[i] = vz;
+  m.fx[i] = 0.0; m.fy[i] = 0.0; m.fz[i] = 0.0;
+  sn.x[i] = m.x[i]; sn.y[i] = m.y[i]; sn.z[i] = m.z[i];
+  sn.vx[i] = vx; sn.vy[i] = vy; sn.vz[i] = vz;
+}
+__global__ void k_tri_prep(DevParams p, Membrane m, TriPre* pre) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < p.nt) tri_prep_one(p, m, j, m.vx, m.vy, m.vz, pre);
+}
+
+__global__ void k_snap(DevParams p, Membrane m, Snap sn) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nv) return;
+  sn.x[i] = m.x[i]; sn.y[i] = m.y[i]; sn.z[i] = m.z[i];
+  sn.vx[i] = m.vx[i]; sn.vy[i] = m.vy[i]; sn.vz[i] = m.vz[i];
+}
+
+// ================================================================ launch ======
+void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st) {
+  k_snap<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.snap[buf]);
+  k_tri_prep<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.pre[buf]);
+}
+
+void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st) {
+  k_kick_snap<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.snap[buf]);
+  k_tri_prep<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.pre[buf]);
+}
+
+void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st) {
+  cudaMemsetAsync(f.qn, 0, sizeof(int), st);
+  if (s.n) {
+    k_stream_fast<<<nb(s.n, 256), 256, 0, st>>>(p, s, c.lstart, c.lidx, f.snap[buf], f.pre[buf], f.queue, f.qn);
+    k_stream_heavy<<<148 * 4, 256, 0, st>>>(p, s, c.lstart, c.lidx, f.snap[buf], f.pre[buf], f.queue, f.qn);
+  }
+}
+
+void fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st) { k_drift_va<<<1, 1024, 0, st>>>(p, m); }
+
+void fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
+                      cudaStream_t st) {
+  int items = 2 * p.ne + p.nt;
+  k_force_items<<<nb(items, 256), 256, 0, st>>>(p, m, f.slot);
+  k_force_gather<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.slot, f.gstart, f.gidx);
+  k_mem_tail<<<1, kTailT, 0, st>>>(p, m, epoch, next_kick, f.pre[next_buf], f.snap[next_buf]);
+}
+
+void fast_membrane(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
+                   cudaStream_t st) {
+  fast_drift_va(p, m, st);
+  fast_forces_tail(p, m, f, epoch, next_kick, next_buf, st);
+}
+
+}  // namespace irbc
+
+// FP32-bulk solvent kernels share the device helpers above
+#include "fp32.cuh"

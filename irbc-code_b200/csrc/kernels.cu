@@ -524,6 +524,21 @@ static void swap_solvent(Solvent& s) {
   std::swap(s.id, s.id2); std::swap(s.indio, s.indio2); std::swap(s.pid, s.pid2);
 }
 
+void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cudaStream_t st) {
+  int n2 = 1;
+  while (n2 < p.nv) n2 <<= 1;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
+    attr_set = true;
+  }
+  k_vbin<<<1, 1024, sizeof(uint64_t) * n2, st>>>(p, m, c.ncm, epoch);
+}
+
+void launch_ghost_flags(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st) {
+  k_ghost_flags<<<nblk(c.n, 256), 256, 0, st>>>(p, c.cnt, c.ncm, m.sc, c.wrank, c.mrank);
+}
+
 void launch_collide(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
                     cudaStream_t st) {
   cudaMemsetAsync(c.cnt, 0, sizeof(int) * c.n, st);
@@ -550,55 +565,8 @@ void launch_collide(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint6
 
 // ============================================================== stream =====
 // Streaming with bounce-back: reflectionFed(i, 0) (Src/solfuncs.cpp:400-598)
-// then the wall treatment and wrap of maincode.cpp:515-560.
-__device__ __forceinline__ double solve_p3_tt(double aa, double b, double c, double dtmd) {
-  // SolveP3 (Src/poly34.cpp:26-55) + root selection of Solve (Src/solfuncs.cpp:369-396)
-  const double TwoPi = 6.28318530717958648, eps = 1e-14;
-  double x[3];
-  int nroot;
-  double a2 = aa * aa;
-  double q = (a2 - 3 * b) / 9;
-  double r = (aa * (2 * a2 - 9 * b) + 27 * c) / 54;
-  double r2 = r * r;
-  double q3 = q * q * q;
-  if (r2 < q3) {
-    double t = r / sqrt(q3);
-    if (t < -1) t = -1;
-    if (t > 1) t = 1;
-    t = acos(t);
-    aa /= 3; q = -2 * sqrt(q);
-    x[0] = q * cos(t / 3) - aa;
-    x[1] = q * cos((t + TwoPi) / 3) - aa;
-    x[2] = q * cos((t - TwoPi) / 3) - aa;
-    nroot = 3;
-  } else {
-    double A = -pow(fabs(r) + sqrt(r2 - q3), 1. / 3);
-    if (r < 0) A = -A;
-    double B = (A == 0) ? 0 : q / A;
-    aa /= 3;
-    x[0] = (A + B) - aa;
-    x[1] = -0.5 * (A + B) - aa;
-    x[2] = 0.5 * sqrt(3.) * (A - B);
-    if (fabs(x[2]) < eps) { x[2] = x[1]; nroot = 2; } else nroot = 1;
-  }
-  double tt;
-  if (nroot == 3 || nroot == 2) {
-    // sort three values ascending (std::sort on 3 doubles without NaN)
-    double u0 = x[0], u1 = x[1], u2 = x[2], t;
-    if (u1 < u0) { t = u0; u0 = u1; u1 = t; }
-    if (u2 < u1) { t = u1; u1 = u2; u2 = t; }
-    if (u1 < u0) { t = u0; u0 = u1; u1 = t; }
-    tt = u0;
-    if ((tt < 0) || (tt > dtmd)) {
-      tt = u1;
-      if ((tt < 0) || (tt > dtmd)) tt = u2;
-    }
-  } else {
-    tt = x[0];
-  }
-  return tt;
-}
-
+// then the wall treatment and wrap of maincode.cpp:515-560.  The cubic
+// contact-time solver solve_p3_tt is in common.cuh.
 struct VertexView {
   const double *x, *y, *z, *vx, *vy, *vz;
 };

@@ -28,6 +28,7 @@ struct Cells {
   int *cnt = nullptr, *start = nullptr, *ncm = nullptr, *wrank = nullptr, *mrank = nullptr;
   int *totals = nullptr;        // [0] particles, [1] wall ghost cells, [2] membrane ghost cells, [3] llist entries
   double *par = nullptr;        // 7 per cell: vcm[3], unit[3], ThE
+  float *parf = nullptr;        // the same as 8 floats per cell (FP32 solvent)
   int *lstart = nullptr, *lidx = nullptr, *lstart2 = nullptr, *lidx2 = nullptr, *lcnt = nullptr;
   int64_t lcap = 0, lcap2 = 0;
   int *scan_part = nullptr;     // scan scratch: 3 ints per block
@@ -68,6 +69,8 @@ void launch_init_solvent(const DevParams& p, Solvent& s, cudaStream_t st);
 void launch_classify(const DevParams& p, Solvent& s, const Membrane& m, cudaStream_t st);
 void launch_collide(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
                     cudaStream_t st);
+void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cudaStream_t st);
+void launch_ghost_flags(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
 void launch_stream(const DevParams& p, Solvent& s, const Cells& c, const Membrane& m, cudaStream_t st);
 // returns the total list length the update needs (host sync inside)
 int64_t launch_llist_count(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
