@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "fast.h"
+#include "fp32.h"
 #include "irbc.h"
 #include "sim.h"
 
@@ -30,6 +31,8 @@ struct irbc_handle {
   cudaStream_t st = nullptr;   // solvent kernels; every public call orders on it
   cudaStream_t st2 = nullptr;  // membrane kernels, run beside the solvent ones
   FastBufs fb;
+  bool fp32 = false;           // solvent held in sf (float4) between exchanges
+  SolventF sf;
   int snap_buf = 0;            // which snapshot the next streaming step reads
   bool snap_ready = false;     // snapshot/triangle prep of the next step done
   cudaEvent_t ev_snap = nullptr, ev_mem = nullptr, ev_coll = nullptr, ev_str[2] = {nullptr, nullptr};
@@ -354,6 +357,16 @@ int upload_mesh(irbc_handle* h, const HostMesh& M) {
 
 int64_t launches_in(const irbc_handle* h) { return g_launches.load() - h->launches0; }
 
+// the solvent kernels of the handle's precision
+void collide_any(irbc_handle* h, uint64_t epoch, cudaStream_t st) {
+  if (h->fp32) launch_collide_f(h->dp, h->sf, h->s, h->c, h->m, epoch, st);
+  else launch_collide(h->dp, h->s, h->c, h->m, epoch, st);
+}
+void stream_any(irbc_handle* h, int buf, cudaStream_t st) {
+  if (h->fp32) fast_stream_f(h->dp, h->sf, h->c, h->fb, buf, st);
+  else fast_stream(h->dp, h->s, h->c, h->fb, buf, st);
+}
+
 // profiling: a pair of events around a launch group of a category
 enum { PROF_STREAM = 0, PROF_COLLIDE = 1, PROF_MEMBRANE = 2 };
 cudaEvent_t next_event(irbc_handle* h) {
@@ -445,7 +458,8 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   auto A = [&](cudaError_t err) { if (err != cudaSuccess && rc == 0) rc = IRBC_ERR_CUDA; };
   for (double** q : {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.x2, &s.y2, &s.z2, &s.vx2, &s.vy2, &s.vz2})
     A(dalloc(q, s.n));
-  for (int** q : {&s.id, &s.indio, &s.pid, &s.id2, &s.indio2, &s.pid2, &s.key, &s.slot}) A(dalloc(q, s.n));
+  for (int** q : {&s.id, &s.indio, &s.pid, &s.id2, &s.indio2, &s.pid2, &s.key, &s.slot, &s.perm})
+    A(dalloc(q, s.n));
   for (int** q : {&c.cnt, &c.ncm, &c.wrank, &c.mrank, &c.lcnt}) A(dalloc(q, c.n));
   A(dalloc(&c.start, c.n + 1));
   A(dalloc(&c.lstart, c.n + 1));
@@ -464,6 +478,14 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   A(dalloc(&h->obs, 64 + 4096));
   A(dalloc(&h->fb.queue, s.n));
   A(dalloc(&h->fb.qn, 4));
+  if (p->precision == IRBC_FP32) {
+    h->fp32 = true;
+    h->sf.n = s.n;
+    for (float4** q : {&h->sf.pos, &h->sf.vel, &h->sf.pos2, &h->sf.vel2}) A(dalloc(q, s.n));
+    A(dalloc(&h->sf.pid, s.n));
+    A(dalloc(&h->sf.pid2, s.n));
+    A(dalloc(&c.parf, c.n * 8));
+  }
   if (rc) { irbc_destroy(h); return rc; }
   cudaMemsetAsync(c.lstart, 0, sizeof(int) * (c.n + 1), h->st);
   cudaMemsetAsync(h->m.ligi, 0, sizeof(int) * h->dp.nlig, h->st);
@@ -485,6 +507,8 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   if (h->st2) cudaStreamSynchronize(h->st2);
   free_fast(h->fb);
   dfree(h->fb.queue); dfree(h->fb.qn);
+  for (float4** q : {&h->sf.pos, &h->sf.vel, &h->sf.pos2, &h->sf.vel2}) dfree(*q);
+  dfree(h->sf.pid); dfree(h->sf.pid2); dfree(h->c.parf);
   for (cudaEvent_t e : {h->ev_snap, h->ev_mem, h->ev_coll, h->ev_str[0], h->ev_str[1]})
     if (e) cudaEventDestroy(e);
   if (h->st2) cudaStreamDestroy(h->st2);
@@ -492,7 +516,7 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   Cells& c = h->c;
   for (double** q : {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.x2, &s.y2, &s.z2, &s.vx2, &s.vy2, &s.vz2})
     dfree(*q);
-  for (int** q : {&s.id, &s.indio, &s.pid, &s.id2, &s.indio2, &s.pid2, &s.key, &s.slot}) dfree(*q);
+  for (int** q : {&s.id, &s.indio, &s.pid, &s.id2, &s.indio2, &s.pid2, &s.key, &s.slot, &s.perm}) dfree(*q);
   for (int** q : {&c.cnt, &c.ncm, &c.wrank, &c.mrank, &c.lcnt, &c.start, &c.lstart, &c.lstart2, &c.totals,
                   &c.scan_part, &c.lidx, &c.lidx2})
     dfree(*q);
@@ -685,6 +709,7 @@ extern "C" int irbc_init(irbc_handle* h, const double* V, int32_t nv, const int3
   }
   if (up(h, m.knob, knob)) return IRBC_ERR_CUDA;
   h->step = 0; h->colsteps = -1; h->upd = 0; h->filecc = 0; h->filec = 0; h->bbi = 0;
+  if (h->fp32) f32_from_f64(h->s, h->sf, h->st);
   CK(cudaStreamSynchronize(h->st));
   CK(cudaGetLastError());
   return 0;
@@ -751,6 +776,7 @@ extern "C" int irbc_set_state(irbc_handle* h, const irbc_view* v) {
         up(h, s.vy, v->svy, n) || up(h, s.vz, v->svz, n) || up(h, s.pid, v->spid, n) ||
         up(h, s.indio, v->sindio, n) || up(h, s.id, id))
       return IRBC_ERR_CUDA;
+    if (h->fp32) f32_from_f64(h->s, h->sf, h->st);
     CK(cudaStreamSynchronize(h->st));
   }
   const int nv = m.nv;
@@ -803,6 +829,7 @@ extern "C" int irbc_get_state(irbc_handle* h, irbc_view* v) {
   Solvent& s = h->s;
   Membrane& m = h->m;
   v->ns = s.n; v->nv = m.nv; v->ncell = h->dp.ncell; v->nlig = h->dp.nlig;
+  if (h->fp32 && v->sx) f32_to_f64(h->sf, h->s, h->st);
   CK(cudaStreamSynchronize(h->st));
   const int64_t n = s.n;
   if (v->sx && n) {
@@ -868,7 +895,7 @@ extern "C" int irbc_get_state(irbc_handle* h, irbc_view* v) {
 extern "C" int irbc_collide(irbc_handle* h, int64_t epoch) {
   if (!h) return IRBC_ERR_ARG;
   if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
-  launch_collide(h->dp, h->s, h->c, h->m, (uint64_t)epoch, h->st);
+  collide_any(h, (uint64_t)epoch, h->st);
   g_launches += 10;
   CK(cudaGetLastError());
   return 0;
@@ -876,7 +903,7 @@ extern "C" int irbc_collide(irbc_handle* h, int64_t epoch) {
 extern "C" int irbc_stream(irbc_handle* h) {
   if (!h || !h->have_mesh) return IRBC_ERR_ARG;
   fast_snap_prep(h->dp, h->m, h->fb, 0, h->st);
-  fast_stream(h->dp, h->s, h->c, h->fb, 0, h->st);
+  stream_any(h, 0, h->st);
   h->snap_ready = false;
   g_launches += 4;
   CK(cudaGetLastError());
@@ -922,7 +949,7 @@ extern "C" int irbc_step_part1(irbc_handle* h) {
   if (s > 0) h->filecc += 1;
   if (h->colsteps == h->csteps) {
     ProfScope ps(h, PROF_COLLIDE);
-    launch_collide(h->dp, h->s, h->c, h->m, (uint64_t)s, h->st);
+    collide_any(h, (uint64_t)s, h->st);
     g_launches += 10;
     h->colsteps = 0;
   }
@@ -939,7 +966,7 @@ extern "C" int irbc_step_part1(irbc_handle* h) {
   }
   {
     ProfScope ps(h, PROF_STREAM);
-    fast_stream(h->dp, h->s, h->c, h->fb, buf, h->st);
+    stream_any(h, buf, h->st);
   }
   {
     ProfScope ps(h, PROF_MEMBRANE);
@@ -991,7 +1018,7 @@ extern "C" int irbc_step(irbc_handle* h, int64_t n) {
       CK(cudaStreamWaitEvent(ms, h->ev_mem, 0));
       {
         ProfScope ps(h, PROF_COLLIDE, ms);
-        launch_collide(h->dp, h->s, h->c, h->m, (uint64_t)s, ms);
+        collide_any(h, (uint64_t)s, ms);
       }
       g_launches += 10;
       h->colsteps = 0;
@@ -1020,7 +1047,7 @@ extern "C" int irbc_step(irbc_handle* h, int64_t n) {
     CK(cudaStreamWaitEvent(ms, h->ev_snap, 0));
     {
       ProfScope ps(h, PROF_STREAM, ms);
-      fast_stream(h->dp, h->s, h->c, h->fb, buf, ms);
+      stream_any(h, buf, ms);
     }
     g_launches += 2;
     CK(cudaEventRecord(h->ev_str[buf], ms));
@@ -1115,6 +1142,7 @@ extern "C" int irbc_write_stl(irbc_handle* h, const char* path) {
 
 extern "C" int irbc_observables(irbc_handle* h, double* out, int32_t nout) {
   if (!h || !out || nout <= 0) return IRBC_ERR_ARG;
+  if (h->fp32) f32_to_f64(h->sf, h->s, h->st);
   launch_observables(h->dp, h->s, h->m, h->obs, nullptr, 0, h->st);
   g_launches += 2;
   double buf[16] = {0};
@@ -1126,6 +1154,7 @@ extern "C" int irbc_observables(irbc_handle* h, double* out, int32_t nout) {
 
 extern "C" int irbc_velocity_profile(irbc_handle* h, double* out, int32_t nbins) {
   if (!h || !out || nbins <= 0 || nbins > 2048) return IRBC_ERR_ARG;
+  if (h->fp32) f32_to_f64(h->sf, h->s, h->st);
   launch_observables(h->dp, h->s, h->m, h->obs, h->obs + 64, nbins, h->st);
   g_launches += 3;
   std::vector<double> buf(2 * nbins);

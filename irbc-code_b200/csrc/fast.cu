@@ -530,12 +530,13 @@ __device__ __forceinline__ bool in_liglist_f(const DevParams& p, int cell, doubl
 // half-kick (:487-496) with the snapshot and triangle prep for its
 // streaming.  Each thread owns a contiguous run of vertices so that a block
 // scan of per-thread counts keeps vertex order in the compacted lists.
-constexpr int kTailT = 1024, kTailList = 1024, kTailDraws = 2048;
+constexpr int kTailT = 1024, kTailList = 1024, kTailDraws = 4096;
 __global__ void __launch_bounds__(kTailT) k_mem_tail(DevParams p, Membrane m, uint64_t epoch, int next_kick,
                                                     TriPre* pre, Snap sn) {
   __shared__ int s_a[kTailT], s_w[kTailT], s_d[kTailT];
-  __shared__ int s_list[kTailList], s_wlist[kTailList], s_doff[kTailList];
-  __shared__ double s_u[kTailDraws];
+  __shared__ int s_wlist[kTailList];
+  __shared__ int s_evv[kTailDraws];        // vertex of an event at draw k, or -1
+  __shared__ short s_evr[kTailDraws];      // its pair index, -1 for unbinding
   __shared__ int s_tot[3];
   const int T = blockDim.x, tid = threadIdx.x;
   MemScalars* sc = m.sc;
@@ -613,28 +614,41 @@ __global__ void __launch_bounds__(kTailT) k_mem_tail(DevParams p, Membrane m, ui
   }
   __syncthreads();
   const bool fits = s_tot[0] <= kTailList && s_tot[1] <= kTailList && s_tot[2] <= kTailDraws;
+  // Draw k decides something only if it passes its probability test (an
+  // "event": poff > u for a bonded vertex, pon > u for a candidate pair);
+  // all other draws leave the state unchanged.  Events are marked by draw
+  // index in parallel; bond_dynamics then applies just the events, in draw
+  // order, which gives the reference's serial result.
   if (fits) {
-    int oa = s_a[tid], ow = s_w[tid], od = s_d[tid];
+    int ow = s_w[tid], od = s_d[tid];
     for (int ii = v0; ii < v1; ++ii) {
       const bool bonded = m.bondi[ii] == 1;
       const bool elig = !bonded && (m.z[ii] < p.dthr) && (m.knob[ii] == 1);
-      if (bonded || elig) {
-        s_list[oa] = ii;
-        s_doff[oa] = od;
-        int n = bonded ? 1 : m.npair[ii];
-        for (int r = 0; r < n; ++r) s_u[od + r] = draw_uniform(p.seed, STREAM_BOND, epoch, (uint64_t)(od + r));
-        oa += 1; od += n;
+      if (bonded) {
+        double u = draw_uniform(p.seed, STREAM_BOND, epoch, (uint64_t)od);
+        s_evv[od] = (m.poff[ii] > u) ? ii : -1;
+        s_evr[od] = -1;
+        od += 1;
+      } else if (elig) {
+        const int n = m.npair[ii];
+        const double pon = m.pon[ii];
+        for (int r = 0; r < n; ++r) {
+          double u = draw_uniform(p.seed, STREAM_BOND, epoch, (uint64_t)(od + r));
+          s_evv[od + r] = (pon > u) ? ii : -1;
+          s_evr[od + r] = r;
+        }
+        od += n;
       }
       double X[3];
       if (wca_f(p, m, sc, ii, X)) s_wlist[ow++] = ii;
     }
   }
   __syncthreads();
-  if (tid == 0) {
-    const int na_t = s_tot[0], nw_t = s_tot[1];
+  if (tid == 32) {
+    // pfdt's parasite sum in vertex order, then the parasite kick
     double fx = 0, fy = 0, fz = 0;
     if (fits) {
-      for (int q = 0; q < nw_t; ++q) {
+      for (int q = 0; q < s_tot[1]; ++q) {
         double X[3];
         wca_f(p, m, sc, s_wlist[q], X);
         fx += X[0]; fy += X[1]; fz += X[2];
@@ -646,13 +660,35 @@ __global__ void __launch_bounds__(kTailT) k_mem_tail(DevParams p, Membrane m, ui
       }
     }
     sc->parafdt[0] += fx; sc->parafdt[1] += fy; sc->parafdt[2] += fz;
+    for (int c = 0; c < 3; ++c) sc->paraV[c] += ((sc->paraft[c] + sc->parafdt[c]) * p.dtmd / (2.0 * p.PRmass));
+    for (int c = 0; c < 3; ++c) { sc->paraft[c] = sc->parafdt[c]; sc->parafdt[c] = 0.0; }
+  }
+  if (fits && tid < 32) {
+    const int nd = s_tot[2];
+    for (int k0 = 0; k0 < nd; k0 += 32) {
+      const int k = k0 + tid;
+      unsigned ev = __ballot_sync(0xffffffffu, k < nd && s_evv[k] >= 0);
+      if (tid == 0) {
+        while (ev) {
+          const int b = __ffs(ev) - 1;
+          ev &= ev - 1;
+          const int ii = s_evv[k0 + b], r = s_evr[k0 + b];
+          if (r < 0) {  // unbinding (maincode.cpp:30-35)
+            int jj = m.bondl[ii];
+            m.bondi[ii] = 0; m.bondl[ii] = p.randno; m.ligi[jj] = 0;
+          } else {      // binding attempt on a free ligand (:45-50)
+            int j = m.pair_j[(int64_t)ii * kMaxPairs + r];
+            if (m.ligi[j] == 0) { m.ligi[j] = 1; m.bondi[ii] = 1; m.bondl[ii] = j; }
+          }
+        }
+      }
+    }
+  } else if (!fits && tid == 0) {
+    // lists larger than the shared buffers: the plain serial walk
     uint64_t k = 0;
-    const int nlist = fits ? na_t : p.nv;
-    for (int q = 0; q < nlist; ++q) {
-      const int ii = fits ? s_list[q] : q;
+    for (int ii = 0; ii < p.nv; ++ii) {
       if (m.bondi[ii] == 1) {
-        double randoff = fits ? s_u[k] : draw_uniform(p.seed, STREAM_BOND, epoch, k);
-        ++k;
+        double randoff = draw_uniform(p.seed, STREAM_BOND, epoch, k++);
         int jj = m.bondl[ii];
         if (m.poff[ii] > randoff) { m.bondi[ii] = 0; m.bondl[ii] = p.randno; m.ligi[jj] = 0; }
       } else if ((m.z[ii] < p.dthr) && (m.bondi[ii] == 0) && (m.knob[ii] == 1)) {
@@ -660,14 +696,11 @@ __global__ void __launch_bounds__(kTailT) k_mem_tail(DevParams p, Membrane m, ui
         for (int r = 0; r < n; ++r) {
           int j = m.pair_j[(int64_t)ii * kMaxPairs + r];
           double pon = m.pon[ii];
-          double randon = fits ? s_u[k] : draw_uniform(p.seed, STREAM_BOND, epoch, k);
-          ++k;
+          double randon = draw_uniform(p.seed, STREAM_BOND, epoch, k++);
           if ((pon > randon) && (m.ligi[j] == 0)) { m.ligi[j] = 1; m.bondi[ii] = 1; m.bondl[ii] = j; }
         }
       }
     }
-    for (int c = 0; c < 3; ++c) sc->paraV[c] += ((sc->paraft[c] + sc->parafdt[c]) * p.dtmd / (2.0 * p.PRmass));
-    for (int c = 0; c < 3; ++c) { sc->paraft[c] = sc->parafdt[c]; sc->parafdt[c] = 0.0; }
   }
   if (!next_kick) return;
   __syncthreads();

@@ -63,43 +63,54 @@ __global__ void k_count_f(DevParams p, SolventF f, int* cnt, int* key, int* slot
   slot[i] = base + rank;
 }
 
-__global__ void k_scatter_f(SolventF f, const int* key, const int* slot, const int* start) {
+__global__ void k_perm_f(const int* __restrict__ key, const int* __restrict__ slot, const int* __restrict__ start,
+                         int64_t n, int* __restrict__ perm) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= f.n) return;
-  int c = key[i];
-  int64_t d = (int64_t)start[c] + slot[i];
-  f.pos2[d] = f.pos[i];
-  f.vel2[d] = f.vel[i];
-  f.pid2[d] = c;
+  if (i >= n) return;
+  perm[(int64_t)start[key[i]] + slot[i]] = (int)i;
+}
+
+// physical re-sort by collision cell every kResortEvery collisions
+__global__ void k_gather_f(SolventF f, const int* __restrict__ perm) {
+  int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= f.n) return;
+  const int i = perm[j];
+  f.pos2[j] = f.pos[i];
+  f.vel2[j] = f.vel[i];
+  f.pid2[j] = f.pid[i];
 }
 
 // per-cell statistics, one thread per cell, sums in double in reference
 // particle order (CollisionStep, Src/solfuncs.cpp:164-318)
 constexpr int kMaxSegF = 48;
-__global__ void k_cells_f(DevParams p, SolventF f, Cells cl, Membrane m, uint64_t epoch) {
+__global__ void k_cells_f(DevParams p, SolventF f, const int* __restrict__ perm, Cells cl, Membrane m,
+                          uint64_t epoch) {
   int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= p.ncell) return;
   const int64_t s0 = cl.start[c];
   const int n = cl.start[c + 1] - (int)s0;
-  int ord[kMaxSegF];
+  const int* __restrict__ PP = perm + s0;
+  int ord[kMaxSegF], oid[kMaxSegF];
   const bool small = n <= kMaxSegF;
   if (small) {
     for (int q = 0; q < n; ++q) {
-      int idq = __float_as_int(f.vel[s0 + q].w);
+      int pq = PP[q];
+      int idq = __float_as_int(f.vel[pq].w);
       int r = q;
-      while (r > 0 && __float_as_int(f.vel[s0 + ord[r - 1]].w) > idq) { ord[r] = ord[r - 1]; --r; }
-      ord[r] = q;
+      while (r > 0 && oid[r - 1] > idq) { ord[r] = ord[r - 1]; oid[r] = oid[r - 1]; --r; }
+      ord[r] = pq;
+      oid[r] = idq;
     }
   }
   auto nth = [&](int q) -> int64_t {
-    if (small) return s0 + ord[q];
+    if (small) return ord[q];
     int last = -1;
-    int64_t at = s0;
+    int64_t at = PP[0];
     for (int t = 0; t <= q; ++t) {
       int best = 0x7fffffff;
       for (int u = 0; u < n; ++u) {
-        int v = __float_as_int(f.vel[s0 + u].w);
-        if (v > last && v < best) { best = v; at = s0 + u; }
+        int v = __float_as_int(f.vel[PP[u]].w);
+        if (v > last && v < best) { best = v; at = PP[u]; }
       }
       last = best;
     }
@@ -245,10 +256,14 @@ void launch_collide_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, Mem
   launch_ghost_flags(p, c, m, st);
   launch_scan3(c.cnt, c.wrank, c.mrank, c.start, c.wrank, c.mrank, c.totals, c.n, c.scan_part, st);
   cudaMemcpyAsync(c.start + c.n, c.totals + 0, sizeof(int), cudaMemcpyDeviceToDevice, st);
-  if (f.n) k_scatter_f<<<nbf(f.n, 256), 256, 0, st>>>(f, s.key, s.slot, c.start);
-  std::swap(f.pos, f.pos2); std::swap(f.vel, f.vel2); std::swap(f.pid, f.pid2);
-  k_cells_f<<<nbf(c.n, 128), 128, 0, st>>>(p, f, c, m, epoch);
+  if (f.n) k_perm_f<<<nbf(f.n, 256), 256, 0, st>>>(s.key, s.slot, c.start, f.n, s.perm);
+  std::swap(f.pid, s.key);  // pid = cell of this collision, in place
+  k_cells_f<<<nbf(c.n, 128), 128, 0, st>>>(p, f, s.perm, c, m, epoch);
   if (f.n) k_rotate_f<<<nbf(f.n, 256), 256, 0, st>>>(f, c.parf, (float)p.cosalpha, (float)p.sinalpha);
+  if (f.n && (++s.ncoll % kResortEvery) == 0) {
+    k_gather_f<<<nbf(f.n, 256), 256, 0, st>>>(f, s.perm);
+    std::swap(f.pos, f.pos2); std::swap(f.vel, f.vel2); std::swap(f.pid, f.pid2);
+  }
 }
 
 // ---- streaming ------------------------------------------------------------------

@@ -328,14 +328,23 @@ __global__ void k_ghost_flags(DevParams p, const int* cnt, const int* ncm, const
   mflag[c] = mem;
 }
 
-__global__ void k_scatter(Solvent s, const int* start) {
+// counting sort of particle indices: perm[start[cell] + slot] = i
+__global__ void k_perm(const int* __restrict__ key, const int* __restrict__ slot, const int* __restrict__ start,
+                       int64_t n, int* __restrict__ perm) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.n) return;
-  int c = s.key[i];
-  int64_t d = (int64_t)start[c] + s.slot[i];
-  s.x2[d] = s.x[i]; s.y2[d] = s.y[i]; s.z2[d] = s.z[i];
-  s.vx2[d] = s.vx[i]; s.vy2[d] = s.vy[i]; s.vz2[d] = s.vz[i];
-  s.id2[d] = s.id[i]; s.indio2[d] = s.indio[i]; s.pid2[d] = c;
+  if (i >= n) return;
+  perm[(int64_t)start[key[i]] + slot[i]] = (int)i;
+}
+
+// physical re-sort by collision cell (every few collisions, to keep the
+// particles of a cell close in memory): coalesced writes, gathered reads
+__global__ void k_gather(Solvent s) {
+  int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= s.n) return;
+  const int i = s.perm[j];
+  s.x2[j] = s.x[i]; s.y2[j] = s.y[i]; s.z2[j] = s.z[i];
+  s.vx2[j] = s.vx[i]; s.vy2[j] = s.vy[i]; s.vz2[j] = s.vz[i];
+  s.id2[j] = s.id[i]; s.indio2[j] = s.indio[i]; s.pid2[j] = s.pid[i];
 }
 
 __device__ __forceinline__ double gauss(const DevParams& p, uint64_t epoch, uint64_t k, double m, double sd) {
@@ -365,27 +374,31 @@ __global__ void k_cells(DevParams p, Solvent s, Cells cl, Membrane m, uint64_t e
   if (c >= p.ncell) return;
   const int64_t s0 = cl.start[c];
   const int n = cl.start[c + 1] - (int)s0;
-  // order of the cell's particles by reference index (Cells[].sol order)
-  int ord[kMaxSeg];
+  // the cell's particles are perm[s0 .. s0+n); order them by reference
+  // index (the order of Cells[].sol)
+  const int* __restrict__ PP = s.perm + s0;
+  int ord[kMaxSeg], oid[kMaxSeg];
   const bool small = n <= kMaxSeg;
   if (small) {
     for (int q = 0; q < n; ++q) {
-      int idq = s.id[s0 + q];
+      int pq = PP[q];
+      int idq = s.id[pq];
       int r = q;
-      while (r > 0 && s.id[s0 + ord[r - 1]] > idq) { ord[r] = ord[r - 1]; --r; }
-      ord[r] = q;
+      while (r > 0 && oid[r - 1] > idq) { ord[r] = ord[r - 1]; oid[r] = oid[r - 1]; --r; }
+      ord[r] = pq;
+      oid[r] = idq;
     }
   }
   auto nth = [&](int q) -> int64_t {
-    if (small) return s0 + ord[q];
+    if (small) return ord[q];
     // large cell: q-th smallest id by selection (rare)
     int last = -1;
-    int64_t at = s0;
+    int64_t at = PP[0];
     for (int t = 0; t <= q; ++t) {
       int best = 0x7fffffff;
       for (int u = 0; u < n; ++u) {
-        int v = s.id[s0 + u];
-        if (v > last && v < best) { best = v; at = s0 + u; }
+        int v = s.id[PP[u]];
+        if (v > last && v < best) { best = v; at = PP[u]; }
       }
       last = best;
     }
@@ -543,24 +556,21 @@ void launch_collide(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint6
                     cudaStream_t st) {
   cudaMemsetAsync(c.cnt, 0, sizeof(int) * c.n, st);
   cudaMemsetAsync(c.ncm, 0, sizeof(int) * c.n, st);
-  int n2 = 1;
-  while (n2 < p.nv) n2 <<= 1;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
-    attr_set = true;
-  }
-  k_vbin<<<1, 1024, sizeof(uint64_t) * n2, st>>>(p, m, c.ncm, epoch);
+  launch_vbin(p, m, c, epoch, st);
   if (s.n) k_count<<<nblk(s.n, 256), 256, 0, st>>>(p, s, c.cnt, epoch);
   // wrank/mrank hold the flags first, then their exclusive scans
   k_ghost_flags<<<nblk(c.n, 256), 256, 0, st>>>(p, c.cnt, c.ncm, m.sc, c.wrank, c.mrank);
   launch_scan3(c.cnt, c.wrank, c.mrank, c.start, c.wrank, c.mrank, c.totals, c.n, c.scan_part, st);
   // start[C] = Ns
   cudaMemcpyAsync(c.start + c.n, c.totals + 0, sizeof(int), cudaMemcpyDeviceToDevice, st);
-  if (s.n) k_scatter<<<nblk(s.n, 256), 256, 0, st>>>(s, c.start);
-  swap_solvent(s);
+  if (s.n) k_perm<<<nblk(s.n, 256), 256, 0, st>>>(s.key, s.slot, c.start, s.n, s.perm);
+  std::swap(s.pid, s.key);  // pid = cell of this collision, in place
   k_cells<<<nblk(c.n, 128), 128, 0, st>>>(p, s, c, m, epoch);
   if (s.n) k_rotate<<<nblk(s.n, 256), 256, 0, st>>>(p, s, c.par);
+  if (s.n && (++s.ncoll % kResortEvery) == 0) {
+    k_gather<<<nblk(s.n, 256), 256, 0, st>>>(s);
+    swap_solvent(s);
+  }
 }
 
 // ============================================================== stream =====

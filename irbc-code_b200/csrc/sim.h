@@ -21,7 +21,13 @@ struct Solvent {
   double *x2 = nullptr, *y2 = nullptr, *z2 = nullptr, *vx2 = nullptr, *vy2 = nullptr, *vz2 = nullptr;
   int *id2 = nullptr, *indio2 = nullptr, *pid2 = nullptr;
   int *key = nullptr, *slot = nullptr;
+  int *perm = nullptr;          // particle indices grouped by collision cell
+  int64_t ncoll = 0;            // collisions so far (physical re-sort cadence)
 };
+
+// every kResortEvery-th collision also re-sorts the particle arrays
+// physically by cell; in between the cells read their particles through perm
+constexpr int kResortEvery = 16;
 
 struct Cells {
   int64_t n = 0;
