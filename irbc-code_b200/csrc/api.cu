@@ -270,7 +270,7 @@ void free_fast(FastBufs& f) {
       dfree(*q);
     dfree(f.pre[b]);
   }
-  dfree(f.slot); dfree(f.gstart); dfree(f.gidx);
+  dfree(f.slot); dfree(f.gstart); dfree(f.gidx); dfree(f.vd); dfree(f.vw); dfree(f.vX);
 }
 
 // per-vertex force slots in the order force_calculate_dt adds the terms:
@@ -338,6 +338,9 @@ int upload_mesh(irbc_handle* h, const HostMesh& M) {
     CK(dalloc(&f.slot, 3 * (int64_t)(8 * M.ne + 9 * M.nt)));
     CK(dalloc(&f.gstart, M.nv + 1));
     CK(dalloc(&f.gidx, (int64_t)gidx.size()));
+    CK(dalloc(&f.vd, M.nv));
+    CK(dalloc(&f.vw, M.nv));
+    CK(dalloc(&f.vX, 3 * (int64_t)M.nv));
     if (up(h, f.gstart, gstart) || up(h, f.gidx, gidx)) return IRBC_ERR_CUDA;
   }
   if (up(h, m.e1, M.e1) || up(h, m.e2, M.e2) || up(h, m.es1, M.es1) || up(h, m.es2, M.es2) ||
@@ -358,9 +361,13 @@ int upload_mesh(irbc_handle* h, const HostMesh& M) {
 int64_t launches_in(const irbc_handle* h) { return g_launches.load() - h->launches0; }
 
 // the solvent kernels of the handle's precision
-void collide_any(irbc_handle* h, uint64_t epoch, cudaStream_t st) {
+// returns the number of kernels launched: vbin, count, ghost flags, three
+// scan kernels, perm, cells, rotate, and the physical re-sort when due
+int collide_any(irbc_handle* h, uint64_t epoch, cudaStream_t st) {
+  const int64_t before = h->s.ncoll;
   if (h->fp32) launch_collide_f(h->dp, h->sf, h->s, h->c, h->m, epoch, st);
   else launch_collide(h->dp, h->s, h->c, h->m, epoch, st);
+  return 9 + ((h->s.ncoll != before && h->s.ncoll % kResortEvery == 0) ? 1 : 0);
 }
 void stream_any(irbc_handle* h, int buf, cudaStream_t st) {
   if (h->fp32) fast_stream_f(h->dp, h->sf, h->c, h->fb, buf, st);
@@ -895,8 +902,7 @@ extern "C" int irbc_get_state(irbc_handle* h, irbc_view* v) {
 extern "C" int irbc_collide(irbc_handle* h, int64_t epoch) {
   if (!h) return IRBC_ERR_ARG;
   if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
-  collide_any(h, (uint64_t)epoch, h->st);
-  g_launches += 10;
+  g_launches += collide_any(h, (uint64_t)epoch, h->st);
   CK(cudaGetLastError());
   return 0;
 }
@@ -949,8 +955,7 @@ extern "C" int irbc_step_part1(irbc_handle* h) {
   if (s > 0) h->filecc += 1;
   if (h->colsteps == h->csteps) {
     ProfScope ps(h, PROF_COLLIDE);
-    collide_any(h, (uint64_t)s, h->st);
-    g_launches += 10;
+    g_launches += collide_any(h, (uint64_t)s, h->st);
     h->colsteps = 0;
   }
   const int buf = (int)(s & 1);
@@ -970,9 +975,8 @@ extern "C" int irbc_step_part1(irbc_handle* h) {
   }
   {
     ProfScope ps(h, PROF_MEMBRANE);
-    fast_drift_va(h->dp, h->m, h->st);
+    g_launches += 2 + fast_drift_va(h->dp, h->m, h->st, true);  // + streaming (2)
   }
-  g_launches += 3;
   h->snap_ready = false;
   CK(cudaGetLastError());
   return 0;
@@ -985,9 +989,8 @@ extern "C" int irbc_step_part2(irbc_handle* h) {
   const int64_t s = h->step;
   {
     ProfScope ps(h, PROF_MEMBRANE);
-    fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)s, 0, (int)((s + 1) & 1), h->st);
+    g_launches += fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)s, 0, (int)((s + 1) & 1), h->st, false);
   }
-  g_launches += 3;
   if (h->filecc == h->P.out_every) { h->filec += 1; h->filecc = 0; }
   h->step = s + 1;
   CK(cudaGetLastError());
@@ -1018,9 +1021,8 @@ extern "C" int irbc_step(irbc_handle* h, int64_t n) {
       CK(cudaStreamWaitEvent(ms, h->ev_mem, 0));
       {
         ProfScope ps(h, PROF_COLLIDE, ms);
-        collide_any(h, (uint64_t)s, ms);
+        g_launches += collide_any(h, (uint64_t)s, ms);
       }
-      g_launches += 10;
       h->colsteps = 0;
       CK(cudaEventRecord(h->ev_coll, ms));
       CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
@@ -1059,10 +1061,9 @@ extern "C" int irbc_step(irbc_handle* h, int64_t n) {
     CK(cudaStreamWaitEvent(ss, h->ev_str[buf ^ 1], 0));
     {
       ProfScope ps(h, PROF_MEMBRANE, ss);
-      fast_drift_va(h->dp, h->m, ss);
-      fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)s, next_kick, buf ^ 1, ss);
+      g_launches += fast_drift_va(h->dp, h->m, ss, false);
+      g_launches += fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)s, next_kick, buf ^ 1, ss, true);
     }
-    g_launches += 4;
     CK(cudaEventRecord(h->ev_mem, ss));
     h->snap_ready = next_kick != 0;
     if (h->filecc == p.out_every) { h->filec += 1; h->filecc = 0; }

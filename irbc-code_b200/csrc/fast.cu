@@ -349,8 +349,14 @@ __global__ void __launch_bounds__(1024) k_drift_va(DevParams p, Membrane m) {
 // force terms of every edge (WLC + POW), triangle (local/global area and
 // volume) and bending dihedral, stored per term in slots so the per-vertex
 // gather can add them in the reference's order (Src/memfuncs.cpp:233-427)
+__device__ void force_item(const DevParams& p, const Membrane& m, double* __restrict__ slot, int t);
+
 __global__ void __launch_bounds__(256) k_force_items(DevParams p, Membrane m, double* __restrict__ slot) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  force_item(p, m, slot, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// item t of [edges | triangles | dihedrals]: its force terms into the slots
+__device__ void force_item(const DevParams& p, const Membrane& m, double* __restrict__ slot, int t) {
   const MemScalars* sc = m.sc;
   if (t < p.ne) {
     int i = t;
@@ -530,7 +536,7 @@ __device__ __forceinline__ bool in_liglist_f(const DevParams& p, int cell, doubl
 // half-kick (:487-496) with the snapshot and triangle prep for its
 // streaming.  Each thread owns a contiguous run of vertices so that a block
 // scan of per-thread counts keeps vertex order in the compacted lists.
-constexpr int kTailT = 1024, kTailList = 1024, kTailDraws = 4096;
+constexpr int kTailT = 1024, kTailList = 1024, kTailDraws = 4096, kWcaList = 512;
 __global__ void __launch_bounds__(kTailT) k_mem_tail(DevParams p, Membrane m, uint64_t epoch, int next_kick,
                                                     TriPre* pre, Snap sn) {
   __shared__ int s_a[kTailT], s_w[kTailT], s_d[kTailT];
@@ -717,6 +723,350 @@ __global__ void __launch_bounds__(kTailT) k_mem_tail(DevParams p, Membrane m, ui
   for (int j = tid; j < p.nt; j += T) tri_prep_one(p, m, j, m.vx, m.vy, m.vz, pre);
 }
 
+// ================================================= membrane step, wide form ===
+// The same phases as k_drift_va / k_force_gather / k_mem_tail, spread over
+// many SMs: per-vertex and per-triangle work in wide kernels, the ordered
+// reductions (Sarea, Volume, the parasite sum, bond_dynamics) in one CTA
+// reading shared memory.
+
+// drift + image counters (maincode.cpp:566-574) and parasite drift (:576-598)
+__global__ void k_m_drift(DevParams p, Membrane m) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < p.nv) {
+    double x = m.x[i], y = m.y[i], z = m.z[i];
+    x += (m.vx[i] * p.dtmd);
+    y += (m.vy[i] * p.dtmd);
+    z += (m.vz[i] * p.dtmd);
+    if (x > p.Lx) { x -= p.Lx; m.ix[i] += 1; }
+    if (x < 0) { x += p.Lx; m.ix[i] -= 1; }
+    if (y > p.Ly) { y -= p.Ly; m.iy[i] += 1; }
+    if (y < 0) { y += p.Ly; m.iy[i] -= 1; }
+    m.x[i] = x; m.y[i] = y; m.z[i] = z;
+  }
+  if (i == 0) {
+    MemScalars* sc = m.sc;
+    for (int k = 0; k < 3; ++k)
+      sc->para[k] += (sc->paraV[k] * p.dtmd) + (sc->paraft[k] * p.dtmd * p.dtmd / (2.0 * p.PRmass));
+    if (sc->para[0] > p.Lx) { sc->para[0] -= p.Lx; sc->paradx += 1; }
+    else if (sc->para[0] < 0) { sc->para[0] += p.Lx; sc->paradx -= 1; }
+    if (sc->para[1] > p.Ly) { sc->para[1] -= p.Ly; sc->parady += 1; }
+    else if (sc->para[1] < 0) { sc->para[1] += p.Ly; sc->parady -= 1; }
+  }
+}
+
+// Areatri / Voltri terms per triangle (Src/memfuncs.cpp:124-157)
+__global__ void k_m_av(DevParams p, Membrane m) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nt) return;
+  int l1 = m.t1[i], l2 = m.t2[i], l3 = m.t3[i];
+  double A[3], B[3], eta[3], Cn[3];
+  A[0] = UXm(l2) - UXm(l1); A[1] = UYm(l2) - UYm(l1); A[2] = m.z[l2] - m.z[l1];
+  B[0] = UXm(l3) - UXm(l1); B[1] = UYm(l3) - UYm(l1); B[2] = m.z[l3] - m.z[l1];
+  cp(A, B, eta);
+  m.area[i] = 0.5 * sqrt(eta[0] * eta[0] + eta[1] * eta[1] + eta[2] * eta[2]);
+  Cn[0] = (UXm(l1) + UXm(l2) + UXm(l3)) / 3.0;
+  Cn[1] = (UYm(l1) + UYm(l2) + UYm(l3)) / 3.0;
+  Cn[2] = (m.z[l1] + m.z[l2] + m.z[l3]) / 3.0;
+  m.vol[i] = (1.0 / 6.0) * ((eta[0] * Cn[0]) + (eta[1] * Cn[1]) + (eta[2] * Cn[2]));
+}
+
+// TotalVA's sums, left to right in triangle order, from shared memory
+constexpr int kSumSmemT = 12288;
+__global__ void __launch_bounds__(1024) k_m_sum(DevParams p, Membrane m) {
+  extern __shared__ double sh[];
+  const bool staged = p.nt <= kSumSmemT;
+  if (staged) {
+    for (int i = threadIdx.x; i < p.nt; i += blockDim.x) { sh[i] = m.area[i]; sh[p.nt + i] = m.vol[i]; }
+    __syncthreads();
+  }
+  const double* a = staged ? sh : m.area;
+  const double* v = staged ? sh + p.nt : m.vol;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+#pragma unroll 16
+    for (int i = 0; i < p.nt; ++i) t += a[i];
+    m.sc->Sarea = t;
+  } else if (threadIdx.x == 32) {
+    double t = 0.0;
+#pragma unroll 16
+    for (int i = 0; i < p.nt; ++i) t += v[i];
+    m.sc->Volume = t;
+  }
+}
+
+// Block 0: TotalVA's two ordered sums (as k_m_sum).  Blocks 1..: the edge
+// and bending terms, which do not depend on Sarea / Volume, so they overlap
+// the sums.  The triangle terms follow in k_force_tri.
+__global__ void __launch_bounds__(1024) k_sum_edges(DevParams p, Membrane m, double* __restrict__ slot, int do_sum) {
+  if (blockIdx.x == 0) {
+    if (!do_sum) return;
+    extern __shared__ double sh[];
+    const bool staged = p.nt <= kSumSmemT;
+    if (staged) {
+      for (int i = threadIdx.x; i < p.nt; i += blockDim.x) { sh[i] = m.area[i]; sh[p.nt + i] = m.vol[i]; }
+      __syncthreads();
+    }
+    const double* a = staged ? sh : m.area;
+    const double* v = staged ? sh + p.nt : m.vol;
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+#pragma unroll 16
+      for (int i = 0; i < p.nt; ++i) t += a[i];
+      m.sc->Sarea = t;
+    } else if (threadIdx.x == 32) {
+      double t = 0.0;
+#pragma unroll 16
+      for (int i = 0; i < p.nt; ++i) t += v[i];
+      m.sc->Volume = t;
+    }
+    return;
+  }
+  const int k = (blockIdx.x - 1) * blockDim.x + threadIdx.x;  // 0 .. 2E
+  if (k < p.ne) force_item(p, m, slot, k);
+  else if (k < 2 * p.ne) force_item(p, m, slot, p.nt + k);  // dihedral k - E
+}
+__global__ void k_force_tri(DevParams p, Membrane m, double* __restrict__ slot) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < p.nt) force_item(p, m, slot, p.ne + k);
+}
+
+// warp per vertex: lanes stage the vertex's force slots in shared memory,
+// lanes 0-2 add them up component-wise in the reference's order, lane 0
+// applies pfdt's -X first and the external forces after (maincode.cpp:603-665)
+constexpr int kGW = 4, kGSlots = 64;
+__global__ void __launch_bounds__(32 * kGW) k_force_gather_w(DevParams p, Membrane m, const double* __restrict__ slot,
+                                                           const int* __restrict__ gstart,
+                                                           const int* __restrict__ gidx) {
+  __shared__ double sh[kGW][kGSlots * 3];
+  __shared__ double ffs[kGW][3];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * kGW + w;
+  if (i >= p.nv) return;
+  const int q0 = gstart[i], q1 = gstart[i + 1];
+  double acc = 0.0;
+  for (int c0 = q0; c0 < q1; c0 += kGSlots) {
+    const int nc = min(kGSlots, q1 - c0);
+    for (int e = lane; e < nc * 3; e += 32) {
+      const int q = e / 3, k = e - 3 * q;
+      sh[w][e] = slot[3 * (int64_t)gidx[c0 + q] + k];
+    }
+    __syncwarp();
+    if (lane < 3)
+      for (int q = 0; q < nc; ++q) acc += sh[w][3 * q + lane];
+    __syncwarp();
+  }
+  if (lane < 3) ffs[w][lane] = acc;
+  __syncwarp();
+  if (lane != 0) return;
+  const MemScalars* sc = m.sc;
+  double f[3] = {m.fx[i], m.fy[i], m.fz[i]};
+  double X[3];
+  if (wca_f(p, m, sc, i, X)) { f[0] -= X[0]; f[1] -= X[1]; f[2] -= X[2]; }
+  f[0] += ffs[w][0]; f[1] += ffs[w][1]; f[2] += ffs[w][2];
+  f[2] += -p.Fg / (double)p.nv;
+  if (m.bondi[i] == 1) {
+    int jj = m.bondl[i];
+    double A[3];
+    A[0] = m.x[i] - m.xlig[jj];
+    A[1] = m.y[i] - m.ylig[jj];
+    A[2] = m.z[i];
+    A[0] -= p.Lx * round(A[0] / p.Lx);
+    A[1] -= p.Ly * round(A[1] / p.Ly);
+    double aa = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+    A[0] /= aa; A[1] /= aa; A[2] /= aa;
+    if (aa > p.el0) {
+      f[0] += -p.ks * (aa - p.el0) * A[0];
+      f[1] += -p.ks * (aa - p.el0) * A[1];
+      f[2] += -p.ks * (aa - p.el0) * A[2];
+    }
+  }
+  double cc = m.z[i];
+  if (cc < 0.5) f[2] += 300.0 * exp(-50.0 * cc);
+  cc = p.Lz - m.z[i];
+  if (cc < 0.5) f[2] -= 300.0 * exp(-50.0 * cc);
+  m.fx[i] = f[0]; m.fy[i] = f[1]; m.fz[i] = f[2];
+}
+
+// per vertex: bond preparation (maincode.cpp:668-723), second half-kick
+// (:727-733), the number of bond draws and the WCA flag for k_tail_b
+__global__ void k_tail_a(DevParams p, Membrane m, int* __restrict__ vd, int* __restrict__ vw,
+                         double* __restrict__ vX) {
+  int ii = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ii >= p.nv) return;
+  double A[3], B[3];
+  int nd = 0;
+  if (m.bondi[ii] == 1) {
+    int p1modx = m.ix[ii], p1mody = m.iy[ii], jj = m.bondl[ii];
+    A[0] = (m.x[ii] + p1modx * p.Lx) - (m.xlig[jj] + p1modx * p.Lx);
+    A[1] = (m.y[ii] + p1mody * p.Ly) - (m.ylig[jj] + p1mody * p.Ly);
+    A[2] = m.z[ii] - 0.0;
+    double xx = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+    if (xx > p.el0) {
+      B[0] = -p.ks * (xx - p.el0) * A[0] / xx;
+      B[1] = -p.ks * (xx - p.el0) * A[1] / xx;
+      B[2] = -p.ks * (xx - p.el0) * A[2] / xx;
+    } else {
+      B[0] = B[1] = B[2] = 0.0;
+    }
+    double bb = sqrt(B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    double koff = p.offrate * exp(bb / p.FD);
+    m.poff[ii] = 1.0 - exp(-koff * p.dtmd);
+    nd = 1;
+  } else if ((m.z[ii] < p.dthr) && (m.bondi[ii] == 0) && (m.knob[ii] == 1)) {
+    const int pid = m.pid[ii];
+    m.pon[ii] = 1.0 - exp(-p.onrate * p.dtmd);
+    int n = 0;
+    double* pd = m.pair_d + (int64_t)ii * kMaxPairs;
+    int* pj = m.pair_j + (int64_t)ii * kMaxPairs;
+    const int p1modx = m.ix[ii], p1mody = m.iy[ii];
+    const double vx = m.x[ii], vy = m.y[ii];
+    int gx0 = max((int)floor((vx - p.dthr) / 0.5) - 1, 0), gx1 = min((int)floor((vx + p.dthr) / 0.5) + 1, p.nligx - 1);
+    int gy0 = max((int)floor((vy - p.dthr) / 0.5) - 1, 0), gy1 = min((int)floor((vy + p.dthr) / 0.5) + 1, p.nligy - 1);
+    for (int gx = gx0; gx <= gx1; ++gx) {
+      for (int gy = gy0; gy <= gy1; ++gy) {
+        int j = gx * p.nligy + gy;
+        double xl = m.xlig[j], yl = m.ylig[j];
+        if (!in_liglist_f(p, pid, xl, yl)) continue;
+        A[0] = (vx + p1modx * p.Lx) - (xl + p1modx * p.Lx);
+        A[1] = (vy + p1mody * p.Ly) - (yl + p1mody * p.Ly);
+        A[2] = m.z[ii] - 0.0;
+        double aaa = (A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+        if (aaa <= p.dthr * p.dthr && n < kMaxPairs) {
+          int r = n++;
+          while (r > 0 && (pd[r - 1] > aaa || (pd[r - 1] == aaa && pj[r - 1] > j))) { pd[r] = pd[r - 1]; pj[r] = pj[r - 1]; --r; }
+          pd[r] = aaa; pj[r] = j;
+        }
+      }
+    }
+    m.npair[ii] = n;
+    nd = n;
+  }
+  double X[3];
+  const bool in_wca = wca_f(p, m, m.sc, ii, X);
+  vw[ii] = in_wca ? 1 : 0;
+  if (in_wca) { vX[3 * ii] = X[0]; vX[3 * ii + 1] = X[1]; vX[3 * ii + 2] = X[2]; }
+  vd[ii] = nd;
+  m.vx[ii] += (m.fx[ii] * p.dtmd / (2.0 * p.pmass));
+  m.vy[ii] += (m.fy[ii] * p.dtmd / (2.0 * p.pmass));
+  m.vz[ii] += (m.fz[ii] * p.dtmd / (2.0 * p.pmass));
+}
+
+// One CTA: exclusive scans of the per-vertex draw counts and WCA flags (each
+// thread owns a contiguous run of vertices, so order is kept), the bond
+// draws marked as events in parallel and applied in draw order by one warp
+// (bond_dynamics, maincode.cpp:16-54), and pfdt's parasite sum in vertex
+// order with the parasite kick (Src/memfuncs.cpp:469-482, maincode.cpp:736-744).
+__global__ void __launch_bounds__(kTailT) k_tail_b(DevParams p, Membrane m, const int* __restrict__ vd,
+                                                   const int* __restrict__ vw, const double* __restrict__ vX,
+                                                   uint64_t epoch) {
+  __shared__ int s_d[kTailT], s_w[kTailT];
+  __shared__ int s_wlist[kWcaList];
+  __shared__ double s_wx[kWcaList * 3];
+  __shared__ int s_evv[kTailDraws];
+  __shared__ short s_evr[kTailDraws];
+  __shared__ int s_tot[2];
+  const int T = blockDim.x, tid = threadIdx.x;
+  MemScalars* sc = m.sc;
+  const int chunk = (p.nv + T - 1) / T;
+  const int v0 = min(tid * chunk, p.nv), v1 = min(v0 + chunk, p.nv);
+  int nd = 0, nw = 0;
+  for (int ii = v0; ii < v1; ++ii) { nd += vd[ii]; nw += vw[ii]; }
+  s_d[tid] = nd; s_w[tid] = nw;
+  __syncthreads();
+  if (tid < 64) {
+    int* arr = tid < 32 ? s_d : s_w;
+    const int lane = tid & 31;
+    int carry = 0;
+    for (int base = 0; base < T; base += 32) {
+      int x = arr[base + lane], v = x;
+      for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += y; }
+      arr[base + lane] = carry + v - x;
+      carry += __shfl_sync(0xffffffffu, v, 31);
+    }
+    if (lane == 0) s_tot[tid >> 5] = carry;
+  }
+  __syncthreads();
+  const bool fits = s_tot[0] <= kTailDraws && s_tot[1] <= kWcaList;
+  if (fits) {
+    int od = s_d[tid], ow = s_w[tid];
+    for (int ii = v0; ii < v1; ++ii) {
+      const int n = vd[ii];
+      if (n > 0) {
+        if (m.bondi[ii] == 1) {
+          double u = draw_uniform(p.seed, STREAM_BOND, epoch, (uint64_t)od);
+          s_evv[od] = (m.poff[ii] > u) ? ii : -1;
+          s_evr[od] = -1;
+        } else {
+          const double pon = m.pon[ii];
+          for (int r = 0; r < n; ++r) {
+            double u = draw_uniform(p.seed, STREAM_BOND, epoch, (uint64_t)(od + r));
+            s_evv[od + r] = (pon > u) ? ii : -1;
+            s_evr[od + r] = r;
+          }
+        }
+        od += n;
+      }
+      if (vw[ii]) {
+        s_wx[3 * ow] = vX[3 * ii]; s_wx[3 * ow + 1] = vX[3 * ii + 1]; s_wx[3 * ow + 2] = vX[3 * ii + 2];
+        s_wlist[ow++] = ii;
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 32) {
+    double fx = 0, fy = 0, fz = 0;
+    if (fits) {
+      for (int q = 0; q < s_tot[1]; ++q) { fx += s_wx[3 * q]; fy += s_wx[3 * q + 1]; fz += s_wx[3 * q + 2]; }
+    } else {
+      for (int ii = 0; ii < p.nv; ++ii) {
+        double X[3];
+        if (wca_f(p, m, sc, ii, X)) { fx += X[0]; fy += X[1]; fz += X[2]; }
+      }
+    }
+    sc->parafdt[0] += fx; sc->parafdt[1] += fy; sc->parafdt[2] += fz;
+    for (int c = 0; c < 3; ++c) sc->paraV[c] += ((sc->paraft[c] + sc->parafdt[c]) * p.dtmd / (2.0 * p.PRmass));
+    for (int c = 0; c < 3; ++c) { sc->paraft[c] = sc->parafdt[c]; sc->parafdt[c] = 0.0; }
+  }
+  if (fits && tid < 32) {
+    const int ndt = s_tot[0];
+    for (int k0 = 0; k0 < ndt; k0 += 32) {
+      const int k = k0 + tid;
+      unsigned ev = __ballot_sync(0xffffffffu, k < ndt && s_evv[k] >= 0);
+      if (tid == 0) {
+        while (ev) {
+          const int b = __ffs(ev) - 1;
+          ev &= ev - 1;
+          const int ii = s_evv[k0 + b], r = s_evr[k0 + b];
+          if (r < 0) {
+            int jj = m.bondl[ii];
+            m.bondi[ii] = 0; m.bondl[ii] = p.randno; m.ligi[jj] = 0;
+          } else {
+            int j = m.pair_j[(int64_t)ii * kMaxPairs + r];
+            if (m.ligi[j] == 0) { m.ligi[j] = 1; m.bondi[ii] = 1; m.bondl[ii] = j; }
+          }
+        }
+      }
+    }
+  } else if (!fits && tid == 0) {
+    uint64_t k = 0;
+    for (int ii = 0; ii < p.nv; ++ii) {
+      if (m.bondi[ii] == 1) {
+        double randoff = draw_uniform(p.seed, STREAM_BOND, epoch, k++);
+        int jj = m.bondl[ii];
+        if (m.poff[ii] > randoff) { m.bondi[ii] = 0; m.bondl[ii] = p.randno; m.ligi[jj] = 0; }
+      } else if (vd[ii] > 0) {
+        const int n = m.npair[ii];
+        for (int r = 0; r < n; ++r) {
+          int j = m.pair_j[(int64_t)ii * kMaxPairs + r];
+          double pon = m.pon[ii];
+          double randon = draw_uniform(p.seed, STREAM_BOND, epoch, k++);
+          if ((pon > randon) && (m.ligi[j] == 0)) { m.ligi[j] = 1; m.bondi[ii] = 1; m.bondl[ii] = j; }
+        }
+      }
+    }
+  }
+}
+
 // half-kick + snapshot + triangle prep as separate launches (after a
 // collision, or at the first step)
 __global__ void k_kick_snap(DevParams p, Membrane m, Snap sn) {
@@ -761,21 +1111,40 @@ void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, in
   }
 }
 
-void fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st) { k_drift_va<<<1, 1024, 0, st>>>(p, m); }
-
-void fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
-                      cudaStream_t st) {
-  int items = 2 * p.ne + p.nt;
-  k_force_items<<<nb(items, 256), 256, 0, st>>>(p, m, f.slot);
-  k_force_gather<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.slot, f.gstart, f.gidx);
-  k_mem_tail<<<1, kTailT, 0, st>>>(p, m, epoch, next_kick, f.pre[next_buf], f.snap[next_buf]);
+static void set_sum_attrs() {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_m_sum, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kSumSmemT * sizeof(double));
+    cudaFuncSetAttribute(k_sum_edges, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kSumSmemT * sizeof(double));
+    attr = true;
+  }
 }
 
-void fast_membrane(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
-                   cudaStream_t st) {
-  fast_drift_va(p, m, st);
-  fast_forces_tail(p, m, f, epoch, next_kick, next_buf, st);
+// drift and the per-triangle TotalVA terms; with_sum also forms Sarea and
+// Volume (otherwise fast_forces_tail does, beside the edge terms)
+int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_sum) {
+  set_sum_attrs();
+  k_m_drift<<<nb(p.nv, 128), 128, 0, st>>>(p, m);
+  k_m_av<<<nb(p.nt, 128), 128, 0, st>>>(p, m);
+  if (!with_sum) return 2;
+  const size_t sm = p.nt <= kSumSmemT ? 2 * (size_t)p.nt * sizeof(double) : 0;
+  k_m_sum<<<1, 1024, sm, st>>>(p, m);
+  return 3;
 }
+
+int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
+                     cudaStream_t st, bool sum_pending) {
+  set_sum_attrs();
+  const size_t sm = (sum_pending && p.nt <= kSumSmemT) ? 2 * (size_t)p.nt * sizeof(double) : 0;
+  k_sum_edges<<<1 + nb(2 * p.ne, 1024), 1024, sm, st>>>(p, m, f.slot, sum_pending ? 1 : 0);
+  k_force_tri<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.slot);
+  k_force_gather_w<<<nb(p.nv, kGW), 32 * kGW, 0, st>>>(p, m, f.slot, f.gstart, f.gidx);
+  k_tail_a<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.vd, f.vw, f.vX);
+  k_tail_b<<<1, kTailT, 0, st>>>(p, m, f.vd, f.vw, f.vX, epoch);
+  if (next_kick) fast_kick_prep(p, m, f, next_buf, st);
+  return 5 + (next_kick ? 2 : 0);
+}
+
 
 }  // namespace irbc
 

@@ -23,15 +23,17 @@ struct FastBufs {
   double* slot = nullptr; // force terms: 3 doubles per slot, 4E + 9T + 4E slots
   int* gstart = nullptr;  // per-vertex slot lists in the reference's order
   int* gidx = nullptr;
+  int* vd = nullptr;      // bond draws per vertex this step
+  int* vw = nullptr;      // vertex within the parasite's WCA cutoff
+  double* vX = nullptr;   // its WCA force (3 per vertex)
 };
 
 void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
 void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st);
-void fast_membrane(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
-                   cudaStream_t st);
-void fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st);
-void fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
-                      cudaStream_t st);
+// these return the number of kernels they launched
+int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_sum);
+int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
+                     cudaStream_t st, bool sum_pending);
 
 }  // namespace irbc
