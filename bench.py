@@ -10,8 +10,10 @@ velocities from the seeded draw stream, the discocyte from
 irbc_b200/mesh.py.
 
 A "step" is one reference timestep (maincode.cpp:461-764): streaming with
-bounce-back of every particle, the membrane update, and every 12th step the
-collision.  `value` = Ns * steps * ranks / max-over-ranks device time of the
+bounce-back of every particle, the membrane update, every 12th step the
+collision and every 390th the triangle-list update (llistupdate).  The
+default 780 timed steps hold 65 collisions and 2 list updates, so every
+part of the step enters at its own frequency.  `value` = Ns * steps * ranks / max-over-ranks device time of the
 timed steps (CUDA events on the library's stream).  The solvent state
 (~630 MB in FP64) is larger than L2 (126 MB), so no flush is needed between
 steps.  N > 1 GPUs run independent replicas (different seeds), no
@@ -203,10 +205,13 @@ def run_ours(args):
     t_ms = reduce_max(prof["total_ms"], world)
     ns = WORKLOAD["Ns"]
     value = ns * args.steps * world / (t_ms * 1e-3)
-    # roofline of the streaming kernel (dominant): algorithmic bytes per launch
-    bpp = 76 if precision == G.FP64 else 36
-    stream_avg_ms = prof["stream_ms"] / max(1, prof["stream_launches"])
-    achieved = ns * bpp / (stream_avg_ms * 1e-3) / 1e9
+    # roofline of the dominant kernel, the bulk streaming kernel (one launch
+    # per step over every particle): algorithmic bytes per particle = state
+    # read + positions written (FP64: 6 x 8 read + 3 x 8 written; FP32: two
+    # float4 read + one written), divided by its CUDA-event time per launch
+    bpp = 72 if precision == G.FP64 else 48
+    bulk_avg_ms = prof["bulk_ms"] / max(1, prof["bulk_launches"])
+    achieved = ns * bpp / (bulk_avg_ms * 1e-3) / 1e9
     peak, kind = peaks()
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "stream_traffic.json")
@@ -228,9 +233,10 @@ def run_ours(args):
         "config": dict(WORKLOAD, parallelism="replicas x%d" % world if world > 1 else "single GPU",
                        l2="state larger than L2 (no flush needed)"),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": "k_stream",
-                     "bytes_per_particle": bpp, "peak_kind": kind,
-                     "kernel_ms_avg": stream_avg_ms},
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "k_stream_fast" if precision == G.FP64 else "k_stream_f",
+                     "bytes_per_particle": bpp, "units_per_launch": ns, "peak_kind": kind,
+                     "kernel_ms_avg": bulk_avg_ms},
         "phase_ms_per_step": {"stream": prof["stream_ms"] / args.steps,
                               "collide": prof["collide_ms"] / args.steps,
                               "membrane": prof["membrane_ms"] / args.steps},
@@ -292,7 +298,7 @@ def run_e2e(G, sim, steps, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--steps", type=int, default=780)
     ap.add_argument("--warmup", type=int, default=12)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])

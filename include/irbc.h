@@ -188,10 +188,12 @@ int irbc_sync(irbc_handle* h);
 /* kernel launches issued by this handle since creation */
 int64_t irbc_launch_count(const irbc_handle* h);
 /* CUDA-event timing on the handle's stream between begin and end.
- * out[0] = ms begin->end, out[1] = ms in the streaming kernel, out[2] = its
- * launches, out[3] = ms in the collision kernels, out[4] = collisions,
- * out[5] = ms in the membrane kernels, out[6] = membrane steps, out[7] =
- * kernel launches in the window */
+ * out[0] = ms begin->end, out[1] = ms in the streaming kernels, out[2] =
+ * streaming steps, out[3] = ms in the collision kernels, out[4] =
+ * collisions, out[5] = ms in the membrane kernels (side stream), out[6] =
+ * membrane launch groups, out[7] = kernel launches in the window, out[8] =
+ * ms in the bulk streaming kernel alone (k_stream_fast / k_stream_f),
+ * out[9] = its launches; nout <= 10 values are written */
 int irbc_profile_begin(irbc_handle* h);
 int irbc_profile_end(irbc_handle* h, double* out, int32_t nout);
 /* page-locked host memory for fast state exchange */

@@ -36,6 +36,7 @@ struct irbc_handle {
   int snap_buf = 0;            // which snapshot the next streaming step reads
   bool snap_ready = false;     // snapshot/triangle prep of the next step done
   cudaEvent_t ev_snap = nullptr, ev_mem = nullptr, ev_coll = nullptr, ev_str[2] = {nullptr, nullptr};
+  cudaEvent_t ev_vbin = nullptr;
   std::string err;
   bool have_mesh = false;
   int64_t step = 0;
@@ -50,7 +51,8 @@ struct irbc_handle {
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
-  std::vector<std::pair<int, size_t>> ev_marks;  // (category, index of the start event)
+  struct Mark { int cat; size_t start, end; };  // a timed span: pool indices of its two events
+  std::vector<Mark> ev_marks;
   int64_t prof_launch0 = 0;
 };
 
@@ -362,20 +364,26 @@ int64_t launches_in(const irbc_handle* h) { return g_launches.load() - h->launch
 
 // the solvent kernels of the handle's precision
 // returns the number of kernels launched: vbin, count, ghost flags, three
-// scan kernels, perm, cells, rotate, and the physical re-sort when due
-int collide_any(irbc_handle* h, uint64_t epoch, cudaStream_t st) {
+// scan kernels, perm, cells, and the physical re-sort when due.  With a
+// side stream the vertex binning runs there (after whatever the side stream
+// already holds: the membrane of the previous step) while the solvent's cell
+// counts start at once on the main stream.
+int collide_any(irbc_handle* h, uint64_t epoch, cudaStream_t st, cudaStream_t side = nullptr) {
   const int64_t before = h->s.ncoll;
-  if (h->fp32) launch_collide_f(h->dp, h->sf, h->s, h->c, h->m, epoch, st);
-  else launch_collide(h->dp, h->s, h->c, h->m, epoch, st);
-  return 9 + ((h->s.ncoll != before && h->s.ncoll % kResortEvery == 0) ? 1 : 0);
-}
-void stream_any(irbc_handle* h, int buf, cudaStream_t st) {
-  if (h->fp32) fast_stream_f(h->dp, h->sf, h->c, h->fb, buf, st);
-  else fast_stream(h->dp, h->s, h->c, h->fb, buf, st);
+  launch_vbin(h->dp, h->m, h->c, epoch, side ? side : st);
+  if (h->fp32) launch_collide_count_f(h->dp, h->sf, h->s, h->c, epoch, st);
+  else launch_collide_count(h->dp, h->s, h->c, epoch, st);
+  if (side) {
+    cudaEventRecord(h->ev_vbin, side);
+    cudaStreamWaitEvent(st, h->ev_vbin, 0);
+  }
+  if (h->fp32) launch_collide_finish_f(h->dp, h->sf, h->s, h->c, h->m, epoch, st);
+  else launch_collide_finish(h->dp, h->s, h->c, h->m, epoch, st);
+  return 8 + ((h->s.ncoll != before && h->s.ncoll % kResortEvery == 0) ? 1 : 0);
 }
 
 // profiling: a pair of events around a launch group of a category
-enum { PROF_STREAM = 0, PROF_COLLIDE = 1, PROF_MEMBRANE = 2 };
+enum { PROF_STREAM = 0, PROF_COLLIDE = 1, PROF_MEMBRANE = 2, PROF_STREAM_BULK = 3 };
 cudaEvent_t next_event(irbc_handle* h) {
   if (h->ev_used == h->ev_pool.size()) {
     cudaEvent_t e;
@@ -386,18 +394,34 @@ cudaEvent_t next_event(irbc_handle* h) {
 }
 struct ProfScope {
   irbc_handle* h;
-  size_t idx;
+  size_t mark;
   cudaStream_t st;
-  ProfScope(irbc_handle* hh, int cat, cudaStream_t s = nullptr) : h(hh), idx(0), st(s ? s : hh->st) {
+  ProfScope(irbc_handle* hh, int cat, cudaStream_t s = nullptr) : h(hh), mark(0), st(s ? s : hh->st) {
     if (!h->prof) return;
-    idx = h->ev_used;
+    const size_t idx = h->ev_used;
     cudaEventRecord(next_event(h), st);
-    h->ev_marks.push_back({cat, idx});
+    mark = h->ev_marks.size();
+    h->ev_marks.push_back({cat, idx, idx});
   }
   ~ProfScope() {
-    if (h->prof) cudaEventRecord(next_event(h), st);
+    if (!h->prof) return;
+    h->ev_marks[mark].end = h->ev_used;
+    cudaEventRecord(next_event(h), st);
   }
 };
+
+// the streaming kernels; in a profiling window the bulk kernel alone is
+// bracketed by a pair of events of its own
+void stream_any(irbc_handle* h, int buf, cudaStream_t st) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (h->prof) {
+    h->ev_marks.push_back({PROF_STREAM_BULK, h->ev_used, h->ev_used + 1});
+    e0 = next_event(h);
+    e1 = next_event(h);
+  }
+  if (h->fp32) fast_stream_f(h->dp, h->sf, h->c, h->fb, buf, st, e0, e1);
+  else fast_stream(h->dp, h->s, h->c, h->fb, buf, st, e0, e1);
+}
 
 }  // namespace
 
@@ -419,8 +443,9 @@ extern "C" int64_t irbc_footprint_bytes(const irbc_params* p, int32_t nv, int32_
   int64_t nx = (int64_t)(p->Lx / p->a), ny = (int64_t)(p->Ly / p->a), nz = (int64_t)(p->Lz / p->a) + 1;
   int64_t C = nx * ny * nz;
   int64_t ns = p->Ns;
-  int64_t b = ns * (2 * (6 * 8 + 3 * 4) + 2 * 4);    // two buffer sets + key/slot
-  b += C * (6 * 4 + 7 * 8) + (C + 1) * 4 * 2;        // cells + llist starts
+  int64_t b = ns * (2 * (3 * 8 + 32 + 2 * 4) + 4 * 4);  // two buffer sets + key/slot/perm/stream queue
+  if (p->precision == IRBC_FP32) b += ns * (2 * 32 + 2 * 4);  // float4 sets + cell ids
+  b += C * (7 * 4) + (C + 1) * 4 * 3;                // cell counts/ranks + cell and llist starts
   b += (int64_t)nv * (12 * 8 + 8 * 4 + kMaxPairs * 12) + (int64_t)ne * 40 + (int64_t)nt * 80;
   b += 2 * (int64_t)(4 * p->Lx * 4 * p->Ly) * 16;    // ligands
   b += 2 * C * 4 * 8;                                 // llist entries (typical)
@@ -450,7 +475,7 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
       delete h;
       return IRBC_ERR_CUDA;
     }
-    for (cudaEvent_t* e : {&h->ev_snap, &h->ev_mem, &h->ev_coll, &h->ev_str[0], &h->ev_str[1]})
+    for (cudaEvent_t* e : {&h->ev_snap, &h->ev_mem, &h->ev_coll, &h->ev_str[0], &h->ev_str[1], &h->ev_vbin})
       cudaEventCreateWithFlags(e, cudaEventDisableTiming);
   }
   fill_devparams(h);
@@ -463,16 +488,15 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   c.n = h->dp.ncell;
   int rc = 0;
   auto A = [&](cudaError_t err) { if (err != cudaSuccess && rc == 0) rc = IRBC_ERR_CUDA; };
-  for (double** q : {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.x2, &s.y2, &s.z2, &s.vx2, &s.vy2, &s.vz2})
-    A(dalloc(q, s.n));
-  for (int** q : {&s.id, &s.indio, &s.pid, &s.id2, &s.indio2, &s.pid2, &s.key, &s.slot, &s.perm})
-    A(dalloc(q, s.n));
-  for (int** q : {&c.cnt, &c.ncm, &c.wrank, &c.mrank, &c.lcnt}) A(dalloc(q, c.n));
+  for (double** q : {&s.x, &s.y, &s.z, &s.x2, &s.y2, &s.z2}) A(dalloc(q, s.n));
+  A(dalloc(&s.v, s.n));
+  A(dalloc(&s.v2, s.n));
+  for (int** q : {&s.indio, &s.pid, &s.indio2, &s.pid2, &s.key, &s.slot, &s.perm}) A(dalloc(q, s.n));
+  for (int** q : {&c.cnt, &c.ncm, &c.wrank, &c.mrank, &c.lcnt, &c.lrank, &c.acell}) A(dalloc(q, c.n));
   A(dalloc(&c.start, c.n + 1));
   A(dalloc(&c.lstart, c.n + 1));
   A(dalloc(&c.lstart2, c.n + 1));
   A(dalloc(&c.totals, 8));
-  A(dalloc(&c.par, c.n * 7));
   c.scan_blocks = scan_part_blocks(c.n + 1);
   A(dalloc(&c.scan_part, c.scan_blocks * 3 + 3));
   c.lcap = c.lcap2 = std::max<int64_t>(1024, c.n / 16);
@@ -491,7 +515,6 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
     for (float4** q : {&h->sf.pos, &h->sf.vel, &h->sf.pos2, &h->sf.vel2}) A(dalloc(q, s.n));
     A(dalloc(&h->sf.pid, s.n));
     A(dalloc(&h->sf.pid2, s.n));
-    A(dalloc(&c.parf, c.n * 8));
   }
   if (rc) { irbc_destroy(h); return rc; }
   cudaMemsetAsync(c.lstart, 0, sizeof(int) * (c.n + 1), h->st);
@@ -513,21 +536,22 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   if (h->st) cudaStreamSynchronize(h->st);
   if (h->st2) cudaStreamSynchronize(h->st2);
   free_fast(h->fb);
-  dfree(h->fb.queue); dfree(h->fb.qn);
+  dfree(h->fb.queue); dfree(h->fb.qn); dfree(h->fb.bcnt); dfree(h->fb.bucket);
   for (float4** q : {&h->sf.pos, &h->sf.vel, &h->sf.pos2, &h->sf.vel2}) dfree(*q);
-  dfree(h->sf.pid); dfree(h->sf.pid2); dfree(h->c.parf);
-  for (cudaEvent_t e : {h->ev_snap, h->ev_mem, h->ev_coll, h->ev_str[0], h->ev_str[1]})
+  dfree(h->sf.pid); dfree(h->sf.pid2);
+  for (cudaEvent_t e : {h->ev_snap, h->ev_mem, h->ev_coll, h->ev_str[0], h->ev_str[1], h->ev_vbin})
     if (e) cudaEventDestroy(e);
   if (h->st2) cudaStreamDestroy(h->st2);
   Solvent& s = h->s;
   Cells& c = h->c;
-  for (double** q : {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.x2, &s.y2, &s.z2, &s.vx2, &s.vy2, &s.vz2})
-    dfree(*q);
-  for (int** q : {&s.id, &s.indio, &s.pid, &s.id2, &s.indio2, &s.pid2, &s.key, &s.slot, &s.perm}) dfree(*q);
-  for (int** q : {&c.cnt, &c.ncm, &c.wrank, &c.mrank, &c.lcnt, &c.start, &c.lstart, &c.lstart2, &c.totals,
+  for (double** q : {&s.x, &s.y, &s.z, &s.x2, &s.y2, &s.z2}) dfree(*q);
+  dfree(s.v);
+  dfree(s.v2);
+  for (int** q : {&s.indio, &s.pid, &s.indio2, &s.pid2, &s.key, &s.slot, &s.perm}) dfree(*q);
+  for (int** q : {&c.cnt, &c.ncm, &c.wrank, &c.mrank, &c.lcnt, &c.lrank, &c.acell, &c.start, &c.lstart,
+                  &c.lstart2, &c.totals,
                   &c.scan_part, &c.lidx, &c.lidx2})
     dfree(*q);
-  dfree(c.par);
   free_membrane(h->m);
   dfree(h->m.ligi); dfree(h->m.xlig); dfree(h->m.ylig); dfree(h->m.sc); dfree(h->obs);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
@@ -548,6 +572,25 @@ extern "C" int irbc_sync(irbc_handle* h) {
 }
 
 // ---- llist -----------------------------------------------------------------
+// ranks of the cells with a list, and room for them in the near-membrane
+// streaming buckets
+static int refresh_listed(irbc_handle* h) {
+  Cells& c = h->c;
+  const int k = launch_llist_ranks(h->dp, c, h->st);
+  if (k < 0) return fail(h, IRBC_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  g_launches += k;
+  FastBufs& f = h->fb;
+  if (c.nact > f.bcap) {
+    dfree(f.bcnt);
+    dfree(f.bucket);
+    f.bcap = c.nact + c.nact / 2 + 64;
+    CK(dalloc(&f.bcnt, f.bcap));
+    CK(dalloc(&f.bucket, f.bcap * kBucket));
+    CK(cudaMemsetAsync(f.bcnt, 0, sizeof(int) * f.bcap, h->st));
+  }
+  return 0;
+}
+
 static int do_llist(irbc_handle* h) {
   Cells& c = h->c;
   int64_t need = launch_llist_count(h->dp, c, h->m, h->st);
@@ -560,7 +603,7 @@ static int do_llist(irbc_handle* h) {
   launch_llist_fill(h->dp, c, h->m, h->st);
   g_launches += 1;
   CK(cudaGetLastError());
-  return 0;
+  return refresh_listed(h);
 }
 
 extern "C" int irbc_llist_update(irbc_handle* h) {
@@ -685,7 +728,10 @@ extern "C" int irbc_init(irbc_handle* h, const double* V, int32_t nv, const int3
     std::sort(keys.begin(), keys.end());
     std::vector<int> id(p.Ns);
     for (int64_t r = 0; r < p.Ns; ++r) id[keys[r].idx] = (int)r;
-    if (up(h, h->s.id, id)) return IRBC_ERR_CUDA;
+    // reference indices into the velocity records (key is free between collisions)
+    if (up(h, h->s.key, id)) return IRBC_ERR_CUDA;
+    launch_pack_vel(h->s, nullptr, nullptr, nullptr, h->s.key, h->st);
+    g_launches += 1;
   }
   // llistupdate (maincode.cpp:391) on empty lists
   CK(cudaMemsetAsync(h->c.lstart, 0, sizeof(int) * (h->c.n + 1), h->st));
@@ -779,10 +825,14 @@ extern "C" int irbc_set_state(irbc_handle* h, const irbc_view* v) {
   if (v->sx) {
     std::vector<int> id(n);
     for (int64_t i = 0; i < n; ++i) id[i] = (int)i;
-    if (up(h, s.x, v->sx, n) || up(h, s.y, v->sy, n) || up(h, s.z, v->sz, n) || up(h, s.vx, v->svx, n) ||
-        up(h, s.vy, v->svy, n) || up(h, s.vz, v->svz, n) || up(h, s.pid, v->spid, n) ||
-        up(h, s.indio, v->sindio, n) || up(h, s.id, id))
+    // velocities and indices go through the free second position set and
+    // key into the velocity records
+    if (up(h, s.x, v->sx, n) || up(h, s.y, v->sy, n) || up(h, s.z, v->sz, n) || up(h, s.x2, v->svx, n) ||
+        up(h, s.y2, v->svy, n) || up(h, s.z2, v->svz, n) || up(h, s.pid, v->spid, n) ||
+        up(h, s.indio, v->sindio, n) || up(h, s.key, id))
       return IRBC_ERR_CUDA;
+    launch_pack_vel(s, s.x2, s.y2, s.z2, s.key, h->st);
+    g_launches += 1;
     if (h->fp32) f32_from_f64(h->s, h->sf, h->st);
     CK(cudaStreamSynchronize(h->st));
   }
@@ -815,6 +865,8 @@ extern "C" int irbc_set_state(irbc_handle* h, const irbc_view* v) {
       CK(dalloc(&c.lidx, c.lcap));
     }
     if (up(h, c.lstart, start) || up(h, c.lidx, v->lidx, tot)) return IRBC_ERR_CUDA;
+    int rc = refresh_listed(h);
+    if (rc) return rc;
   }
   h->dp.wallspeed = v->wallspeed;
   h->step = v->step; h->colsteps = v->colsteps; h->upd = v->upd; h->filecc = v->filecc; h->filec = v->filec;
@@ -843,7 +895,9 @@ extern "C" int irbc_get_state(irbc_handle* h, irbc_view* v) {
     std::vector<int> id(n);
     std::vector<double> buf(n);
     std::vector<int> ibuf(n);
-    if (down(h, id.data(), s.id, n)) return IRBC_ERR_CUDA;
+    launch_unpack_vel(s, s.x2, s.y2, s.z2, s.key, h->st);
+    g_launches += 1;
+    if (down(h, id.data(), s.key, n)) return IRBC_ERR_CUDA;
     CK(cudaStreamSynchronize(h->st));
     for (int64_t i = 0; i < n; ++i)
       if (id[i] < 0 || id[i] >= n) return fail(h, IRBC_ERR_STATE, "corrupt particle ids");
@@ -859,8 +913,8 @@ extern "C" int irbc_get_state(irbc_handle* h, irbc_view* v) {
       for (int64_t i = 0; i < n; ++i) dst[id[i]] = ibuf[i];
       return 0;
     };
-    if (pull(v->sx, s.x) || pull(v->sy, s.y) || pull(v->sz, s.z) || pull(v->svx, s.vx) || pull(v->svy, s.vy) ||
-        pull(v->svz, s.vz) || pulli(v->spid, s.pid) || pulli(v->sindio, s.indio))
+    if (pull(v->sx, s.x) || pull(v->sy, s.y) || pull(v->sz, s.z) || pull(v->svx, s.x2) || pull(v->svy, s.y2) ||
+        pull(v->svz, s.z2) || pulli(v->spid, s.pid) || pulli(v->sindio, s.indio))
       return IRBC_ERR_CUDA;
   }
   const int nv = m.nv;
@@ -1018,10 +1072,9 @@ extern "C" int irbc_step(irbc_handle* h, int64_t n) {
     if (s > 0) h->filecc += 1;
     const int buf = (int)(s & 1);
     if (h->colsteps == h->csteps) {
-      CK(cudaStreamWaitEvent(ms, h->ev_mem, 0));
       {
         ProfScope ps(h, PROF_COLLIDE, ms);
-        g_launches += collide_any(h, (uint64_t)s, ms);
+        g_launches += collide_any(h, (uint64_t)s, ms, ss);
       }
       h->colsteps = 0;
       CK(cudaEventRecord(h->ev_coll, ms));
@@ -1214,18 +1267,19 @@ extern "C" int irbc_profile_end(irbc_handle* h, double* out, int32_t nout) {
   CK(cudaEventRecord(h->ev_end, h->st));
   CK(cudaEventSynchronize(h->ev_end));
   h->prof = false;
-  double r[8] = {0};
+  double r[10] = {0};
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, h->ev_begin, h->ev_end));
   r[0] = ms;
   for (auto& mk : h->ev_marks) {
     float t = 0;
-    CK(cudaEventElapsedTime(&t, h->ev_pool[mk.second], h->ev_pool[mk.second + 1]));
-    r[1 + 2 * mk.first] += t;
-    r[2 + 2 * mk.first] += 1;
+    CK(cudaEventElapsedTime(&t, h->ev_pool[mk.start], h->ev_pool[mk.end]));
+    const int slot = mk.cat == PROF_STREAM_BULK ? 8 : 1 + 2 * mk.cat;
+    r[slot] += t;
+    r[slot + 1] += 1;
   }
   r[7] = (double)(g_launches.load() - h->prof_launch0);
-  for (int k = 0; k < nout && k < 8; ++k) out[k] = r[k];
+  for (int k = 0; k < nout && k < 10; ++k) out[k] = r[k];
   return 0;
 }
 

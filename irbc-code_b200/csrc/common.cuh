@@ -66,9 +66,19 @@ __device__ inline double draw_normal(uint64_t seed, uint32_t stream, uint64_t ep
   return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
 }
 
-// periodic wrap by repeated subtraction (bbound, Src/solfuncs.cpp:603-622)
+// periodic wrap by repeated subtraction (bbound, Src/solfuncs.cpp:603-622).
+// The reference's loop never ends for an infinite coordinate and runs for
+// ages for a huge one (reachable only through a degenerate contact time);
+// here a coordinate beyond 64 periods is first reduced with fmod (exact,
+// |result| < lx) and a non-finite one passes through unchanged, so every
+// call ends after at most 64 subtractions.  Below 64 periods the result is
+// the reference's.
 template <typename R>
 __device__ __forceinline__ R bbound(R x, R lx) {
+  if (!(fabs(x) < R(64) * lx)) {
+    if (!isfinite(x)) return x;
+    x = fmod(x, lx);
+  }
   if (x > lx) { while (x > lx) x -= lx; }
   if (x < R(0)) { while (x < R(0)) x += lx; }
   return x;

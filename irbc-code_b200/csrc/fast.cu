@@ -1,12 +1,13 @@
-// fast.cu -- the production FP64 step: streaming that hands particles with
-// long cell lists to a warp each, and the membrane update as four kernels
-// (drift + TotalVA in one CTA, per-item force terms, an ordered per-vertex
-// gather, and a one-CTA tail with the serial bond and parasite work) that
-// run on a side stream beside the solvent kernels.
+// fast.cu -- the production step: streaming that hands particles in cells
+// with triangles to the near-membrane kernel, and the membrane update as
+// wide per-vertex / per-item kernels plus one-CTA ordered reductions (Sarea /
+// Volume, the parasite sum, bond_dynamics) that run on a side stream beside
+// the solvent kernels.
 //
 // Results equal the one-kernel-per-phase path (kernels.cu) bit for bit.
 #include <cstdio>
 #include "fast.h"
+#include "fp32.h"
 
 namespace irbc {
 
@@ -52,10 +53,11 @@ __device__ void tri_prep_one(const DevParams& p, const Membrane& m, int j, const
 
 // ================================================================ stream =====
 // reflectionFed's per-triangle test and hit, reading the vertex snapshot.
-// Returns true if the triangle was hit (state updated).  `pre` gives the
-// precomputed normals when the particle is outside the periodic stencil
-// bands (3a from each side wall), where reflectionFed applies no shift.
-__device__ __forceinline__ bool tri_visit(const DevParams& p, const Snap& sn, const TriPre* __restrict__ pre, int jj,
+// Returns true if the triangle was hit (state updated).  `q` holds the
+// triangle's precomputed normals, used when the particle is outside the
+// periodic stencil bands (3a from each side wall), where reflectionFed
+// applies no shift.
+__device__ __forceinline__ bool tri_visit(const DevParams& p, const Snap& sn, const TriPre& q, int jj,
                                           double& X_, double& Y_, double& Z_, double& VX, double& VY, double& VZ,
                                           int indio, double& fulldt, bool use_pre) {
   const double rstep = 0.0, dtmd = p.dtmd, a = p.a, Lx = p.Lx, Ly = p.Ly;
@@ -65,7 +67,6 @@ __device__ __forceinline__ bool tri_visit(const DevParams& p, const Snap& sn, co
   double v1x, v1y, v1z, v2x, v2y, v2z, v3x, v3y, v3z;
   int p1 = sn.t1[jj], p2 = sn.t2[jj], p3 = sn.t3[jj];
   if (use_pre) {
-    const TriPre& q = pre[jj];
     double PSt0 = solvx - q.A1[0], PSt1 = solvy - q.A1[1], PSt2 = solvz - q.A1[2];
     double PD0 = (solvx + VX * (dtmd - rstep)) - q.A2[0];
     double PD1 = (solvy + VY * (dtmd - rstep)) - q.A2[1];
@@ -202,159 +203,168 @@ __device__ __forceinline__ bool in_stencil(const DevParams& p, double x, double 
   return (x < 3.0 * p.a) || (x > p.Lx - (3.0 * p.a)) || (y < 3.0 * p.a) || (y > p.Ly - (3.0 * p.a));
 }
 
+// hand-off of a particle whose cell has triangles: into the bucket of its
+// cell (rank lrank among the listed cells) when the bucket has room, else
+// onto the overflow queue
+__device__ __forceinline__ void hand_off(const int* __restrict__ lrank, int pid, int i, int* bcnt, int* bucket,
+                                         int* queue, int* qn) {
+  const int a = lrank[pid];
+  const int slot = atomicAdd(bcnt + a, 1);
+  if (slot < kBucket) { bucket[(int64_t)a * kBucket + slot] = i; return; }
+  const int q = atomicAdd(qn, 1);
+  queue[q] = i;
+}
+
 // one thread per particle: free flight, walls and wrap for particles whose
-// cell has no triangles; the others are queued for k_stream_heavy and left
+// cell has no triangles; the others are handed to k_stream_cells and left
 // untouched here
 __global__ void __launch_bounds__(256) k_stream_fast(DevParams p, Solvent s, const int* __restrict__ lstart,
-                                                     const int* __restrict__ lidx, Snap sn,
-                                                     const TriPre* __restrict__ pre, int* queue, int* qn) {
+                                                     const int* __restrict__ lrank, int* bcnt, int* bucket,
+                                                     int* queue, int* qn) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.n) return;
   double X = s.x[i], Y = s.y[i], Z = s.z[i];
-  double VX = s.vx[i], VY = s.vy[i], VZ = s.vz[i];
+  const SolVel r = s.v[i];
+  double VX = r.vx, VY = r.vy, VZ = r.vz;
   const double VX0 = VX, VY0 = VY, VZ0 = VZ;
   int fx = (int)floor(bbound(X, p.Lx));
   int fy = (int)floor(bbound(Y, p.Ly));
   int fz = (int)floor(Z + 1.0);
   int pid = cell_of(p, fx, fy, fz);
   const int l0 = __ldg(lstart + pid), l1 = __ldg(lstart + pid + 1);
-  (void)sn; (void)pre; (void)lidx;
   if (l1 > l0) {
-    // near the membrane: a warp of k_stream_heavy takes this particle
-    unsigned m = __activemask();
-    int leader = __ffs(m) - 1;
-    int lane = threadIdx.x & 31;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(qn, __popc(m));
-    base = __shfl_sync(m, base, leader);
-    queue[base + __popc(m & ((1u << lane) - 1))] = (int)i;
+    hand_off(lrank, pid, (int)i, bcnt, bucket, queue, qn);
     return;
   }
   finish_stream(p, 0.0, X, Y, Z, VX, VY, VZ);
   s.x[i] = X; s.y[i] = Y; s.z[i] = Z;
-  if (VX != VX0 || VY != VY0 || VZ != VZ0 || VX0 != VX0) { s.vx[i] = VX; s.vy[i] = VY; s.vz[i] = VZ; }
+  if (VX != VX0 || VY != VY0 || VZ != VZ0 || VX0 != VX0) { s.v[i].vx = VX; s.v[i].vy = VY; s.v[i].vz = VZ; }
 }
 
-// one warp per queued particle: lanes test 32 triangles of the list at a
-// time against the current particle state; the first candidate (lowest list
-// position) is resolved, and testing resumes after it with the updated
-// state -- the same sequence of states as the sequential loop.
-// the triangle walk of reflectionFed for one particle, by a whole warp:
-// lanes test 32 list entries at a time on copies of the particle state;
-// the first entry that would hit (lowest list position) is applied on every
-// lane and testing resumes after it with the updated state
-__device__ __forceinline__ void stream_heavy_walk(const DevParams& p, const Snap& sn, const TriPre* __restrict__ pre,
-                                                  const int* __restrict__ lidx, int l0, int l1, int lane, int indio,
-                                                  double& X, double& Y, double& Z, double& VX, double& VY,
-                                                  double& VZ, double& fulldt) {
-  int cur = l0;
-  while (cur < l1) {
+// The triangle walk of reflectionFed for one particle, by a whole warp:
+// lanes test 32 list entries at a time on copies of the particle state; the
+// first entry that would hit (lowest list position) is applied on every lane
+// and testing resumes after it with the updated state -- the same sequence
+// of states as the reference's sequential loop.  tri(e) gives the TriPre of
+// list entry e, jj(e) its triangle.
+template <class TriAt, class IdAt>
+__device__ __forceinline__ void heavy_walk(const DevParams& p, const Snap& sn, TriAt tri, IdAt jj, int len, int lane,
+                                           int indio, double& X, double& Y, double& Z, double& VX, double& VY,
+                                           double& VZ, double& fulldt) {
+  int cur = 0;
+  while (cur < len) {
     bool found = false;
-    const int j = cur + lane;
-    if (j < l1) {
+    const int e = cur + lane;
+    if (e < len) {
       double x = X, y = Y, z = Z, vx = VX, vy = VY, vz = VZ, fd = 0.0;
-      found = tri_visit(p, sn, pre, lidx[j], x, y, z, vx, vy, vz, indio, fd, !in_stencil(p, X, Y));
+      found = tri_visit(p, sn, tri(e), jj(e), x, y, z, vx, vy, vz, indio, fd, !in_stencil(p, X, Y));
     }
-    unsigned ball = __ballot_sync(0xffffffffu, found);
+    const unsigned ball = __ballot_sync(0xffffffffu, found);
     if (ball == 0) { cur += 32; continue; }
-    int first = __ffs(ball) - 1;
-    int jj = lidx[cur + first];
-    tri_visit(p, sn, pre, jj, X, Y, Z, VX, VY, VZ, indio, fulldt, !in_stencil(p, X, Y));
-    cur += first + 1;
+    const int first = cur + __ffs(ball) - 1;
+    tri_visit(p, sn, tri(first), jj(first), X, Y, Z, VX, VY, VZ, indio, fulldt, !in_stencil(p, X, Y));
+    cur = first + 1;
   }
 }
 
-__global__ void __launch_bounds__(256) k_stream_heavy(DevParams p, Solvent s, const int* __restrict__ lstart,
-                                                      const int* __restrict__ lidx, Snap sn,
-                                                      const TriPre* __restrict__ pre, const int* queue,
-                                                      const int* qn) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int nq = *qn;
-  for (int64_t q = w; q < nq; q += nw) {
-    const int64_t i = queue[q];
-    double X = s.x[i], Y = s.y[i], Z = s.z[i];
-    double VX = s.vx[i], VY = s.vy[i], VZ = s.vz[i];
-    const double VX0 = VX, VY0 = VY, VZ0 = VZ;
-    const int indio = s.indio[i];
-    int fx = (int)floor(bbound(X, p.Lx));
-    int fy = (int)floor(bbound(Y, p.Ly));
-    int fz = (int)floor(Z + 1.0);
-    int pid = cell_of(p, fx, fy, fz);
-    const int l0 = lstart[pid], l1 = lstart[pid + 1];
-    double fulldt = 0.0;
-    stream_heavy_walk(p, sn, pre, lidx, l0, l1, lane, indio, X, Y, Z, VX, VY, VZ, fulldt);
-    if (lane == 0) {
-      finish_stream(p, fulldt, X, Y, Z, VX, VY, VZ);
-      s.x[i] = X; s.y[i] = Y; s.z[i] = Z;
-      if (VX != VX0 || VY != VY0 || VZ != VZ0 || VX0 != VX0) { s.vx[i] = VX; s.vy[i] = VY; s.vz[i] = VZ; }
+// particle state in double for the walk, and its write-back
+template <bool F32>
+struct HeavyIO {
+  __device__ static void load(const Solvent& s, const SolventF& f, int64_t i, double st[6], int& indio) {
+    if constexpr (F32) {
+      const float4 q4 = f.pos[i], v4 = f.vel[i];
+      st[0] = q4.x; st[1] = q4.y; st[2] = q4.z; st[3] = v4.x; st[4] = v4.y; st[5] = v4.z;
+      indio = __float_as_int(q4.w);
+    } else {
+      const SolVel r = s.v[i];
+      st[0] = s.x[i]; st[1] = s.y[i]; st[2] = s.z[i]; st[3] = r.vx; st[4] = r.vy; st[5] = r.vz;
+      indio = s.indio[i];
     }
+  }
+  __device__ static void store(Solvent& s, SolventF& f, int64_t i, const double st[6], const double st0[6]) {
+    if constexpr (F32) {
+      f.pos[i] = make_float4((float)st[0], (float)st[1], (float)st[2], f.pos[i].w);
+      f.vel[i] = make_float4((float)st[3], (float)st[4], (float)st[5], f.vel[i].w);
+    } else {
+      s.x[i] = st[0]; s.y[i] = st[1]; s.z[i] = st[2];
+      if (st[3] != st0[3] || st[4] != st0[4] || st[5] != st0[5] || st0[3] != st0[3]) {
+        s.v[i].vx = st[3]; s.v[i].vy = st[4]; s.v[i].vz = st[5];
+      }
+    }
+  }
+};
+
+template <bool F32, class TriAt, class IdAt>
+__device__ __forceinline__ void heavy_particle(const DevParams& p, Solvent& s, SolventF& f, const Snap& sn,
+                                               int64_t i, int lane, int len, TriAt tri, IdAt ids) {
+  double st[6], st0[6];
+  int indio;
+  HeavyIO<F32>::load(s, f, i, st, indio);
+  for (int k = 0; k < 6; ++k) st0[k] = st[k];
+  double fulldt = 0.0;
+  heavy_walk(p, sn, tri, ids, len, lane, indio, st[0], st[1], st[2], st[3], st[4], st[5], fulldt);
+  if (lane == 0) {
+    finish_stream(p, fulldt, st[0], st[1], st[2], st[3], st[4], st[5]);
+    HeavyIO<F32>::store(s, f, i, st, st0);
+  }
+}
+
+// Particles in cells with triangles (reflectionFed, Src/solfuncs.cpp:400-598,
+// then the walls and wrap).  Block a < nact takes the bucket of listed cell
+// a, each warp walking one of its particles at a time; the warps of a block
+// read the same list, so its TriPre records come from L1 after the first
+// touch.  The bucket count is reset for the next step.  Blocks from nact on
+// walk the overflow queue, a warp per particle.
+template <bool F32>
+__global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, SolventF f,
+                                                      const int* __restrict__ lstart, const int* __restrict__ lidx,
+                                                      const int* __restrict__ acell, int* bcnt,
+                                                      const int* __restrict__ bucket, Snap sn,
+                                                      const TriPre* __restrict__ pre, const int* queue,
+                                                      const int* qn, int nact) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if ((int)blockIdx.x >= nact) {
+    const int nq = *qn;
+    const int64_t gw = (int64_t)(blockIdx.x - nact) * nw + w;
+    const int64_t tw = (int64_t)(gridDim.x - nact) * nw;
+    for (int64_t q = gw; q < nq; q += tw) {
+      const int64_t i = queue[q];
+      double X, Y, Z;
+      if constexpr (F32) { const float4 q4 = f.pos[i]; X = q4.x; Y = q4.y; Z = q4.z; }
+      else { X = s.x[i]; Y = s.y[i]; Z = s.z[i]; }
+      int fx = (int)floor(bbound(X, p.Lx));
+      int fy = (int)floor(bbound(Y, p.Ly));
+      int fz = (int)floor(Z + 1.0);
+      const int pid = cell_of(p, fx, fy, fz);
+      const int* L = lidx + lstart[pid];
+      heavy_particle<F32>(p, s, f, sn, i, lane, lstart[pid + 1] - lstart[pid],
+                          [&](int e) -> const TriPre& { return pre[L[e]]; }, [&](int e) { return L[e]; });
+    }
+    return;
+  }
+  const int a = blockIdx.x;
+  __shared__ int s_n;
+  if (threadIdx.x == 0) {
+    s_n = min(bcnt[a], kBucket);
+    bcnt[a] = 0;
+  }
+  __syncthreads();
+  const int n = s_n;
+  if (n == 0) return;
+  const int c = acell[a];
+  const int l0 = lstart[c], len = lstart[c + 1] - l0;
+  const int* L = lidx + l0;
+  for (int q = w; q < n; q += nw) {
+    const int64_t i = bucket[(int64_t)a * kBucket + q];
+    heavy_particle<F32>(p, s, f, sn, i, lane, len, [&](int e) -> const TriPre& { return pre[L[e]]; },
+                        [&](int e) { return L[e]; });
   }
 }
 
 // ========================================================= membrane step ====
-// drift (maincode.cpp:566-598) then TotalVA (Src/memfuncs.cpp:161-190), one CTA
-__global__ void __launch_bounds__(1024) k_drift_va(DevParams p, Membrane m) {
-  for (int i = threadIdx.x; i < p.nv; i += blockDim.x) {
-    double x = m.x[i], y = m.y[i], z = m.z[i];
-    x += (m.vx[i] * p.dtmd);
-    y += (m.vy[i] * p.dtmd);
-    z += (m.vz[i] * p.dtmd);
-    if (x > p.Lx) { x -= p.Lx; m.ix[i] += 1; }
-    if (x < 0) { x += p.Lx; m.ix[i] -= 1; }
-    if (y > p.Ly) { y -= p.Ly; m.iy[i] += 1; }
-    if (y < 0) { y += p.Ly; m.iy[i] -= 1; }
-    m.x[i] = x; m.y[i] = y; m.z[i] = z;
-  }
-  if (threadIdx.x == 0) {
-    MemScalars* sc = m.sc;
-    for (int k = 0; k < 3; ++k)
-      sc->para[k] += (sc->paraV[k] * p.dtmd) + (sc->paraft[k] * p.dtmd * p.dtmd / (2.0 * p.PRmass));
-    if (sc->para[0] > p.Lx) { sc->para[0] -= p.Lx; sc->paradx += 1; }
-    else if (sc->para[0] < 0) { sc->para[0] += p.Lx; sc->paradx -= 1; }
-    if (sc->para[1] > p.Ly) { sc->para[1] -= p.Ly; sc->parady += 1; }
-    else if (sc->para[1] < 0) { sc->para[1] += p.Ly; sc->parady -= 1; }
-  }
-  __syncthreads();
-  // per-triangle terms in parallel; the two sums left to right in triangle
-  // order, as the reference's one-thread reduction forms them: the area
-  // constraint multiplies the rounding drift of Sarea by kappasa/Sarea0
-  for (int i = threadIdx.x; i < p.nt; i += blockDim.x) {
-    int l1 = m.t1[i], l2 = m.t2[i], l3 = m.t3[i];
-    double A[3], B[3], eta[3], Cn[3];
-    A[0] = UXm(l2) - UXm(l1); A[1] = UYm(l2) - UYm(l1); A[2] = m.z[l2] - m.z[l1];
-    B[0] = UXm(l3) - UXm(l1); B[1] = UYm(l3) - UYm(l1); B[2] = m.z[l3] - m.z[l1];
-    cp(A, B, eta);
-    m.area[i] = 0.5 * sqrt(eta[0] * eta[0] + eta[1] * eta[1] + eta[2] * eta[2]);
-    Cn[0] = (UXm(l1) + UXm(l2) + UXm(l3)) / 3.0;
-    Cn[1] = (UYm(l1) + UYm(l2) + UYm(l3)) / 3.0;
-    Cn[2] = (m.z[l1] + m.z[l2] + m.z[l3]) / 3.0;
-    m.vol[i] = (1.0 / 6.0) * ((eta[0] * Cn[0]) + (eta[1] * Cn[1]) + (eta[2] * Cn[2]));
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-#pragma unroll 8
-    for (int i = 0; i < p.nt; ++i) t += m.area[i];
-    m.sc->Sarea = t;
-  } else if (threadIdx.x == 32) {
-    double t = 0.0;
-#pragma unroll 8
-    for (int i = 0; i < p.nt; ++i) t += m.vol[i];
-    m.sc->Volume = t;
-  }
-}
-
 // force terms of every edge (WLC + POW), triangle (local/global area and
 // volume) and bending dihedral, stored per term in slots so the per-vertex
 // gather can add them in the reference's order (Src/memfuncs.cpp:233-427)
-__device__ void force_item(const DevParams& p, const Membrane& m, double* __restrict__ slot, int t);
-
-__global__ void __launch_bounds__(256) k_force_items(DevParams p, Membrane m, double* __restrict__ slot) {
-  force_item(p, m, slot, blockIdx.x * blockDim.x + threadIdx.x);
-}
-
 // item t of [edges | triangles | dihedrals]: its force terms into the slots
 __device__ void force_item(const DevParams& p, const Membrane& m, double* __restrict__ slot, int t) {
   const MemScalars* sc = m.sc;
@@ -475,46 +485,7 @@ __device__ __forceinline__ bool wca_f(const DevParams& p, const Membrane& m, con
   return false;
 }
 
-// per vertex, in the order of maincode.cpp:603-665: pfdt's -X, the sum of
-// the force slots (reference order), gravity, bond spring, wall repulsion
-__global__ void __launch_bounds__(128) k_force_gather(DevParams p, Membrane m, const double* __restrict__ slot,
-                                                      const int* __restrict__ gstart, const int* __restrict__ gidx) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.nv) return;
-  const MemScalars* sc = m.sc;
-  double f[3] = {m.fx[i], m.fy[i], m.fz[i]};
-  double X[3];
-  if (wca_f(p, m, sc, i, X)) { f[0] -= X[0]; f[1] -= X[1]; f[2] -= X[2]; }
-  double ff[3] = {0.0, 0.0, 0.0};
-  for (int q = gstart[i]; q < gstart[i + 1]; ++q) {
-    const double* S = slot + 3 * (int64_t)gidx[q];
-    ff[0] += S[0]; ff[1] += S[1]; ff[2] += S[2];
-  }
-  f[0] += ff[0]; f[1] += ff[1]; f[2] += ff[2];
-  f[2] += -p.Fg / (double)p.nv;
-  if (m.bondi[i] == 1) {
-    int jj = m.bondl[i];
-    double A[3];
-    A[0] = m.x[i] - m.xlig[jj];
-    A[1] = m.y[i] - m.ylig[jj];
-    A[2] = m.z[i];
-    A[0] -= p.Lx * round(A[0] / p.Lx);
-    A[1] -= p.Ly * round(A[1] / p.Ly);
-    double aa = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
-    A[0] /= aa; A[1] /= aa; A[2] /= aa;
-    if (aa > p.el0) {
-      f[0] += -p.ks * (aa - p.el0) * A[0];
-      f[1] += -p.ks * (aa - p.el0) * A[1];
-      f[2] += -p.ks * (aa - p.el0) * A[2];
-    }
-  }
-  double cc = m.z[i];
-  if (cc < 0.5) f[2] += 300.0 * exp(-50.0 * cc);
-  cc = p.Lz - m.z[i];
-  if (cc < 0.5) f[2] -= 300.0 * exp(-50.0 * cc);
-  m.fx[i] = f[0]; m.fy[i] = f[1]; m.fz[i] = f[2];
-}
-
+// ligand (xl, yl) on the ligand list of a cell (maincode.cpp:138-154)
 __device__ __forceinline__ bool in_liglist_f(const DevParams& p, int cell, double xl, double yl) {
   int k = cell % p.nz, j = (cell / p.nz) % p.ny, i = cell / (p.nz * p.ny);
   double zmax = -1.0 + (double)k * p.a + p.a;
@@ -528,204 +499,10 @@ __device__ __forceinline__ bool in_liglist_f(const DevParams& p, int cell, doubl
   return (A0 < 1.5) && (A1 < 1.5);
 }
 
-// One CTA: bond preparation (maincode.cpp:668-723), second half-kick
-// (:727-733), pfdt's parasite sum in vertex order (Src/memfuncs.cpp:469-482),
-// bond_dynamics (:16-54) over the compacted, ordered list of bonded or
-// eligible vertices with its uniforms drawn in parallel, the parasite kick
-// (:736-744), and, when the next step has no collision, the next step's
-// half-kick (:487-496) with the snapshot and triangle prep for its
-// streaming.  Each thread owns a contiguous run of vertices so that a block
-// scan of per-thread counts keeps vertex order in the compacted lists.
-constexpr int kTailT = 1024, kTailList = 1024, kTailDraws = 4096, kWcaList = 512;
-__global__ void __launch_bounds__(kTailT) k_mem_tail(DevParams p, Membrane m, uint64_t epoch, int next_kick,
-                                                    TriPre* pre, Snap sn) {
-  __shared__ int s_a[kTailT], s_w[kTailT], s_d[kTailT];
-  __shared__ int s_wlist[kTailList];
-  __shared__ int s_evv[kTailDraws];        // vertex of an event at draw k, or -1
-  __shared__ short s_evr[kTailDraws];      // its pair index, -1 for unbinding
-  __shared__ int s_tot[3];
-  const int T = blockDim.x, tid = threadIdx.x;
-  MemScalars* sc = m.sc;
-  const int chunk = (p.nv + T - 1) / T;
-  const int v0 = min(tid * chunk, p.nv), v1 = min(v0 + chunk, p.nv);
-  int na = 0, nw = 0, nd = 0;
-  for (int ii = v0; ii < v1; ++ii) {
-    double A[3], B[3];
-    if (m.bondi[ii] == 1) {
-      int p1modx = m.ix[ii], p1mody = m.iy[ii], jj = m.bondl[ii];
-      A[0] = (m.x[ii] + p1modx * p.Lx) - (m.xlig[jj] + p1modx * p.Lx);
-      A[1] = (m.y[ii] + p1mody * p.Ly) - (m.ylig[jj] + p1mody * p.Ly);
-      A[2] = m.z[ii] - 0.0;
-      double xx = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
-      if (xx > p.el0) {
-        B[0] = -p.ks * (xx - p.el0) * A[0] / xx;
-        B[1] = -p.ks * (xx - p.el0) * A[1] / xx;
-        B[2] = -p.ks * (xx - p.el0) * A[2] / xx;
-      } else {
-        B[0] = B[1] = B[2] = 0.0;
-      }
-      double bb = sqrt(B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
-      double koff = p.offrate * exp(bb / p.FD);
-      m.poff[ii] = 1.0 - exp(-koff * p.dtmd);
-      na += 1; nd += 1;
-    } else if ((m.z[ii] < p.dthr) && (m.bondi[ii] == 0) && (m.knob[ii] == 1)) {
-      const int pid = m.pid[ii];
-      m.pon[ii] = 1.0 - exp(-p.onrate * p.dtmd);
-      int n = 0;
-      double* pd = m.pair_d + (int64_t)ii * kMaxPairs;
-      int* pj = m.pair_j + (int64_t)ii * kMaxPairs;
-      const int p1modx = m.ix[ii], p1mody = m.iy[ii];
-      const double vx = m.x[ii], vy = m.y[ii];
-      int gx0 = max((int)floor((vx - p.dthr) / 0.5) - 1, 0), gx1 = min((int)floor((vx + p.dthr) / 0.5) + 1, p.nligx - 1);
-      int gy0 = max((int)floor((vy - p.dthr) / 0.5) - 1, 0), gy1 = min((int)floor((vy + p.dthr) / 0.5) + 1, p.nligy - 1);
-      for (int gx = gx0; gx <= gx1; ++gx) {
-        for (int gy = gy0; gy <= gy1; ++gy) {
-          int j = gx * p.nligy + gy;
-          double xl = m.xlig[j], yl = m.ylig[j];
-          if (!in_liglist_f(p, pid, xl, yl)) continue;
-          A[0] = (vx + p1modx * p.Lx) - (xl + p1modx * p.Lx);
-          A[1] = (vy + p1mody * p.Ly) - (yl + p1mody * p.Ly);
-          A[2] = m.z[ii] - 0.0;
-          double aaa = (A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
-          if (aaa <= p.dthr * p.dthr && n < kMaxPairs) {
-            int r = n++;
-            while (r > 0 && (pd[r - 1] > aaa || (pd[r - 1] == aaa && pj[r - 1] > j))) { pd[r] = pd[r - 1]; pj[r] = pj[r - 1]; --r; }
-            pd[r] = aaa; pj[r] = j;
-          }
-        }
-      }
-      m.npair[ii] = n;
-      na += 1; nd += n;
-    }
-    double X[3];
-    nw += wca_f(p, m, sc, ii, X) ? 1 : 0;
-    m.vx[ii] += (m.fx[ii] * p.dtmd / (2.0 * p.pmass));
-    m.vy[ii] += (m.fy[ii] * p.dtmd / (2.0 * p.pmass));
-    m.vz[ii] += (m.fz[ii] * p.dtmd / (2.0 * p.pmass));
-  }
-  s_a[tid] = na; s_w[tid] = nw; s_d[tid] = nd;
-  __syncthreads();
-  // exclusive scans of the three per-thread counts, one warp per array
-  if (tid < 96) {
-    int* arr = tid < 32 ? s_a : (tid < 64 ? s_w : s_d);
-    const int lane = tid & 31;
-    int carry = 0;
-    for (int base = 0; base < T; base += 32) {
-      int x = arr[base + lane], v = x;
-      for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += y; }
-      arr[base + lane] = carry + v - x;
-      carry += __shfl_sync(0xffffffffu, v, 31);
-    }
-    if (lane == 0) s_tot[tid >> 5] = carry;
-  }
-  __syncthreads();
-  const bool fits = s_tot[0] <= kTailList && s_tot[1] <= kTailList && s_tot[2] <= kTailDraws;
-  // Draw k decides something only if it passes its probability test (an
-  // "event": poff > u for a bonded vertex, pon > u for a candidate pair);
-  // all other draws leave the state unchanged.  Events are marked by draw
-  // index in parallel; bond_dynamics then applies just the events, in draw
-  // order, which gives the reference's serial result.
-  if (fits) {
-    int ow = s_w[tid], od = s_d[tid];
-    for (int ii = v0; ii < v1; ++ii) {
-      const bool bonded = m.bondi[ii] == 1;
-      const bool elig = !bonded && (m.z[ii] < p.dthr) && (m.knob[ii] == 1);
-      if (bonded) {
-        double u = draw_uniform(p.seed, STREAM_BOND, epoch, (uint64_t)od);
-        s_evv[od] = (m.poff[ii] > u) ? ii : -1;
-        s_evr[od] = -1;
-        od += 1;
-      } else if (elig) {
-        const int n = m.npair[ii];
-        const double pon = m.pon[ii];
-        for (int r = 0; r < n; ++r) {
-          double u = draw_uniform(p.seed, STREAM_BOND, epoch, (uint64_t)(od + r));
-          s_evv[od + r] = (pon > u) ? ii : -1;
-          s_evr[od + r] = r;
-        }
-        od += n;
-      }
-      double X[3];
-      if (wca_f(p, m, sc, ii, X)) s_wlist[ow++] = ii;
-    }
-  }
-  __syncthreads();
-  if (tid == 32) {
-    // pfdt's parasite sum in vertex order, then the parasite kick
-    double fx = 0, fy = 0, fz = 0;
-    if (fits) {
-      for (int q = 0; q < s_tot[1]; ++q) {
-        double X[3];
-        wca_f(p, m, sc, s_wlist[q], X);
-        fx += X[0]; fy += X[1]; fz += X[2];
-      }
-    } else {
-      for (int ii = 0; ii < p.nv; ++ii) {
-        double X[3];
-        if (wca_f(p, m, sc, ii, X)) { fx += X[0]; fy += X[1]; fz += X[2]; }
-      }
-    }
-    sc->parafdt[0] += fx; sc->parafdt[1] += fy; sc->parafdt[2] += fz;
-    for (int c = 0; c < 3; ++c) sc->paraV[c] += ((sc->paraft[c] + sc->parafdt[c]) * p.dtmd / (2.0 * p.PRmass));
-    for (int c = 0; c < 3; ++c) { sc->paraft[c] = sc->parafdt[c]; sc->parafdt[c] = 0.0; }
-  }
-  if (fits && tid < 32) {
-    const int nd = s_tot[2];
-    for (int k0 = 0; k0 < nd; k0 += 32) {
-      const int k = k0 + tid;
-      unsigned ev = __ballot_sync(0xffffffffu, k < nd && s_evv[k] >= 0);
-      if (tid == 0) {
-        while (ev) {
-          const int b = __ffs(ev) - 1;
-          ev &= ev - 1;
-          const int ii = s_evv[k0 + b], r = s_evr[k0 + b];
-          if (r < 0) {  // unbinding (maincode.cpp:30-35)
-            int jj = m.bondl[ii];
-            m.bondi[ii] = 0; m.bondl[ii] = p.randno; m.ligi[jj] = 0;
-          } else {      // binding attempt on a free ligand (:45-50)
-            int j = m.pair_j[(int64_t)ii * kMaxPairs + r];
-            if (m.ligi[j] == 0) { m.ligi[j] = 1; m.bondi[ii] = 1; m.bondl[ii] = j; }
-          }
-        }
-      }
-    }
-  } else if (!fits && tid == 0) {
-    // lists larger than the shared buffers: the plain serial walk
-    uint64_t k = 0;
-    for (int ii = 0; ii < p.nv; ++ii) {
-      if (m.bondi[ii] == 1) {
-        double randoff = draw_uniform(p.seed, STREAM_BOND, epoch, k++);
-        int jj = m.bondl[ii];
-        if (m.poff[ii] > randoff) { m.bondi[ii] = 0; m.bondl[ii] = p.randno; m.ligi[jj] = 0; }
-      } else if ((m.z[ii] < p.dthr) && (m.bondi[ii] == 0) && (m.knob[ii] == 1)) {
-        const int n = m.npair[ii];
-        for (int r = 0; r < n; ++r) {
-          int j = m.pair_j[(int64_t)ii * kMaxPairs + r];
-          double pon = m.pon[ii];
-          double randon = draw_uniform(p.seed, STREAM_BOND, epoch, k++);
-          if ((pon > randon) && (m.ligi[j] == 0)) { m.ligi[j] = 1; m.bondi[ii] = 1; m.bondl[ii] = j; }
-        }
-      }
-    }
-  }
-  if (!next_kick) return;
-  __syncthreads();
-  for (int i = tid; i < p.nv; i += T) {
-    double vx = m.vx[i] + (m.fx[i] * p.dtmd / (2.0 * p.pmass));
-    double vy = m.vy[i] + (m.fy[i] * p.dtmd / (2.0 * p.pmass));
-    double vz = m.vz[i] + (m.fz[i] * p.dtmd / (2.0 * p.pmass));
-    m.vx[i] = vx; m.vy[i] = vy; m.vz[i] = vz;
-    m.fx[i] = 0.0; m.fy[i] = 0.0; m.fz[i] = 0.0;
-    sn.x[i] = m.x[i]; sn.y[i] = m.y[i]; sn.z[i] = m.z[i];
-    sn.vx[i] = vx; sn.vy[i] = vy; sn.vz[i] = vz;
-  }
-  __syncthreads();
-  for (int j = tid; j < p.nt; j += T) tri_prep_one(p, m, j, m.vx, m.vy, m.vz, pre);
-}
+constexpr int kTailT = 1024, kTailDraws = 4096, kWcaList = 512;
 
 // ================================================= membrane step, wide form ===
-// The same phases as k_drift_va / k_force_gather / k_mem_tail, spread over
-// many SMs: per-vertex and per-triangle work in wide kernels, the ordered
+// The membrane step spread over many SMs: per-vertex and per-triangle work in wide kernels, the ordered
 // reductions (Sarea, Volume, the parasite sum, bond_dynamics) in one CTA
 // reading shared memory.
 
@@ -1103,11 +880,23 @@ void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaS
   k_tri_prep<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.pre[buf]);
 }
 
-void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st) {
+template <bool F32>
+static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
+                                cudaStream_t st) {
+  k_stream_cells<F32><<<c.nact + kOverflowBlocks, 256, 0, st>>>(p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt,
+                                                               f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
+                                                               c.nact);
+}
+
+void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
+                 cudaEvent_t ev0, cudaEvent_t ev1) {
   cudaMemsetAsync(f.qn, 0, sizeof(int), st);
   if (s.n) {
-    k_stream_fast<<<nb(s.n, 256), 256, 0, st>>>(p, s, c.lstart, c.lidx, f.snap[buf], f.pre[buf], f.queue, f.qn);
-    k_stream_heavy<<<148 * 4, 256, 0, st>>>(p, s, c.lstart, c.lidx, f.snap[buf], f.pre[buf], f.queue, f.qn);
+    if (ev0) cudaEventRecord(ev0, st);
+    k_stream_fast<<<nb(s.n, 256), 256, 0, st>>>(p, s, c.lstart, c.lrank, f.bcnt, f.bucket, f.queue, f.qn);
+    if (ev1) cudaEventRecord(ev1, st);
+    SolventF none;
+    launch_stream_cells<false>(p, s, none, c, f, buf, st);
   }
 }
 

@@ -15,11 +15,19 @@ struct Snap {
   const int *t1, *t2, *t3;
 };
 
+// near-membrane streaming: particles per listed cell taken by the cell's
+// block, and the blocks that walk the overflow queue (full buckets)
+constexpr int kBucket = 32;
+constexpr int kOverflowBlocks = 8;
+
 struct FastBufs {
   Snap snap[2];
   TriPre* pre[2] = {nullptr, nullptr};
-  int* queue = nullptr;   // particles with long cell lists (capacity Ns)
+  int* queue = nullptr;   // overflow: particles of full buckets or over-long lists (capacity Ns)
   int* qn = nullptr;
+  int* bcnt = nullptr;    // particles handed to each listed cell this step (reset by k_stream_cells)
+  int* bucket = nullptr;  // kBucket particle slots per listed cell
+  int64_t bcap = 0;       // listed cells the buckets have room for
   double* slot = nullptr; // force terms: 3 doubles per slot, 4E + 9T + 4E slots
   int* gstart = nullptr;  // per-vertex slot lists in the reference's order
   int* gidx = nullptr;
@@ -30,7 +38,9 @@ struct FastBufs {
 
 void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
-void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st);
+// ev0/ev1 (optional) are recorded around the bulk kernel k_stream_fast
+void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
+                 cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
 // these return the number of kernels they launched
 int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_sum);
 int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include "fast.h"
 #include "fp32.h"
+#include "cells_tile.cuh"
 
 namespace irbc {
 
@@ -17,7 +18,8 @@ __global__ void k_to_f32(Solvent s, SolventF f) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.n) return;
   f.pos[i] = make_float4((float)s.x[i], (float)s.y[i], (float)s.z[i], __int_as_float(s.indio[i]));
-  f.vel[i] = make_float4((float)s.vx[i], (float)s.vy[i], (float)s.vz[i], __int_as_float(s.id[i]));
+  const SolVel r = s.v[i];
+  f.vel[i] = make_float4((float)r.vx, (float)r.vy, (float)r.vz, __int_as_float(r.id));
   f.pid[i] = s.pid[i];
 }
 __global__ void k_to_f64(SolventF f, Solvent s) {
@@ -25,7 +27,9 @@ __global__ void k_to_f64(SolventF f, Solvent s) {
   if (i >= s.n) return;
   float4 p = f.pos[i], v = f.vel[i];
   s.x[i] = p.x; s.y[i] = p.y; s.z[i] = p.z; s.indio[i] = __float_as_int(p.w);
-  s.vx[i] = v.x; s.vy[i] = v.y; s.vz[i] = v.z; s.id[i] = __float_as_int(v.w);
+  SolVel r;
+  r.vx = v.x; r.vy = v.y; r.vz = v.z; r.id = __float_as_int(v.w); r.pad = 0;
+  s.v[i] = r;
   s.pid[i] = f.pid[i];
 }
 void f32_from_f64(Solvent& s, SolventF& f, cudaStream_t st) {
@@ -80,186 +84,22 @@ __global__ void k_gather_f(SolventF f, const int* __restrict__ perm) {
   f.pid2[j] = f.pid[i];
 }
 
-// per-cell statistics, one thread per cell, sums in double in reference
-// particle order (CollisionStep, Src/solfuncs.cpp:164-318)
-constexpr int kMaxSegF = 48;
-__global__ void k_cells_f(DevParams p, SolventF f, const int* __restrict__ perm, Cells cl, Membrane m,
-                          uint64_t epoch) {
-  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= p.ncell) return;
-  const int64_t s0 = cl.start[c];
-  const int n = cl.start[c + 1] - (int)s0;
-  const int* __restrict__ PP = perm + s0;
-  int ord[kMaxSegF], oid[kMaxSegF];
-  const bool small = n <= kMaxSegF;
-  if (small) {
-    for (int q = 0; q < n; ++q) {
-      int pq = PP[q];
-      int idq = __float_as_int(f.vel[pq].w);
-      int r = q;
-      while (r > 0 && oid[r - 1] > idq) { ord[r] = ord[r - 1]; oid[r] = oid[r - 1]; --r; }
-      ord[r] = pq;
-      oid[r] = idq;
-    }
-  }
-  auto nth = [&](int q) -> int64_t {
-    if (small) return ord[q];
-    int last = -1;
-    int64_t at = PP[0];
-    for (int t = 0; t <= q; ++t) {
-      int best = 0x7fffffff;
-      for (int u = 0; u < n; ++u) {
-        int v = __float_as_int(f.vel[PP[u]].w);
-        if (v > last && v < best) { best = v; at = PP[u]; }
-      }
-      last = best;
-    }
-    return at;
-  };
-  const MemScalars* sc = m.sc;
-  double vcm[3] = {0.0, 0.0, 0.0}, ncc = 0.0;
-  int nc = 0;
-  for (int q = 0; q < n; ++q) {
-    float4 v = f.vel[nth(q)];
-    vcm[0] += p.mass * (double)v.x;
-    vcm[1] += p.mass * (double)v.y;
-    vcm[2] += p.mass * (double)v.z;
-    ncc += (1 * p.mass);
-    nc += 1;
-  }
-  const int k = (int)(c % p.nz);
-  const double zmin = -1.0 + (double)k * p.a, zmax = -1.0 + (double)k * p.a + p.a;
-  {
-    int nn = nc;
-    uint64_t g = 3 * (uint64_t)cl.wrank[c];
-    if ((zmax >= p.Lz || zmin <= 0) && nn < p.navg) {
-      const double sd = sqrt((p.navg - nn) * p.Theta / p.mass);
-      const double mx = zmax >= p.Lz ? (p.navg - nn) * p.wallspeed : 0.0;
-      vcm[0] += p.mass * (draw_normal(p.seed, STREAM_COLLIDE_N, epoch, g + 0) * sd + mx);
-      vcm[1] += p.mass * (draw_normal(p.seed, STREAM_COLLIDE_N, epoch, g + 1) * sd + 0);
-      vcm[2] += p.mass * (draw_normal(p.seed, STREAM_COLLIDE_N, epoch, g + 2) * sd + 0);
-      ncc = p.navg * p.mass;
-    }
-  }
-  const int nmem = cl.ncm[c];
-  int v0 = 0;
-  if (nmem > 0) {
-    int lo = 0, hi = p.nv;
-    const uint64_t key0 = (uint64_t)(uint32_t)c << 32;
-    while (lo < hi) { int mid = (lo + hi) >> 1; if (m.vkey[mid] < key0) lo = mid + 1; else hi = mid; }
-    v0 = lo;
-    for (int q = 0; q < nmem; ++q) {
-      int i = (int)(m.vkey[v0 + q] & 0xffffffffu);
-      vcm[0] += p.pmass * m.vx[i];
-      vcm[1] += p.pmass * m.vy[i];
-      vcm[2] += p.pmass * m.vz[i];
-      ncc += (1 * p.pmass);
-      nc += 1;
-    }
-  }
-  const bool has_para = (c == sc->paraid);
-  if (has_para) {
-    for (int q = 0; q < 3; ++q) vcm[q] += p.PRmass * sc->paraV[q];
-    ncc += (1 * p.PRmass);
-    nc += 1;
-  }
-  {
-    int nn = nc;
-    if ((nn < p.navg) && (nmem > 0)) {
-      uint64_t g = 3 * ((uint64_t)cl.totals[1] + (uint64_t)cl.mrank[c]);
-      const double sd = sqrt((p.navg - nn) * p.Theta / p.mass);
-      for (int q = 0; q < 3; ++q) vcm[q] += p.mass * (draw_normal(p.seed, STREAM_COLLIDE_N, epoch, g + q) * sd + 0);
-      ncc += (p.navg - nn) * p.mass;
-    }
-  }
-  {
-    int nn = (int)ncc;
-    if (nn != 0) { vcm[0] /= (double)nn; vcm[1] /= (double)nn; vcm[2] /= (double)nn; }
-  }
-  const double rand1 = 2.0 * p.Pi * draw_uniform(p.seed, STREAM_COLLIDE_U, epoch, 3 + 2 * (uint64_t)c);
-  const double rand2 = -1.0 + (2.0 * draw_uniform(p.seed, STREAM_COLLIDE_U, epoch, 4 + 2 * (uint64_t)c));
-  double dvv = 0.0;
-  for (int q = 0; q < n; ++q) {
-    float4 v = f.vel[nth(q)];
-    double A0 = (double)v.x - vcm[0], A1 = (double)v.y - vcm[1], A2 = (double)v.z - vcm[2];
-    dvv += (p.mass * (A0 * A0 + A1 * A1 + A2 * A2));
-  }
-  for (int q = 0; q < nmem; ++q) {
-    int i = (int)(m.vkey[v0 + q] & 0xffffffffu);
-    double A0 = m.vx[i] - vcm[0], A1 = m.vy[i] - vcm[1], A2 = m.vz[i] - vcm[2];
-    dvv += (p.pmass * (A0 * A0 + A1 * A1 + A2 * A2));
-  }
-  if (has_para) {
-    double A0 = sc->paraV[0] - vcm[0], A1 = sc->paraV[1] - vcm[1], A2 = sc->paraV[2] - vcm[2];
-    dvv += (p.PRmass * (A0 * A0 + A1 * A1 + A2 * A2));
-  }
-  double ThE = 1.0;
-  if ((nc > 0) && (dvv != 0)) ThE = sqrt(3.0 * ((double)nc - 1.0) * p.Theta / (dvv));
-  double P[7];
-  P[0] = vcm[0]; P[1] = vcm[1]; P[2] = vcm[2];
-  P[3] = sqrt(1.0 - (rand2 * rand2)) * cos(rand1);
-  P[4] = sqrt(1.0 - (rand2 * rand2)) * sin(rand1);
-  P[5] = rand2;
-  P[6] = ThE;
-  float* out = cl.parf + c * 8;
-  for (int q = 0; q < 7; ++q) out[q] = (float)P[q];
-  // vertices and parasite: rotated in double (CollisionDynmem / Dynpara)
-  for (int q = 0; q < nmem; ++q) {
-    int i = (int)(m.vkey[v0 + q] & 0xffffffffu);
-    double v[3] = {m.vx[i], m.vy[i], m.vz[i]};
-    double unit[3] = {P[3], P[4], P[5]}, dv[3], dvp[3], dvn[3], dvpn[3];
-    for (int e = 0; e < 3; ++e) dv[e] = v[e] - P[e];
-    double xxx = dv[0] * unit[0] + dv[1] * unit[1] + dv[2] * unit[2];
-    for (int e = 0; e < 3; ++e) { dvp[e] = xxx * unit[e]; dvn[e] = dv[e] - dvp[e]; }
-    cp(dvn, unit, dvpn);
-    for (int e = 0; e < 3; ++e) v[e] = P[e] + ThE * (p.cosalpha * dvn[e] + p.sinalpha * dvpn[e] + dvp[e]);
-    m.vx[i] = v[0]; m.vy[i] = v[1]; m.vz[i] = v[2];
-  }
-  if (has_para) {
-    MemScalars* scw = m.sc;
-    double v[3] = {scw->paraV[0], scw->paraV[1], scw->paraV[2]};
-    double unit[3] = {P[3], P[4], P[5]}, dv[3], dvp[3], dvn[3], dvpn[3];
-    for (int e = 0; e < 3; ++e) dv[e] = v[e] - P[e];
-    double xxx = dv[0] * unit[0] + dv[1] * unit[1] + dv[2] * unit[2];
-    for (int e = 0; e < 3; ++e) { dvp[e] = xxx * unit[e]; dvn[e] = dv[e] - dvp[e]; }
-    cp(dvn, unit, dvpn);
-    for (int e = 0; e < 3; ++e) scw->paraV[e] = P[e] + ThE * (p.cosalpha * dvn[e] + p.sinalpha * dvpn[e] + dvp[e]);
-  }
-}
-
-// rotation of the solvent in float (CollisionDyn, Src/solfuncs.cpp:700-736)
-__global__ void __launch_bounds__(256) k_rotate_f(SolventF f, const float* __restrict__ parf, float cosalpha,
-                                                  float sinalpha) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= f.n) return;
-  const float4* P4 = reinterpret_cast<const float4*>(parf + (int64_t)f.pid[i] * 8);
-  float4 a = __ldg(P4), b = __ldg(P4 + 1);   // vcm xyz, ux | uy uz ThE -
-  float4 v = f.vel[i];
-  float ux = a.w, uy = b.x, uz = b.y, s = b.z;
-  float dx = v.x - a.x, dy = v.y - a.y, dz = v.z - a.z;
-  float xx = dx * ux + dy * uy + dz * uz;
-  float px = xx * ux, py = xx * uy, pz = xx * uz;
-  float nx = dx - px, ny = dy - py, nz = dz - pz;
-  float cx = (ny * uz) - (uy * nz), cy = (nz * ux) - (uz * nx), cz = (nx * uy) - (ux * ny);
-  v.x = a.x + s * (cosalpha * nx + sinalpha * cx + px);
-  v.y = a.y + s * (cosalpha * ny + sinalpha * cy + py);
-  v.z = a.z + s * (cosalpha * nz + sinalpha * cz + pz);
-  f.vel[i] = v;
-}
-
-void launch_collide_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
-                      cudaStream_t st) {
+void launch_collide_count_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, uint64_t epoch,
+                            cudaStream_t st) {
   cudaMemsetAsync(c.cnt, 0, sizeof(int) * c.n, st);
-  cudaMemsetAsync(c.ncm, 0, sizeof(int) * c.n, st);
-  launch_vbin(p, m, c, epoch, st);
   if (f.n) k_count_f<<<nbf(f.n, 256), 256, 0, st>>>(p, f, c.cnt, s.key, s.slot, epoch);
+}
+
+// per-cell statistics (sums in double, reference particle order) and the
+// float rotation: k_cells_tile<true> (cells_tile.cuh)
+void launch_collide_finish_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
+                             cudaStream_t st) {
   launch_ghost_flags(p, c, m, st);
   launch_scan3(c.cnt, c.wrank, c.mrank, c.start, c.wrank, c.mrank, c.totals, c.n, c.scan_part, st);
   cudaMemcpyAsync(c.start + c.n, c.totals + 0, sizeof(int), cudaMemcpyDeviceToDevice, st);
   if (f.n) k_perm_f<<<nbf(f.n, 256), 256, 0, st>>>(s.key, s.slot, c.start, f.n, s.perm);
   std::swap(f.pid, s.key);  // pid = cell of this collision, in place
-  k_cells_f<<<nbf(c.n, 128), 128, 0, st>>>(p, f, s.perm, c, m, epoch);
-  if (f.n) k_rotate_f<<<nbf(f.n, 256), 256, 0, st>>>(f, c.parf, (float)p.cosalpha, (float)p.sinalpha);
+  k_cells_tile<true><<<cells_tile_blocks(c.n), 32 * kTileWarps, 0, st>>>(p, s, f, c, m, epoch);
   if (f.n && (++s.ncoll % kResortEvery) == 0) {
     k_gather_f<<<nbf(f.n, 256), 256, 0, st>>>(f, s.perm);
     std::swap(f.pos, f.pos2); std::swap(f.vel, f.vel2); std::swap(f.pid, f.pid2);
@@ -268,8 +108,9 @@ void launch_collide_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, Mem
 
 // ---- streaming ------------------------------------------------------------------
 // free flight, walls and wrap in float (maincode.cpp:516-560); particles in
-// cells with triangles are queued for the double-precision kernel
+// cells with triangles are handed to k_stream_cells<true> (double precision)
 __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const int* __restrict__ lstart,
+                                                  const int* __restrict__ lrank, int* bcnt, int* bucket,
                                                   int* queue, int* qn) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= f.n) return;
@@ -279,13 +120,9 @@ __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const
   int fy = (int)floorf(bbound(q.y, Ly));
   int fz = (int)floorf(q.z + 1.0f);
   int pid = cell_of(p, fx, fy, fz);
-  if (__ldg(lstart + pid + 1) > __ldg(lstart + pid)) {
-    unsigned mk = __activemask();
-    int leader = __ffs(mk) - 1, lane = threadIdx.x & 31;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(qn, __popc(mk));
-    base = __shfl_sync(mk, base, leader);
-    queue[base + __popc(mk & ((1u << lane) - 1))] = (int)i;
+  const int l0 = __ldg(lstart + pid), l1 = __ldg(lstart + pid + 1);
+  if (l1 > l0) {
+    hand_off(lrank, pid, (int)i, bcnt, bucket, queue, qn);
     return;
   }
   float X = q.x + v.x * dt, Y = q.y + v.y * dt, Z = q.z + v.z * dt;
@@ -306,40 +143,16 @@ __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const
   f.pos[i] = make_float4(X, Y, Z, q.w);
 }
 
-// near the membrane: promote to double and run the FP64 warp kernel logic
-__global__ void __launch_bounds__(256) k_stream_heavy_f(DevParams p, SolventF f, const int* __restrict__ lstart,
-                                                        const int* __restrict__ lidx, Snap sn,
-                                                        const TriPre* __restrict__ pre, const int* queue,
-                                                        const int* qn) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int nq = *qn;
-  for (int64_t q = w; q < nq; q += nw) {
-    const int64_t i = queue[q];
-    float4 q4 = f.pos[i], v4 = f.vel[i];
-    double X = q4.x, Y = q4.y, Z = q4.z, VX = v4.x, VY = v4.y, VZ = v4.z;
-    const int indio = __float_as_int(q4.w);
-    int fx = (int)floor(bbound(X, p.Lx));
-    int fy = (int)floor(bbound(Y, p.Ly));
-    int fz = (int)floor(Z + 1.0);
-    int pid = cell_of(p, fx, fy, fz);
-    const int l0 = lstart[pid], l1 = lstart[pid + 1];
-    double fulldt = 0.0;
-    stream_heavy_walk(p, sn, pre, lidx, l0, l1, lane, indio, X, Y, Z, VX, VY, VZ, fulldt);
-    if (lane == 0) {
-      finish_stream(p, fulldt, X, Y, Z, VX, VY, VZ);
-      f.pos[i] = make_float4((float)X, (float)Y, (float)Z, q4.w);
-      f.vel[i] = make_float4((float)VX, (float)VY, (float)VZ, v4.w);
-    }
-  }
-}
-
-void fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb, int buf, cudaStream_t st) {
+void fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb, int buf, cudaStream_t st,
+                   cudaEvent_t ev0, cudaEvent_t ev1) {
   cudaMemsetAsync(fb.qn, 0, sizeof(int), st);
   if (f.n) {
-    k_stream_f<<<nbf(f.n, 256), 256, 0, st>>>(p, f, c.lstart, fb.queue, fb.qn);
-    k_stream_heavy_f<<<148 * 4, 256, 0, st>>>(p, f, c.lstart, c.lidx, fb.snap[buf], fb.pre[buf], fb.queue, fb.qn);
+    if (ev0) cudaEventRecord(ev0, st);
+    k_stream_f<<<nbf(f.n, 256), 256, 0, st>>>(p, f, c.lstart, c.lrank, fb.bcnt, fb.bucket, fb.queue, fb.qn);
+    if (ev1) cudaEventRecord(ev1, st);
+    Solvent none;
+    none.n = f.n;
+    launch_stream_cells<true>(p, none, f, c, fb, buf, st);
   }
 }
 

@@ -7,6 +7,7 @@
 // exp, log) elsewhere.
 #include <cstdio>
 #include "sim.h"
+#include "cells_tile.cuh"
 
 namespace irbc {
 
@@ -23,16 +24,43 @@ __global__ void k_init_solvent(DevParams p, Solvent s) {
   s.x[i] = (p.Lx * draw_uniform(p.seed, STREAM_INIT, 0, b + 0));
   s.y[i] = (p.Ly * draw_uniform(p.seed, STREAM_INIT, 0, b + 1));
   s.z[i] = (p.Lz * draw_uniform(p.seed, STREAM_INIT, 0, b + 2));
-  s.vx[i] = -vmax + 2.0 * vmax * draw_uniform(p.seed, STREAM_INIT, 0, b + 3);
-  s.vy[i] = -vmax + 2.0 * vmax * draw_uniform(p.seed, STREAM_INIT, 0, b + 4);
-  s.vz[i] = -vmax + 2.0 * vmax * draw_uniform(p.seed, STREAM_INIT, 0, b + 5);
-  s.id[i] = (int)i;
+  SolVel r;
+  r.vx = -vmax + 2.0 * vmax * draw_uniform(p.seed, STREAM_INIT, 0, b + 3);
+  r.vy = -vmax + 2.0 * vmax * draw_uniform(p.seed, STREAM_INIT, 0, b + 4);
+  r.vz = -vmax + 2.0 * vmax * draw_uniform(p.seed, STREAM_INIT, 0, b + 5);
+  r.id = (int)i;
+  r.pad = 0;
+  s.v[i] = r;
   s.indio[i] = 1;
   s.pid[i] = 0;
 }
 
 void launch_init_solvent(const DevParams& p, Solvent& s, cudaStream_t st) {
   if (s.n) k_init_solvent<<<nblk(s.n, 256), 256, 0, st>>>(p, s);
+}
+
+__global__ void k_pack_vel(Solvent s, const double* vx, const double* vy, const double* vz, const int* id) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  SolVel r = s.v[i];
+  if (vx) { r.vx = vx[i]; r.vy = vy[i]; r.vz = vz[i]; }
+  if (id) r.id = id[i];
+  r.pad = 0;
+  s.v[i] = r;
+}
+__global__ void k_unpack_vel(Solvent s, double* vx, double* vy, double* vz, int* id) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const SolVel r = s.v[i];
+  if (vx) { vx[i] = r.vx; vy[i] = r.vy; vz[i] = r.vz; }
+  if (id) id[i] = r.id;
+}
+void launch_pack_vel(Solvent& s, const double* vx, const double* vy, const double* vz, const int* id,
+                     cudaStream_t st) {
+  if (s.n) k_pack_vel<<<nblk(s.n, 256), 256, 0, st>>>(s, vx, vy, vz, id);
+}
+void launch_unpack_vel(const Solvent& s, double* vx, double* vy, double* vz, int* id, cudaStream_t st) {
+  if (s.n) k_unpack_vel<<<nblk(s.n, 256), 256, 0, st>>>(s, vx, vy, vz, id);
 }
 
 // inside/outside ray test, sortsolvent_initial1 (Src/solfuncs.cpp:31-94).
@@ -232,9 +260,9 @@ void launch_scan3(const int* a, const int* b, const int* c, int* oa, int* ob, in
 
 // ============================================================== collide =====
 // CollisionStep (Src/solfuncs.cpp:109-323) as: vertex binning + shift,
-// counting sort of the solvent (count -> scan -> scatter), one thread per
-// cell for the cell statistics in reference order, one thread per particle
-// for the rotation (CollisionDyn, :700-736).
+// counting sort of the solvent (count -> scan -> scatter), then one warp per
+// tile of 32 cells for the cell statistics in reference order and the
+// rotation (CollisionDyn, :700-736; cells_tile.cuh).
 
 __device__ __forceinline__ void grid_shift(const DevParams& p, uint64_t epoch, double r[3]) {
   uint32_t o[4];
@@ -343,198 +371,15 @@ __global__ void k_gather(Solvent s) {
   if (j >= s.n) return;
   const int i = s.perm[j];
   s.x2[j] = s.x[i]; s.y2[j] = s.y[i]; s.z2[j] = s.z[i];
-  s.vx2[j] = s.vx[i]; s.vy2[j] = s.vy[i]; s.vz2[j] = s.vz[i];
-  s.id2[j] = s.id[i]; s.indio2[j] = s.indio[i]; s.pid2[j] = s.pid[i];
+  s.v2[j] = s.v[i];
+  s.indio2[j] = s.indio[i]; s.pid2[j] = s.pid[i];
 }
 
-__device__ __forceinline__ double gauss(const DevParams& p, uint64_t epoch, uint64_t k, double m, double sd) {
-  return draw_normal(p.seed, STREAM_COLLIDE_N, epoch, k) * sd + m;
-}
-
-__device__ __forceinline__ void rotate_v(double v[3], const double* P, double cosalpha, double sinalpha) {
-  // CollisionDyn (:711-733) with the cell's vcm (P[0..2]), axis (P[3..5]), ThE (P[6])
-  double unit[3] = {P[3], P[4], P[5]}, dvv[3], dvp[3], dvn[3], dvpn[3];
-  double scalev = P[6];
-  for (int k = 0; k < 3; ++k) dvv[k] = v[k] - P[k];
-  double xxx = dvv[0] * unit[0] + dvv[1] * unit[1] + dvv[2] * unit[2];
-  for (int k = 0; k < 3; ++k) dvp[k] = xxx * unit[k];
-  for (int k = 0; k < 3; ++k) dvn[k] = dvv[k] - dvp[k];
-  cp(dvn, unit, dvpn);
-  for (int k = 0; k < 3; ++k) v[k] = P[k] + scalev * (cosalpha * dvn[k] + sinalpha * dvpn[k] + dvp[k]);
-}
-
-constexpr int kMaxSeg = 48;
-
-// one thread per cell: momentum, ghosts, vcm, axis, relative energy, ThE in
-// the reference's order (solvent in particle order, wall ghost, vertices in
-// vertex order, parasite, membrane ghost); rotates the cell's vertices and
-// the parasite
-__global__ void k_cells(DevParams p, Solvent s, Cells cl, Membrane m, uint64_t epoch) {
-  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= p.ncell) return;
-  const int64_t s0 = cl.start[c];
-  const int n = cl.start[c + 1] - (int)s0;
-  // the cell's particles are perm[s0 .. s0+n); order them by reference
-  // index (the order of Cells[].sol)
-  const int* __restrict__ PP = s.perm + s0;
-  int ord[kMaxSeg], oid[kMaxSeg];
-  const bool small = n <= kMaxSeg;
-  if (small) {
-    for (int q = 0; q < n; ++q) {
-      int pq = PP[q];
-      int idq = s.id[pq];
-      int r = q;
-      while (r > 0 && oid[r - 1] > idq) { ord[r] = ord[r - 1]; oid[r] = oid[r - 1]; --r; }
-      ord[r] = pq;
-      oid[r] = idq;
-    }
-  }
-  auto nth = [&](int q) -> int64_t {
-    if (small) return ord[q];
-    // large cell: q-th smallest id by selection (rare)
-    int last = -1;
-    int64_t at = PP[0];
-    for (int t = 0; t <= q; ++t) {
-      int best = 0x7fffffff;
-      for (int u = 0; u < n; ++u) {
-        int v = s.id[PP[u]];
-        if (v > last && v < best) { best = v; at = PP[u]; }
-      }
-      last = best;
-    }
-    return at;
-  };
-  const MemScalars* sc = m.sc;
-  double vcm[3] = {0.0, 0.0, 0.0}, ncc = 0.0;
-  int nc = 0;
-  for (int q = 0; q < n; ++q) {
-    int64_t pi = nth(q);
-    vcm[0] += p.mass * s.vx[pi];
-    vcm[1] += p.mass * s.vy[pi];
-    vcm[2] += p.mass * s.vz[pi];
-    ncc += (1 * p.mass);
-    nc += 1;
-  }
-  const int k = (int)(c % p.nz);
-  const double zmin = -1.0 + (double)k * p.a, zmax = -1.0 + (double)k * p.a + p.a;
-  {
-    int nn = nc;
-    uint64_t g = 3 * (uint64_t)cl.wrank[c];
-    if (zmax >= p.Lz) {
-      if (nn < p.navg) {
-        vcm[0] += p.mass * gauss(p, epoch, g + 0, (p.navg - nn) * p.wallspeed, sqrt((p.navg - nn) * p.Theta / p.mass));
-        vcm[1] += p.mass * gauss(p, epoch, g + 1, 0, sqrt((p.navg - nn) * p.Theta / p.mass));
-        vcm[2] += p.mass * gauss(p, epoch, g + 2, 0, sqrt((p.navg - nn) * p.Theta / p.mass));
-        ncc = p.navg * p.mass;
-      }
-    } else if (zmin <= 0) {
-      if (nn < p.navg) {
-        vcm[0] += p.mass * gauss(p, epoch, g + 0, 0, sqrt((p.navg - nn) * p.Theta / p.mass));
-        vcm[1] += p.mass * gauss(p, epoch, g + 1, 0, sqrt((p.navg - nn) * p.Theta / p.mass));
-        vcm[2] += p.mass * gauss(p, epoch, g + 2, 0, sqrt((p.navg - nn) * p.Theta / p.mass));
-        ncc = p.navg * p.mass;
-      }
-    }
-  }
-  // vertices of this cell: range in the sorted keys
-  const int nmem = cl.ncm[c];
-  int v0 = 0;
-  if (nmem > 0) {
-    int lo = 0, hi = p.nv;
-    const uint64_t key0 = (uint64_t)(uint32_t)c << 32;
-    while (lo < hi) { int mid = (lo + hi) >> 1; if (m.vkey[mid] < key0) lo = mid + 1; else hi = mid; }
-    v0 = lo;
-    for (int q = 0; q < nmem; ++q) {
-      int i = (int)(m.vkey[v0 + q] & 0xffffffffu);
-      vcm[0] += p.pmass * m.vx[i];
-      vcm[1] += p.pmass * m.vy[i];
-      vcm[2] += p.pmass * m.vz[i];
-      ncc += (1 * p.pmass);
-      nc += 1;
-    }
-  }
-  const bool has_para = (c == sc->paraid);
-  if (has_para) {
-    vcm[0] += p.PRmass * sc->paraV[0];
-    vcm[1] += p.PRmass * sc->paraV[1];
-    vcm[2] += p.PRmass * sc->paraV[2];
-    ncc += (1 * p.PRmass);
-    nc += 1;
-  }
-  {
-    int nn = nc;
-    if ((nn < p.navg) && (nmem > 0)) {
-      uint64_t g = 3 * ((uint64_t)cl.totals[1] + (uint64_t)cl.mrank[c]);
-      vcm[0] += p.mass * gauss(p, epoch, g + 0, 0, sqrt((p.navg - nn) * p.Theta / p.mass));
-      vcm[1] += p.mass * gauss(p, epoch, g + 1, 0, sqrt((p.navg - nn) * p.Theta / p.mass));
-      vcm[2] += p.mass * gauss(p, epoch, g + 2, 0, sqrt((p.navg - nn) * p.Theta / p.mass));
-      ncc += (p.navg - nn) * p.mass;
-    }
-  }
-  {
-    int nn = (int)ncc;
-    if (nn != 0) { vcm[0] /= (double)nn; vcm[1] /= (double)nn; vcm[2] /= (double)nn; }
-  }
-  // axis (:262-271): draws 3+2c and 4+2c of the COLLIDE_U stream
-  const double rand1 = 2.0 * p.Pi * draw_uniform(p.seed, STREAM_COLLIDE_U, epoch, 3 + 2 * (uint64_t)c);
-  const double rand2 = -1.0 + (2.0 * draw_uniform(p.seed, STREAM_COLLIDE_U, epoch, 4 + 2 * (uint64_t)c));
-  double dvv = 0.0;
-  for (int q = 0; q < n; ++q) {
-    int64_t pi = nth(q);
-    double A0 = s.vx[pi] - vcm[0], A1 = s.vy[pi] - vcm[1], A2 = s.vz[pi] - vcm[2];
-    double aa = (A0 * A0 + A1 * A1 + A2 * A2);
-    dvv += (p.mass * aa);
-  }
-  for (int q = 0; q < nmem; ++q) {
-    int i = (int)(m.vkey[v0 + q] & 0xffffffffu);
-    double A0 = m.vx[i] - vcm[0], A1 = m.vy[i] - vcm[1], A2 = m.vz[i] - vcm[2];
-    double aa = (A0 * A0 + A1 * A1 + A2 * A2);
-    dvv += (p.pmass * aa);
-  }
-  if (has_para) {
-    double A0 = sc->paraV[0] - vcm[0], A1 = sc->paraV[1] - vcm[1], A2 = sc->paraV[2] - vcm[2];
-    double aa = (A0 * A0 + A1 * A1 + A2 * A2);
-    dvv += (p.PRmass * aa);
-  }
-  double ThE = 1.0;
-  if ((nc > 0) && (dvv != 0)) ThE = sqrt(3.0 * ((double)nc - 1.0) * p.Theta / (dvv));
-  double P[7];
-  P[0] = vcm[0]; P[1] = vcm[1]; P[2] = vcm[2];
-  P[3] = sqrt(1.0 - (rand2 * rand2)) * cos(rand1);
-  P[4] = sqrt(1.0 - (rand2 * rand2)) * sin(rand1);
-  P[5] = rand2;
-  P[6] = ThE;
-  for (int q = 0; q < 7; ++q) cl.par[c * 7 + q] = P[q];
-  // CollisionDynmem (:739-776) and CollisionDynpara (:779-810)
-  for (int q = 0; q < nmem; ++q) {
-    int i = (int)(m.vkey[v0 + q] & 0xffffffffu);
-    double v[3] = {m.vx[i], m.vy[i], m.vz[i]};
-    rotate_v(v, P, p.cosalpha, p.sinalpha);
-    m.vx[i] = v[0]; m.vy[i] = v[1]; m.vz[i] = v[2];
-  }
-  if (has_para) {
-    MemScalars* scw = m.sc;
-    double v[3] = {scw->paraV[0], scw->paraV[1], scw->paraV[2]};
-    rotate_v(v, P, p.cosalpha, p.sinalpha);
-    scw->paraV[0] = v[0]; scw->paraV[1] = v[1]; scw->paraV[2] = v[2];
-  }
-}
-
-__global__ void k_rotate(DevParams p, Solvent s, const double* par) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.n) return;
-  const double* P = par + (int64_t)s.pid[i] * 7;
-  double Pl[7];
-  for (int q = 0; q < 7; ++q) Pl[q] = P[q];
-  double v[3] = {s.vx[i], s.vy[i], s.vz[i]};
-  rotate_v(v, Pl, p.cosalpha, p.sinalpha);
-  s.vx[i] = v[0]; s.vy[i] = v[1]; s.vz[i] = v[2];
-}
 
 static void swap_solvent(Solvent& s) {
   std::swap(s.x, s.x2); std::swap(s.y, s.y2); std::swap(s.z, s.z2);
-  std::swap(s.vx, s.vx2); std::swap(s.vy, s.vy2); std::swap(s.vz, s.vz2);
-  std::swap(s.id, s.id2); std::swap(s.indio, s.indio2); std::swap(s.pid, s.pid2);
+  std::swap(s.v, s.v2);
+  std::swap(s.indio, s.indio2); std::swap(s.pid, s.pid2);
 }
 
 void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cudaStream_t st) {
@@ -545,6 +390,7 @@ void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cuda
     cudaFuncSetAttribute(k_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
     attr_set = true;
   }
+  cudaMemsetAsync(c.ncm, 0, sizeof(int) * c.n, st);
   k_vbin<<<1, 1024, sizeof(uint64_t) * n2, st>>>(p, m, c.ncm, epoch);
 }
 
@@ -552,12 +398,13 @@ void launch_ghost_flags(const DevParams& p, Cells& c, const Membrane& m, cudaStr
   k_ghost_flags<<<nblk(c.n, 256), 256, 0, st>>>(p, c.cnt, c.ncm, m.sc, c.wrank, c.mrank);
 }
 
-void launch_collide(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
-                    cudaStream_t st) {
+void launch_collide_count(const DevParams& p, Solvent& s, Cells& c, uint64_t epoch, cudaStream_t st) {
   cudaMemsetAsync(c.cnt, 0, sizeof(int) * c.n, st);
-  cudaMemsetAsync(c.ncm, 0, sizeof(int) * c.n, st);
-  launch_vbin(p, m, c, epoch, st);
   if (s.n) k_count<<<nblk(s.n, 256), 256, 0, st>>>(p, s, c.cnt, epoch);
+}
+
+void launch_collide_finish(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
+                           cudaStream_t st) {
   // wrank/mrank hold the flags first, then their exclusive scans
   k_ghost_flags<<<nblk(c.n, 256), 256, 0, st>>>(p, c.cnt, c.ncm, m.sc, c.wrank, c.mrank);
   launch_scan3(c.cnt, c.wrank, c.mrank, c.start, c.wrank, c.mrank, c.totals, c.n, c.scan_part, st);
@@ -565,8 +412,7 @@ void launch_collide(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint6
   cudaMemcpyAsync(c.start + c.n, c.totals + 0, sizeof(int), cudaMemcpyDeviceToDevice, st);
   if (s.n) k_perm<<<nblk(s.n, 256), 256, 0, st>>>(s.key, s.slot, c.start, s.n, s.perm);
   std::swap(s.pid, s.key);  // pid = cell of this collision, in place
-  k_cells<<<nblk(c.n, 128), 128, 0, st>>>(p, s, c, m, epoch);
-  if (s.n) k_rotate<<<nblk(s.n, 256), 256, 0, st>>>(p, s, c.par);
+  k_cells_tile<false><<<cells_tile_blocks(c.n), 32 * kTileWarps, 0, st>>>(p, s, SolventF{}, c, m, epoch);
   if (s.n && (++s.ncoll % kResortEvery) == 0) {
     k_gather<<<nblk(s.n, 256), 256, 0, st>>>(s);
     swap_solvent(s);
@@ -708,7 +554,8 @@ __device__ double reflection(const DevParams& p, const int* lstart, const int* l
 __global__ void k_stream(DevParams p, Solvent s, const int* lstart, const int* lidx, Membrane m) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.n) return;
-  double X = s.x[i], Y = s.y[i], Z = s.z[i], VX = s.vx[i], VY = s.vy[i], VZ = s.vz[i];
+  const SolVel r = s.v[i];
+  double X = s.x[i], Y = s.y[i], Z = s.z[i], VX = r.vx, VY = r.vy, VZ = r.vz;
   const double VX0 = VX, VY0 = VY, VZ0 = VZ;
   const double dtmd = p.dtmd;
   double fullts = reflection(p, lstart, lidx, m, X, Y, Z, VX, VY, VZ, s.indio[i]);
@@ -736,7 +583,7 @@ __global__ void k_stream(DevParams p, Solvent s, const int* lstart, const int* l
   X = bbound(X, p.Lx);
   Y = bbound(Y, p.Ly);
   s.x[i] = X; s.y[i] = Y; s.z[i] = Z;
-  if (VX != VX0 || VY != VY0 || VZ != VZ0 || VX0 != VX0) { s.vx[i] = VX; s.vy[i] = VY; s.vz[i] = VZ; }
+  if (VX != VX0 || VY != VY0 || VZ != VZ0 || VX0 != VX0) { s.v[i].vx = VX; s.v[i].vy = VY; s.v[i].vz = VZ; }
 }
 
 void launch_stream(const DevParams& p, Solvent& s, const Cells& c, const Membrane& m, cudaStream_t st) {
@@ -757,10 +604,18 @@ __global__ void k_tri_centroid(DevParams p, Membrane m) {
   m.tcz[j] = (m.z[p1] + m.z[p2] + m.z[p3]) / 3.0;
 }
 
+// One block of kLTile consecutive cells per pass; each tile of kLTile
+// centroids is first culled against the block's box of cell centres (a
+// conservative box test with the same minimum-image convention), and the
+// survivors, compacted in index order, get the exact test of :340-350.
 constexpr int kLTile = 256;
 template <bool FILL>
-__global__ void k_llist(DevParams p, Cells cl, Membrane m) {
+__global__ void __launch_bounds__(kLTile) k_llist(DevParams p, Cells cl, Membrane m) {
   __shared__ double tc[3][kLTile];
+  __shared__ int tj[kLTile];
+  __shared__ double red[6][kLTile / 32];
+  __shared__ int wcnt[kLTile / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = c < p.ncell;
   double cellx = 0, celly = 0, cellz = 0;
@@ -771,19 +626,52 @@ __global__ void k_llist(DevParams p, Cells cl, Membrane m) {
     double zmin = -1.0 + (double)k * p.a, zmax = -1.0 + (double)k * p.a + p.a;
     cellx = (xmin + xmax) * 0.5; celly = (ymin + ymax) * 0.5; cellz = (zmin + zmax) * 0.5;
   }
+  // the block's box of cell centres: min of (x, y, z, -x, -y, -z)
+  double bb[6] = {act ? cellx : 1e300, act ? celly : 1e300, act ? cellz : 1e300,
+                  act ? -cellx : 1e300, act ? -celly : 1e300, act ? -cellz : 1e300};
+  for (int o = 16; o > 0; o >>= 1)
+    for (int e = 0; e < 6; ++e) bb[e] = fmin(bb[e], __shfl_xor_sync(0xffffffffu, bb[e], o));
+  if (lane == 0)
+    for (int e = 0; e < 6; ++e) red[e][w] = bb[e];
+  __syncthreads();
+  for (int e = 0; e < 6; ++e) {
+    double v = red[e][0];
+    for (int u = 1; u < kLTile / 32; ++u) v = fmin(v, red[e][u]);
+    bb[e] = v;
+  }
+  const double xm = 0.5 * (bb[0] - bb[3]), hx = 0.5 * (-bb[3] - bb[0]);
+  const double ym = 0.5 * (bb[1] - bb[4]), hy = 0.5 * (-bb[4] - bb[1]);
+  const double zm = 0.5 * (bb[2] - bb[5]), hz = 0.5 * (-bb[5] - bb[2]);
+  const double reach = 2.0 * p.a + 1e-6;
   int count = 0;
   int old_n = act ? cl.lstart[c + 1] - cl.lstart[c] : 0;
   int64_t out0 = (FILL && act) ? cl.lstart2[c] : 0;
   const double lim = 4.0 * p.a * p.a;
   for (int t0 = 0; t0 < p.nt; t0 += kLTile) {
-    int nt = min(kLTile, p.nt - t0);
+    const int nt = min(kLTile, p.nt - t0);
+    bool keep = false;
+    double tx = 0, ty = 0, tz = 0;
+    if ((int)threadIdx.x < nt) {
+      tx = m.tcx[t0 + threadIdx.x]; ty = m.tcy[t0 + threadIdx.x]; tz = m.tcz[t0 + threadIdx.x];
+      double dx = tx - xm, dy = ty - ym;
+      dx -= p.Lx * round(dx / p.Lx);
+      dy -= p.Ly * round(dy / p.Ly);
+      keep = (fabs(dx) - hx < reach) && (fabs(dy) - hy < reach) && (fabs(tz - zm) - hz < reach);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    __syncthreads();  // the previous tile's survivors are consumed
+    if (lane == 0) wcnt[w] = __popc(bal);
     __syncthreads();
-    for (int q = threadIdx.x; q < nt; q += blockDim.x) {
-      tc[0][q] = m.tcx[t0 + q]; tc[1][q] = m.tcy[t0 + q]; tc[2][q] = m.tcz[t0 + q];
+    int off = 0, K = 0;
+    for (int u = 0; u < kLTile / 32; ++u) { const int cu = wcnt[u]; off += (u < w) ? cu : 0; K += cu; }
+    if (keep) {
+      const int pos = off + __popc(bal & ((1u << lane) - 1));
+      tc[0][pos] = tx; tc[1][pos] = ty; tc[2][pos] = tz;
+      tj[pos] = t0 + threadIdx.x;
     }
     __syncthreads();
     if (act) {
-      for (int q = 0; q < nt; ++q) {
+      for (int q = 0; q < K; ++q) {
         double xxx1 = tc[0][q] - cellx;
         double yyy1 = tc[1][q] - celly;
         xxx1 -= p.Lx * round(xxx1 / p.Lx);
@@ -791,7 +679,7 @@ __global__ void k_llist(DevParams p, Cells cl, Membrane m) {
         double zzz = fabs(tc[2][q] - cellz);
         double A1aa = xxx1 * xxx1 + yyy1 * yyy1 + zzz * zzz;
         if (A1aa < lim) {
-          if (FILL) cl.lidx2[out0 + count] = t0 + q;
+          if (FILL) cl.lidx2[out0 + count] = tj[q];
           count += 1;
         }
       }
@@ -808,7 +696,7 @@ __global__ void k_llist(DevParams p, Cells cl, Membrane m) {
 
 int64_t launch_llist_count(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st) {
   k_tri_centroid<<<nblk(p.nt, 128), 128, 0, st>>>(p, m);
-  k_llist<false><<<nblk(c.n, 256), 256, 0, st>>>(p, c, m);
+  k_llist<false><<<nblk(c.n, kLTile), kLTile, 0, st>>>(p, c, m);
   launch_scan3(c.lcnt, nullptr, nullptr, c.lstart2, nullptr, nullptr, c.totals + 3, c.n, c.scan_part, st);
   int tot = 0;
   cudaMemcpyAsync(&tot, c.totals + 3, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -818,10 +706,37 @@ int64_t launch_llist_count(const DevParams& p, Cells& c, const Membrane& m, cuda
 }
 
 void launch_llist_fill(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st) {
-  k_llist<true><<<nblk(c.n, 256), 256, 0, st>>>(p, c, m);
+  k_llist<true><<<nblk(c.n, kLTile), kLTile, 0, st>>>(p, c, m);
   std::swap(c.lstart, c.lstart2);
   std::swap(c.lidx, c.lidx2);
   std::swap(c.lcap, c.lcap2);
+}
+
+// cells with a non-empty list: their rank (lrank), the cell of each rank
+// (acell), their number and the longest list (host copies nact, lmax)
+__global__ void k_lflags(DevParams p, Cells cl) {
+  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.ncell) return;
+  const int len = cl.lstart[c + 1] - cl.lstart[c];
+  cl.lrank[c] = len > 0 ? 1 : 0;
+  if (len > 0) atomicMax(cl.totals + 7, len);
+}
+__global__ void k_acell(DevParams p, Cells cl) {
+  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.ncell) return;
+  if (cl.lstart[c + 1] > cl.lstart[c]) cl.acell[cl.lrank[c]] = (int)c;
+}
+int launch_llist_ranks(const DevParams& p, Cells& c, cudaStream_t st) {
+  cudaMemsetAsync(c.totals + 7, 0, sizeof(int), st);
+  k_lflags<<<nblk(c.n, 256), 256, 0, st>>>(p, c);
+  launch_scan3(c.lrank, nullptr, nullptr, c.lrank, nullptr, nullptr, c.totals + 4, c.n, c.scan_part, st);
+  k_acell<<<nblk(c.n, 256), 256, 0, st>>>(p, c);
+  int h[4] = {0, 0, 0, 0};
+  cudaMemcpyAsync(h, c.totals + 4, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return -1;
+  c.nact = h[0];
+  c.lmax = h[3];
+  return 5;
 }
 
 // ============================================================ membrane =====
@@ -1231,7 +1146,8 @@ __global__ void k_obs_solvent(DevParams p, Solvent s, double* out, double* prof,
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0, vxs = 0;
   if (i < s.n) {
-    double vx = s.vx[i], vy = s.vy[i], vz = s.vz[i];
+    const SolVel r = s.v[i];
+    double vx = r.vx, vy = r.vy, vz = r.vz;
     e = p.mass * (vx * vx + vy * vy + vz * vz);
     vxs = vx;
     if (prof) {

@@ -1,10 +1,10 @@
 // sim.h -- device-resident state of one simulation and the launchers of the
 // kernels that advance it.  Layout in HBM (FP64 build):
-//   solvent    SoA double x,y,z,vx,vy,vz + int id (reference index),
-//              indio, pid; kept physically sorted by collision cell (the
-//              counting sort of each collision writes the second buffer set)
+//   solvent    SoA double x,y,z; one 32-byte record (vx, vy, vz, reference
+//              index) per particle; int indio, pid; re-sorted physically by
+//              collision cell every kResortEvery collisions (second buffer set)
 //   cells      int cnt, start (exclusive scan), ncm (membrane vertices),
-//              ghost ranks; 7 doubles of collision parameters per cell
+//              ghost ranks
 //   llist      CSR lstart[C+1], lidx[cap], double-buffered
 //   membrane   SoA vertex arrays, topology, per-vertex incidence lists
 #pragma once
@@ -14,12 +14,22 @@
 
 namespace irbc {
 
+// velocity and reference index of a solvent particle in one 32-byte record:
+// the collision, which visits particles in cell order, reads and writes one
+// sector per particle
+struct __align__(16) SolVel {
+  double vx, vy, vz;
+  int id, pad;
+};
+
 struct Solvent {
   int64_t n = 0;
-  double *x = nullptr, *y = nullptr, *z = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
-  int *id = nullptr, *indio = nullptr, *pid = nullptr;
-  double *x2 = nullptr, *y2 = nullptr, *z2 = nullptr, *vx2 = nullptr, *vy2 = nullptr, *vz2 = nullptr;
-  int *id2 = nullptr, *indio2 = nullptr, *pid2 = nullptr;
+  double *x = nullptr, *y = nullptr, *z = nullptr;
+  SolVel* v = nullptr;
+  int *indio = nullptr, *pid = nullptr;
+  double *x2 = nullptr, *y2 = nullptr, *z2 = nullptr;
+  SolVel* v2 = nullptr;
+  int *indio2 = nullptr, *pid2 = nullptr;
   int *key = nullptr, *slot = nullptr;
   int *perm = nullptr;          // particle indices grouped by collision cell
   int64_t ncoll = 0;            // collisions so far (physical re-sort cadence)
@@ -32,11 +42,13 @@ constexpr int kResortEvery = 16;
 struct Cells {
   int64_t n = 0;
   int *cnt = nullptr, *start = nullptr, *ncm = nullptr, *wrank = nullptr, *mrank = nullptr;
-  int *totals = nullptr;        // [0] particles, [1] wall ghost cells, [2] membrane ghost cells, [3] llist entries
-  double *par = nullptr;        // 7 per cell: vcm[3], unit[3], ThE
-  float *parf = nullptr;        // the same as 8 floats per cell (FP32 solvent)
+  int *totals = nullptr;        // [0] particles, [1] wall ghost cells, [2] membrane ghost cells, [3] llist
+                                // entries, [4] cells with a list, [7] longest list
   int *lstart = nullptr, *lidx = nullptr, *lstart2 = nullptr, *lidx2 = nullptr, *lcnt = nullptr;
   int64_t lcap = 0, lcap2 = 0;
+  int *lrank = nullptr;         // rank among the cells with a non-empty list
+  int *acell = nullptr;         // the cell of each such rank
+  int nact = 0, lmax = 0;       // (host) their number and the longest list
   int *scan_part = nullptr;     // scan scratch: 3 ints per block
   int64_t scan_blocks = 0;
 };
@@ -72,15 +84,26 @@ constexpr int kMaxPairs = 64;        // bond candidates per vertex (<= 25 with d
 
 // ---- launchers (kernels.cu) ---------------------------------------------------
 void launch_init_solvent(const DevParams& p, Solvent& s, cudaStream_t st);
+// velocity records from / to plain arrays (state exchange); a null vx keeps
+// the velocities, a null id keeps the indices
+void launch_pack_vel(Solvent& s, const double* vx, const double* vy, const double* vz, const int* id,
+                     cudaStream_t st);
+void launch_unpack_vel(const Solvent& s, double* vx, double* vy, double* vz, int* id, cudaStream_t st);
 void launch_classify(const DevParams& p, Solvent& s, const Membrane& m, cudaStream_t st);
-void launch_collide(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
-                    cudaStream_t st);
+// a collision = launch_vbin (membrane only) + launch_collide_count (solvent
+// only) in any order or on two streams, then launch_collide_finish
 void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cudaStream_t st);
+void launch_collide_count(const DevParams& p, Solvent& s, Cells& c, uint64_t epoch, cudaStream_t st);
+void launch_collide_finish(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
+                           cudaStream_t st);
 void launch_ghost_flags(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
 void launch_stream(const DevParams& p, Solvent& s, const Cells& c, const Membrane& m, cudaStream_t st);
 // returns the total list length the update needs (host sync inside)
 int64_t launch_llist_count(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
 void launch_llist_fill(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
+// lrank / acell / nact / lmax of the current lists (host sync inside);
+// returns the kernels launched, -1 on a CUDA error
+int launch_llist_ranks(const DevParams& p, Cells& c, cudaStream_t st);
 void launch_half_kick(const DevParams& p, Membrane& m, cudaStream_t st);
 void launch_drift(const DevParams& p, Membrane& m, cudaStream_t st);
 void launch_total_va(const DevParams& p, Membrane& m, cudaStream_t st);

@@ -302,11 +302,11 @@ class Simulation:
 
     def profile_end(self):
         """dict of CUDA-event times (ms) since profile_begin"""
-        out = np.zeros(8)
-        self._ck(self.L.irbc_profile_end(self.h, _p(out, D), 8), "irbc_profile_end")
-        return dict(total_ms=out[0], stream_ms=out[1], stream_launches=int(out[2]), collide_ms=out[3],
+        out = np.zeros(10)
+        self._ck(self.L.irbc_profile_end(self.h, _p(out, D), 10), "irbc_profile_end")
+        return dict(total_ms=out[0], stream_ms=out[1], stream_steps=int(out[2]), collide_ms=out[3],
                     collides=int(out[4]), membrane_ms=out[5], membrane_groups=int(out[6]),
-                    launches=int(out[7]))
+                    launches=int(out[7]), bulk_ms=out[8], bulk_launches=int(out[9]))
 
 
 class PinnedArray:

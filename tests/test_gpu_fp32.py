@@ -80,3 +80,23 @@ def test_fp32_collision_conserves_momentum(base):
     e1 = np.sum(after.a["svx"] ** 2 + after.a["svy"] ** 2 + after.a["svz"] ** 2)
     assert abs(e1 - e0) / e0 < 0.05
     assert bulk.sum() > 0.8 * st.ns
+
+
+def test_fp32_long_run_stays_physical(base):
+    """800 steps (list updates and collisions included) in FP32 beside the
+    same run in FP64: every particle stays finite and inside the box, and
+    the solvent temperature and membrane area agree to a few percent."""
+    op, mesh, st = base
+    o = _fresh(op, mesh, st)
+    f32 = H.gpu_like(op, o, 41, precision=1, state=st)
+    f64 = H.gpu_like(op, o, 41, precision=0, state=st)
+    f32.step(800)
+    f64.step(800)
+    g, r = f32.get_state(), f64.get_state()
+    for k, L in (("sx", op.Lx), ("sy", op.Ly), ("sz", op.Lz)):
+        assert np.isfinite(g.a[k]).all(), k
+        assert g.a[k].min() >= -1e-3 and g.a[k].max() <= L + 1e-3, k
+    v2g = np.mean(g.a["svx"] ** 2 + g.a["svy"] ** 2 + g.a["svz"] ** 2)
+    v2r = np.mean(r.a["svx"] ** 2 + r.a["svy"] ** 2 + r.a["svz"] ** 2)
+    assert np.isfinite(v2g) and abs(v2g - v2r) / v2r < 0.05
+    assert abs(g.s["Sarea"] - r.s["Sarea"]) / r.s["Sarea"] < 0.02

@@ -61,6 +61,45 @@ def test_phase_matches_oracle(base, phase):
     assert bad == {}, (phase, bad)
 
 
+def test_stream_crowded_cell_and_long_list(base):
+    """Near-membrane streaming off its usual path: 80 particles crowded into
+    one listed cell (more than a cell's bucket takes, so most go to the
+    overflow queue), and a second cell whose list is padded to 1500 entries
+    with repeats; both must follow the reference's sequential triangle walk."""
+    op, mesh, st = base
+    st2 = st.copy()
+    off, lidx = st2.llists()
+    llen = st2.a["llen"]
+    nz = int(op.Lz / op.a) + 1
+    ny = int(op.Ly / op.a)
+    listed = np.nonzero(llen > 0)[0]
+    assert listed.size >= 2
+    c1, c2 = int(listed[listed.size // 3]), int(listed[2 * listed.size // 3])
+    rng = np.random.default_rng(3)
+
+    def crowd(c, idx):
+        i, j, k = c // (ny * nz), (c // nz) % ny, c % nz
+        n = idx.size
+        st2.a["sx"][idx] = (i + rng.uniform(0.05, 0.95, n)) * op.a
+        st2.a["sy"][idx] = (j + rng.uniform(0.05, 0.95, n)) * op.a
+        st2.a["sz"][idx] = (k - 1 + rng.uniform(0.05, 0.95, n)) * op.a
+
+    crowd(c1, np.arange(0, 80))
+    crowd(c2, np.arange(80, 100))
+    # pad c2's list with repeats of its own entries to 1500
+    lists = [lidx[off[c]:off[c + 1]] for c in range(st2.ncell)]
+    own = lists[c2]
+    lists[c2] = np.resize(own, 1500)
+    st2.a["llen"] = np.array([x.size for x in lists], np.int32)
+    st2.a["lidx"] = np.concatenate(lists).astype(np.int32)
+    o = fresh_oracle(op, mesh, st2)
+    sim = H.gpu_like(op, o, 11, state=st2)
+    sim.call("stream")
+    o.stream()
+    bad = H.compare(sim.get_state(), o.get_state(), RTOL)
+    assert bad == {}, bad
+
+
 def test_collide_counts_every_particle_once(base):
     op, mesh, st = base
     o = fresh_oracle(op, mesh, st)
