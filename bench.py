@@ -207,9 +207,10 @@ def run_ours(args):
     value = ns * args.steps * world / (t_ms * 1e-3)
     # roofline of the dominant kernel, the bulk streaming kernel (one launch
     # per step over every particle): algorithmic bytes per particle = state
-    # read + positions written (FP64: 6 x 8 read + 3 x 8 written; FP32: two
-    # float4 read + one written), divided by its CUDA-event time per launch
-    bpp = 72 if precision == G.FP64 else 48
+    # read + positions written (FP64: positions 3 x 8 and the 32-byte
+    # velocity record read, 3 x 8 written; FP32: two float4 read, one
+    # written), divided by its CUDA-event time per launch
+    bpp = 80 if precision == G.FP64 else 48
     bulk_avg_ms = prof["bulk_ms"] / max(1, prof["bulk_launches"])
     achieved = ns * bpp / (bulk_avg_ms * 1e-3) / 1e9
     peak, kind = peaks()

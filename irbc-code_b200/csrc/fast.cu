@@ -65,7 +65,7 @@ __device__ __forceinline__ bool tri_visit(const DevParams& p, const Snap& sn, co
   const double solvx = X_ + 0 * Lx, solvy = Y_ + 0 * Ly, solvz = Z_;
   double bt, bdt;
   double v1x, v1y, v1z, v2x, v2y, v2z, v3x, v3y, v3z;
-  int p1 = sn.t1[jj], p2 = sn.t2[jj], p3 = sn.t3[jj];
+  int p1, p2, p3;
   if (use_pre) {
     double PSt0 = solvx - q.A1[0], PSt1 = solvy - q.A1[1], PSt2 = solvz - q.A1[2];
     double PD0 = (solvx + VX * (dtmd - rstep)) - q.A2[0];
@@ -76,12 +76,15 @@ __device__ __forceinline__ bool tri_visit(const DevParams& p, const Snap& sn, co
     if ((indio == 1) && (bt < 0)) flg = 1;
     if ((indio == 0) && (bt > 0)) flg = 1;
     if (!((bt * bdt <= 0) && (flg == 0))) return false;
+    // the corners are read only for a crossing candidate
+    p1 = sn.t1[jj]; p2 = sn.t2[jj]; p3 = sn.t3[jj];
     v1x = q.A1[0]; v1y = q.A1[1]; v1z = q.A1[2];
     v2x = (sn.x[p2] + 0 * Lx) + sn.vx[p2] * rstep; v2y = (sn.y[p2] + 0 * Ly) + sn.vy[p2] * rstep;
     v2z = sn.z[p2] + sn.vz[p2] * rstep;
     v3x = (sn.x[p3] + 0 * Lx) + sn.vx[p3] * rstep; v3y = (sn.y[p3] + 0 * Ly) + sn.vy[p3] * rstep;
     v3z = sn.z[p3] + sn.vz[p3] * rstep;
   } else {
+    p1 = sn.t1[jj]; p2 = sn.t2[jj]; p3 = sn.t3[jj];
     v1x = (sn.x[p1] + 0 * Lx) + sn.vx[p1] * rstep; v1y = (sn.y[p1] + 0 * Ly) + sn.vy[p1] * rstep;
     v1z = sn.z[p1] + sn.vz[p1] * rstep;
     v2x = (sn.x[p2] + 0 * Lx) + sn.vx[p2] * rstep; v2y = (sn.y[p2] + 0 * Ly) + sn.vy[p2] * rstep;
@@ -204,13 +207,16 @@ __device__ __forceinline__ bool in_stencil(const DevParams& p, double x, double 
 }
 
 // hand-off of a particle whose cell has triangles: into the bucket of its
-// cell (rank lrank among the listed cells) when the bucket has room, else
-// onto the overflow queue
-__device__ __forceinline__ void hand_off(const int* __restrict__ lrank, int pid, int i, int* bcnt, int* bucket,
-                                         int* queue, int* qn) {
-  const int a = lrank[pid];
-  const int slot = atomicAdd(bcnt + a, 1);
-  if (slot < kBucket) { bucket[(int64_t)a * kBucket + slot] = i; return; }
+// cell (rank lrank among the listed cells) when the list fits the shared
+// staging of k_stream_cells and the bucket has room, else onto the overflow
+// queue
+__device__ __forceinline__ void hand_off(const int* __restrict__ lrank, int pid, int len, int i, int* bcnt,
+                                         int* bucket, int* queue, int* qn) {
+  if (len <= kHeavyList) {
+    const int a = lrank[pid];
+    const int slot = atomicAdd(bcnt + a, 1);
+    if (slot < kBucket) { bucket[(int64_t)a * kBucket + slot] = i; return; }
+  }
   const int q = atomicAdd(qn, 1);
   queue[q] = i;
 }
@@ -233,7 +239,7 @@ __global__ void __launch_bounds__(256) k_stream_fast(DevParams p, Solvent s, con
   int pid = cell_of(p, fx, fy, fz);
   const int l0 = __ldg(lstart + pid), l1 = __ldg(lstart + pid + 1);
   if (l1 > l0) {
-    hand_off(lrank, pid, (int)i, bcnt, bucket, queue, qn);
+    hand_off(lrank, pid, l1 - l0, (int)i, bcnt, bucket, queue, qn);
     return;
   }
   finish_stream(p, 0.0, X, Y, Z, VX, VY, VZ);
@@ -311,10 +317,12 @@ __device__ __forceinline__ void heavy_particle(const DevParams& p, Solvent& s, S
 
 // Particles in cells with triangles (reflectionFed, Src/solfuncs.cpp:400-598,
 // then the walls and wrap).  Block a < nact takes the bucket of listed cell
-// a, each warp walking one of its particles at a time; the warps of a block
-// read the same list, so its TriPre records come from L1 after the first
-// touch.  The bucket count is reset for the next step.  Blocks from nact on
-// walk the overflow queue, a warp per particle.
+// a: its list's TriPre records and triangle indices are staged in shared
+// memory once, then each warp walks one particle of the bucket at a time
+// from there (the walk's per-entry test reads no global memory).  The
+// bucket count is reset for the next step.  Blocks from nact on walk the
+// overflow queue (full buckets, lists longer than kHeavyList), a warp per
+// particle, from global memory.
 template <bool F32>
 __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, SolventF f,
                                                       const int* __restrict__ lstart, const int* __restrict__ lidx,
@@ -322,6 +330,7 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
                                                       const int* __restrict__ bucket, Snap sn,
                                                       const TriPre* __restrict__ pre, const int* queue,
                                                       const int* qn, int nact) {
+  extern __shared__ double sh[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if ((int)blockIdx.x >= nact) {
     const int nq = *qn;
@@ -352,12 +361,19 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
   const int n = s_n;
   if (n == 0) return;
   const int c = acell[a];
-  const int l0 = lstart[c], len = lstart[c + 1] - l0;
-  const int* L = lidx + l0;
+  const int l0 = lstart[c], len = lstart[c + 1] - l0;  // len <= kHeavyList (hand_off)
+  TriPre* st = reinterpret_cast<TriPre*>(sh);
+  int* sj = reinterpret_cast<int*>(st + len);
+  for (int e = threadIdx.x; e < len; e += blockDim.x) {
+    const int jj = lidx[l0 + e];
+    sj[e] = jj;
+    st[e] = pre[jj];
+  }
+  __syncthreads();
   for (int q = w; q < n; q += nw) {
     const int64_t i = bucket[(int64_t)a * kBucket + q];
-    heavy_particle<F32>(p, s, f, sn, i, lane, len, [&](int e) -> const TriPre& { return pre[L[e]]; },
-                        [&](int e) { return L[e]; });
+    heavy_particle<F32>(p, s, f, sn, i, lane, len, [&](int e) -> const TriPre& { return st[e]; },
+                        [&](int e) { return sj[e]; });
   }
 }
 
@@ -883,9 +899,17 @@ void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaS
 template <bool F32>
 static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
                                 cudaStream_t st) {
-  k_stream_cells<F32><<<c.nact + kOverflowBlocks, 256, 0, st>>>(p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt,
-                                                               f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
-                                                               c.nact);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_stream_cells<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kHeavyList * (int)(sizeof(TriPre) + sizeof(int)));
+    attr_set = true;
+  }
+  const int lmax = c.lmax < kHeavyList ? c.lmax : kHeavyList;
+  const size_t smem = (size_t)lmax * (sizeof(TriPre) + sizeof(int));
+  k_stream_cells<F32><<<c.nact + kOverflowBlocks, 256, smem, st>>>(p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt,
+                                                                  f.bucket, f.snap[buf], f.pre[buf], f.queue,
+                                                                  f.qn, c.nact);
 }
 
 void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,

@@ -16,8 +16,10 @@ struct Snap {
 };
 
 // near-membrane streaming: particles per listed cell taken by the cell's
-// block, and the blocks that walk the overflow queue (full buckets)
+// block, the longest list staged in its shared memory, and the blocks that
+// walk the overflow queue
 constexpr int kBucket = 32;
+constexpr int kHeavyList = 1024;
 constexpr int kOverflowBlocks = 8;
 
 struct FastBufs {

@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const
   int pid = cell_of(p, fx, fy, fz);
   const int l0 = __ldg(lstart + pid), l1 = __ldg(lstart + pid + 1);
   if (l1 > l0) {
-    hand_off(lrank, pid, (int)i, bcnt, bucket, queue, qn);
+    hand_off(lrank, pid, l1 - l0, (int)i, bcnt, bucket, queue, qn);
     return;
   }
   float X = q.x + v.x * dt, Y = q.y + v.y * dt, Z = q.z + v.z * dt;
