@@ -197,6 +197,8 @@ def run_ours(args):
     sim.init(V, E, T, WORKLOAD["nknobs"])
     sim.step(args.warmup)
     sim.sync()
+    # the end-to-end leg below replays the same steps from this state
+    start = sim.get_state() if args.e2e else None
     barrier(world)
     with ClockSampler(local) as clocks:
         sim.profile_begin()
@@ -224,9 +226,11 @@ def run_ours(args):
             traffic = None
     # end to end through the C ABI with host buffers: the full state in from
     # page-locked memory, every step the RBCdata record out, the final state out
+    # the state must still be physical after the timed steps
+    finite = bool(np.isfinite(sim.observables()[:6]).all())
     e2e = None
     if args.e2e:
-        e2e = run_e2e(G, sim, args.steps, world)
+        e2e = run_e2e(G, sim, start, args.steps, world)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -243,6 +247,7 @@ def run_ours(args):
                               "membrane": prof["membrane_ms"] / args.steps},
         "gpu_launches": prof["launches"],
         "clocks": clocks.summary(),
+        "state_finite": finite,
     }
     if e2e:
         line["e2e"] = e2e
@@ -263,13 +268,13 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_e2e(G, sim, steps, world):
+def run_e2e(G, sim, st, steps, world):
     """Same metric through the public API with host buffers: set_state of
-    the full state from page-locked memory, `steps` steps each followed by
-    the RBCdata record (vertex x,y,z,ix,iy,bondi) to host, then the full
-    state back.  Host wall clock with a device synchronize on both ends."""
+    the full state `st` (the state the timed steps started from) from
+    page-locked memory, the same `steps` steps each followed by the RBCdata
+    record (vertex x,y,z,ix,iy,bondi) to host, then the full state back.
+    Host wall clock with a device synchronize on both ends."""
     import numpy as np
-    st = sim.get_state()
     pinned = {}
     for k, a in st.a.items():
         pa = G.PinnedArray(a.size, a.dtype)
@@ -282,18 +287,22 @@ def run_e2e(G, sim, steps, world):
     sim.sync()
     t0 = time.perf_counter()
     sim.set_state(st)
+    t1 = time.perf_counter()
     for _ in range(steps):
         sim.step(1)
         v = rec.view()
         # vertex record only: solvent and list pointers are left NULL
         sim._ck(sim.L.irbc_get_state(sim.h, __import__("ctypes").byref(v)), "irbc_get_state")
+    t2 = time.perf_counter()
     out = sim.get_state()
     sim.sync()
-    dt = time.perf_counter() - t0
+    t3 = time.perf_counter()
+    dt = t3 - t0
     d2h = d2h_rec * steps + sum(out.a[k].nbytes for k in out.a)
     ns = WORKLOAD["Ns"]
     return {"value": ns * steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d / steps),
-            "d2h_bytes_per_step": int(d2h / steps)}
+            "d2h_bytes_per_step": int(d2h / steps),
+            "seconds": {"set_state": t1 - t0, "steps": t2 - t1, "get_state": t3 - t2}}
 
 
 def main():

@@ -3,13 +3,12 @@
 // (:700-810), as one kernel over tiles of 32 consecutive collision cells.
 //
 // One warp per tile.  The tile's particles are contiguous in perm (the
-// counting sort's output), so the warp gathers them with independent loads
-// (no dependent chain per cell): first their storage and reference indices,
-// then their velocities, each stored in shared memory at its rank within its
-// cell by reference index (the order of Cells[].sol).  Each lane then forms
-// its cell's vcm / axis / ThE from the sorted segment with the sums in the
-// reference's order, and the warp rotates the tile's particles and writes
-// them back.  A tile with more particles than the shared buffer holds falls
+// counting sort's output), so the warp gathers their velocity records into
+// shared memory with independent loads (no dependent chain per cell) and
+// ranks each particle within its cell by reference index (the order of
+// Cells[].sol).  Each lane then forms its cell's vcm / axis / ThE with the
+// sums in the reference's order, and the warp rotates the tile's particles
+// and writes their records back.  A tile with more particles than the shared buffer holds falls
 // back to one lane per cell reading global memory.
 //
 // Included by kernels.cu (FP64 solvent) and fp32.cuh (FP32-bulk solvent).
@@ -179,15 +178,14 @@ constexpr int kTileWarps = 2;    // warps per block
 constexpr int kTileBatch = 8;    // gathers in flight per lane
 constexpr int kMaxSeg = 48;      // fallback: cells up to this size sort in registers
 
-// one warp's tile: particles in reference order within each cell segment
+// one warp's tile, in perm order; ord lists each cell's particles in
+// reference order
 struct CellTile {
-  double vx[kTileCap], vy[kTileCap], vz[kTileCap];  // sorted
+  double vx[kTileCap], vy[kTileCap], vz[kTileCap];
   double P[kTileCells][7];
-  int uid[kTileCap];      // reference index, in perm order (for the ranks)
-  int uq[kTileCap];       // storage index, in perm order
-  int id[kTileCap];       // sorted
-  int q[kTileCap];        // sorted: storage index
+  int id[kTileCap];
   int st[kTileCells + 1];
+  unsigned short ord[kTileCap];
   unsigned char cell[kTileCap];
 };
 
@@ -297,31 +295,14 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Sol
     const int e = t.st[lane + 1];
     for (int j = stl; j < e; ++j) t.cell[j] = (unsigned char)lane;
   }
-  // pass 1: storage and reference indices of the tile's particles (perm order)
-  for (int j0 = 0; j0 < total; j0 += 32 * kTileBatch) {
-    int qv[kTileBatch];
-#pragma unroll
-    for (int u = 0; u < kTileBatch; ++u) {
-      const int j = j0 + u * 32 + lane;
-      qv[u] = j < total ? perm[S0 + j] : -1;
-    }
-#pragma unroll
-    for (int u = 0; u < kTileBatch; ++u)
-      if (qv[u] >= 0) {
-        t.uq[j0 + u * 32 + lane] = qv[u];
-        t.uid[j0 + u * 32 + lane] = load_id<F32>(s, f, qv[u]);
-      }
-  }
-  __syncwarp();
-  // pass 2: velocities, each particle stored at its rank within its cell by
-  // reference index (indices are unique), i.e. in the order of Cells[].sol
+  // gather: one record per particle, kTileBatch independent loads per lane
   for (int j0 = 0; j0 < total; j0 += 32 * kTileBatch) {
     int qv[kTileBatch], idv[kTileBatch];
     double vv[kTileBatch][3];
 #pragma unroll
     for (int u = 0; u < kTileBatch; ++u) {
       const int j = j0 + u * 32 + lane;
-      qv[u] = j < total ? t.uq[j] : -1;
+      qv[u] = j < total ? perm[S0 + j] : -1;
     }
 #pragma unroll
     for (int u = 0; u < kTileBatch; ++u)
@@ -330,29 +311,39 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Sol
     for (int u = 0; u < kTileBatch; ++u) {
       const int j = j0 + u * 32 + lane;
       if (qv[u] >= 0) {
-        const int l = t.cell[j], b = t.st[l], e = t.st[l + 1], me = idv[u];
-        int r = 0;
-#pragma unroll 4
-        for (int w = b; w < e; ++w) r += (t.uid[w] < me) ? 1 : 0;
-        t.q[b + r] = qv[u];
-        t.id[b + r] = me;
-        t.vx[b + r] = vv[u][0]; t.vy[b + r] = vv[u][1]; t.vz[b + r] = vv[u][2];
+        t.id[j] = idv[u];
+        t.vx[j] = vv[u][0]; t.vy[j] = vv[u][1]; t.vz[j] = vv[u][2];
       }
     }
+  }
+  __syncwarp();
+  // rank of each particle within its cell by reference index (indices are
+  // unique): ord[b + rank] = its tile slot, the order of Cells[].sol
+  for (int j = lane; j < total; j += 32) {
+    const int l = t.cell[j], b = t.st[l], e = t.st[l + 1], me = t.id[j];
+    int r = 0;
+#pragma unroll 4
+    for (int u = b; u < e; ++u) r += (t.id[u] < me) ? 1 : 0;
+    t.ord[b + r] = (unsigned short)j;
   }
   __syncwarp();
   if (lane < ncl) {
     const int b = stl, n = t.st[lane + 1] - stl;
     double P[7];
     cell_par(p, cl, m, epoch, c0 + lane, n,
-             [&](int q, double v[3]) { v[0] = t.vx[b + q]; v[1] = t.vy[b + q]; v[2] = t.vz[b + q]; }, P);
+             [&](int q, double v[3]) {
+               const int j = t.ord[b + q];
+               v[0] = t.vx[j]; v[1] = t.vy[j]; v[2] = t.vz[j];
+             },
+             P);
     for (int e = 0; e < 7; ++e) t.P[lane][e] = P[e];
   }
   __syncwarp();
+  // rotation and write-back, in perm order (perm is read again from L2)
 #pragma unroll 2
   for (int j = lane; j < total; j += 32) {
     const double v[3] = {t.vx[j], t.vy[j], t.vz[j]};
-    store_rotated<F32>(p, s, f, t.q[j], t.id[j], v, t.P[t.cell[j]]);
+    store_rotated<F32>(p, s, f, perm[S0 + j], t.id[j], v, t.P[t.cell[j]]);
   }
 }
 

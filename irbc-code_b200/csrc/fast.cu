@@ -565,6 +565,29 @@ __global__ void k_m_av(DevParams p, Membrane m) {
 
 // TotalVA's sums, left to right in triangle order, from shared memory
 constexpr int kSumSmemT = 12288;
+
+// a[0] + a[1] + ... + a[n-1] added left to right (the reference's one-thread
+// order); the terms come in 16 at a time with 128-bit shared-memory loads so
+// that only the chain of additions is serial
+__device__ __forceinline__ double ordered_sum(const double* a, int n) {
+  double t = 0.0;
+  int i = 0;
+  if ((reinterpret_cast<uintptr_t>(a) & 15) == 0) {
+    const double2* a2 = reinterpret_cast<const double2*>(a);
+    const int n16 = n & ~15;
+#pragma unroll 2
+    for (; i < n16; i += 16) {
+      double2 r[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) r[k] = a2[(i >> 1) + k];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { t += r[k].x; t += r[k].y; }
+    }
+  }
+  for (; i < n; ++i) t += a[i];
+  return t;
+}
+
 __global__ void __launch_bounds__(1024) k_m_sum(DevParams p, Membrane m) {
   extern __shared__ double sh[];
   const bool staged = p.nt <= kSumSmemT;
@@ -574,17 +597,8 @@ __global__ void __launch_bounds__(1024) k_m_sum(DevParams p, Membrane m) {
   }
   const double* a = staged ? sh : m.area;
   const double* v = staged ? sh + p.nt : m.vol;
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-#pragma unroll 16
-    for (int i = 0; i < p.nt; ++i) t += a[i];
-    m.sc->Sarea = t;
-  } else if (threadIdx.x == 32) {
-    double t = 0.0;
-#pragma unroll 16
-    for (int i = 0; i < p.nt; ++i) t += v[i];
-    m.sc->Volume = t;
-  }
+  if (threadIdx.x == 0) m.sc->Sarea = ordered_sum(a, p.nt);
+  else if (threadIdx.x == 32) m.sc->Volume = ordered_sum(v, p.nt);
 }
 
 // Block 0: TotalVA's two ordered sums (as k_m_sum).  Blocks 1..: the edge
@@ -601,17 +615,8 @@ __global__ void __launch_bounds__(1024) k_sum_edges(DevParams p, Membrane m, dou
     }
     const double* a = staged ? sh : m.area;
     const double* v = staged ? sh + p.nt : m.vol;
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-#pragma unroll 16
-      for (int i = 0; i < p.nt; ++i) t += a[i];
-      m.sc->Sarea = t;
-    } else if (threadIdx.x == 32) {
-      double t = 0.0;
-#pragma unroll 16
-      for (int i = 0; i < p.nt; ++i) t += v[i];
-      m.sc->Volume = t;
-    }
+    if (threadIdx.x == 0) m.sc->Sarea = ordered_sum(a, p.nt);
+    else if (threadIdx.x == 32) m.sc->Volume = ordered_sum(v, p.nt);
     return;
   }
   const int k = (blockIdx.x - 1) * blockDim.x + threadIdx.x;  // 0 .. 2E
