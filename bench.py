@@ -22,10 +22,24 @@ collective in the data path.
 `--impl reference` times the reference's own OpenMP code (oracle/_ref, the
 same box, Ns, mesh, angle and dt compiled into its define.h) on the host
 cores.
+
+Two more objects ride on the same JSON line (skip with --no-batch /
+--no-serve): "batched", 64 replicas of uneven box (Lx 32..96, Ly = Lz = 32,
+the shipped 600-vertex mesh, seeded knob counts and rates, FP32 bulk)
+stepped together through irbc_batch against the same replicas stepped one
+at a time; and "served", Poisson-arriving sweep requests admitted by the
+request server by device-memory footprint, with p50/p99 completion
+latency, sims/hr and the aggregate rate against running each request
+alone.  Both use shortened step counts so that the run stays within
+minutes; the requests' shapes, sizes and parameter ranges are the
+workload's.
 """
 import argparse
 import json
 import os
+# many replicas' streams need more than the default 8 hardware queues;
+# read by CUDA when the process first uses it
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 import subprocess
 import sys
 import tempfile
@@ -207,13 +221,23 @@ def run_ours(args):
     t_ms = reduce_max(prof["total_ms"], world)
     ns = WORKLOAD["Ns"]
     value = ns * args.steps * world / (t_ms * 1e-3)
+    # the state must still be physical after the timed steps
+    finite = bool(np.isfinite(sim.observables()[:6]).all())
+    # per-phase and per-kernel times: a short window launched kernel by
+    # kernel (the timed steps run as captured graphs, which carry no
+    # per-kernel events), right after the timed steps
+    sim.set_graphs(False)
+    sim.profile_begin()
+    sim.step(48)
+    kprof = sim.profile_end()
+    sim.set_graphs(True)
     # roofline of the dominant kernel, the bulk streaming kernel (one launch
     # per step over every particle): algorithmic bytes per particle = state
     # read + positions written (FP64: positions 3 x 8 and the 32-byte
     # velocity record read, 3 x 8 written; FP32: two float4 read, one
     # written), divided by its CUDA-event time per launch
     bpp = 80 if precision == G.FP64 else 48
-    bulk_avg_ms = prof["bulk_ms"] / max(1, prof["bulk_launches"])
+    bulk_avg_ms = kprof["bulk_ms"] / max(1, kprof["bulk_launches"])
     achieved = ns * bpp / (bulk_avg_ms * 1e-3) / 1e9
     peak, kind = peaks()
     traffic = None
@@ -226,8 +250,6 @@ def run_ours(args):
             traffic = None
     # end to end through the C ABI with host buffers: the full state in from
     # page-locked memory, every step the RBCdata record out, the final state out
-    # the state must still be physical after the timed steps
-    finite = bool(np.isfinite(sim.observables()[:6]).all())
     e2e = None
     if args.e2e:
         e2e = run_e2e(G, sim, start, args.steps, world)
@@ -242,9 +264,9 @@ def run_ours(args):
                      "kernel": "k_stream_fast" if precision == G.FP64 else "k_stream_f",
                      "bytes_per_particle": bpp, "units_per_launch": ns, "peak_kind": kind,
                      "kernel_ms_avg": bulk_avg_ms},
-        "phase_ms_per_step": {"stream": prof["stream_ms"] / args.steps,
-                              "collide": prof["collide_ms"] / args.steps,
-                              "membrane": prof["membrane_ms"] / args.steps},
+        "phase_ms_per_step": {"stream": kprof["stream_ms"] / 48, "collide": kprof["collide_ms"] / 48,
+                              "membrane": kprof["membrane_ms"] / 48,
+                              "window": "48 steps launched kernel by kernel after the timed steps"},
         "gpu_launches": prof["launches"],
         "clocks": clocks.summary(),
         "state_finite": finite,
@@ -260,12 +282,117 @@ def run_ours(args):
             line["cpu_baseline"] = {"value": d["value"], "unit": UNIT, "cores": d["cores"], "kind": "reference",
                                     "sample": "12 whole timesteps (one collision) of the reference's main loop on "
                                               "the same workload, after 1 warm-up step; set-up excluded"}
+    sim.close()
+    if world == 1 and args.batch:
+        line["batched"] = run_batched(G)
+    if world == 1 and args.serve:
+        line["served"] = run_served(G)
     if rank == 0:
         print(json.dumps(line))
-    sim.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+TROPH = [os.path.join(ROOT, "tests", "golden", "troph600", n) for n in ("TrophV600.dat", "TrophE600.dat",
+                                                                      "TrophT600.dat")]
+
+
+def replica_params(G, rng, precision, Lx, Ly, Lz, seed, kon, koff, walls_frac=0.01):
+    import math
+    a = math.radians(130.0)
+    return G.default_params(Lx=float(Lx), Ly=float(Ly), Lz=float(Lz), Ns=int(Lx * Ly * (Lz + 1) * 10),
+                            cosalpha=math.cos(a), sinalpha=math.sin(a), dtcd=0.025, dtmd=0.002,
+                            walls=walls_frac * Lz, onrate=kon, offrate=koff, seed=seed, precision=precision)
+
+
+def run_batched(G, nrep=64, steps=240, alone=4, nthreads=8):
+    """64 replicas of uneven box (Lx in 32..96, Ly = Lz = 32 cells, 10 per
+    cell), the 600-vertex mesh, knobs in 100..1000, kon log-uniform in
+    1e-4..1e-1, koff in 1e-3..1e-1, FP32 bulk: stepped together vs the
+    first `alone` of them stepped one at a time (the plain path)."""
+    import numpy as np
+    from irbc_b200 import mesh
+    V, E, T = mesh.read_reference_files(*TROPH)
+    rng = np.random.default_rng(2024)
+    sims = []
+    for r in range(nrep):
+        Lx = int(rng.integers(32, 97))
+        kon, koff = 10 ** rng.uniform(-4, -1), 10 ** rng.uniform(-3, -1)
+        p = replica_params(G, rng, G.FP32, Lx, 32, 32, 5000 + r, kon, koff)
+        s = G.Simulation(p)
+        s.init(V, E, T, int(rng.integers(100, 601)))
+        sims.append(s)
+    ns = [s.params.Ns for s in sims]
+    # plain path: each replica alone, one after the other
+    t_alone = 0.0
+    for s in sims[:alone]:
+        s.step(48)
+        s.sync()
+        t = time.perf_counter()
+        s.step(steps)
+        s.sync()
+        t_alone += time.perf_counter() - t
+    plain = sum(ns[:alone]) * steps / t_alone
+    b = G.Batch(nthreads=nthreads)
+    for s in sims:
+        b.add(s)
+    b.step(48)  # past the first collision: every member's graphs are captured
+    t = time.perf_counter()
+    b.step(steps)
+    dt = time.perf_counter() - t
+    agg = sum(ns) * steps / dt
+    finite = all(bool(np.isfinite(s.observables()[:6]).all()) for s in sims)
+    b.close()
+    for s in sims:
+        s.close()
+    return {"metric": "aggregate solvent particle-steps/s, %d replicas stepped together" % nrep,
+            "value": agg, "unit": UNIT, "replicas": nrep, "particles": int(sum(ns)), "steps": steps,
+            "seconds": dt, "plain_value": plain, "plain_sample": "%d of the replicas alone, one after another" % alone,
+            "vs_plain": agg / plain, "host_threads": nthreads, "dtype": "f32-bulk", "state_finite": finite,
+            "config": "Lx uniform 32..96, Ly = Lz = 32, 10/cell, 600-vertex mesh, knobs 100..600, "
+                      "kon log-U 1e-4..1e-1, koff log-U 1e-3..1e-1, seeded"}
+
+
+def run_served(G, nreq=40, rate=8.0, steps_range=(240, 960), nthreads=8):
+    """Poisson-arriving sweep requests (mean `rate`/s, `nreq` of them): kon,
+    koff log-uniform, knobs 50..1000 (at most the mesh's vertices), shear
+    walls/Lz in 0.002..0.02, Lx 32..128, Ly = Lz in 24..48 cells, the
+    600-vertex or the 2562-vertex mesh, FP32 bulk; admitted by footprint."""
+    import numpy as np
+    from irbc_b200 import mesh
+    meshes = [mesh.read_reference_files(*TROPH), mesh.discocyte()]
+    rng = np.random.default_rng(77)
+    reqs = []
+    for k in range(nreq):
+        V, E, T = meshes[int(rng.integers(0, 2))]
+        Ly = int(rng.integers(24, 49))
+        p = replica_params(G, rng, G.FP32, int(rng.integers(32, 129)), Ly, Ly, 9000 + k,
+                           10 ** rng.uniform(-4, -1), 10 ** rng.uniform(-3, -1), rng.uniform(0.002, 0.02))
+        nk = int(rng.integers(50, min(1000, len(V)) + 1))
+        steps = int(rng.integers(steps_range[0] // 24, steps_range[1] // 24 + 1)) * 24
+        reqs.append((p, V, E, T, nk, steps, float(rng.exponential(1.0 / rate))))
+    srv = G.Server(nthreads=nthreads, round_steps=96)
+    t0 = srv.clock()
+    for p, V, E, T, nk, steps, gap in reqs:
+        time.sleep(gap)
+        srv.submit(p, V, E, T, nk, steps)
+    got = []
+    while len(got) < nreq:
+        more = srv.poll(64, wait=60.0)
+        if not more:
+            break
+        got += more
+    t1 = srv.clock()
+    srv.close()
+    lat = np.array([r["t_end"] - r["t_submit"] for r in got])
+    work = sum(r["ns"] * r["steps"] for r in got if r["status"] == 0)
+    return {"metric": "served sweep requests", "requests": nreq, "completed": int(sum(r["status"] == 0 for r in got)),
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "sims_per_hour": 3600.0 * len(got) / (t1 - t0), "value": work / (t1 - t0), "unit": UNIT,
+            "arrival_rate_per_s": rate, "steps_per_request": list(steps_range), "dtype": "f32-bulk",
+            "config": "Poisson arrivals; kon log-U 1e-4..1e-1, koff log-U 1e-3..1e-1, knobs 50..1000, "
+                      "walls/Lz 0.002..0.02, Lx 32..128, Ly = Lz 24..48, 600- or 2562-vertex mesh"}
 
 
 def run_e2e(G, sim, st, steps, world):
@@ -314,8 +441,12 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-batch", dest="batch", action="store_false")
+    ap.add_argument("--no-serve", dest="serve", action="store_false")
     args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
+    # at least 3; and past the third collision, so the first 24-step graph
+    # is captured before the timed steps
+    args.warmup = max(args.warmup, 36)
     if args.impl == "reference":
         run_reference(args)
     else:

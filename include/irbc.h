@@ -134,6 +134,10 @@ int32_t irbc_nlig(const irbc_handle* h);
  * entry points run the halves either side of the TotalVA call at
  * maincode.cpp:602 (part 1 = :462-602, part 2 = :603-762). */
 int irbc_step(irbc_handle* h, int64_t n);
+/* Not in the reference.  irbc_step launches whole 24-step stretches
+ * between list updates as one captured CUDA graph (on by default); on = 0
+ * launches every kernel separately.  The results are the same either way. */
+int irbc_set_graphs(irbc_handle* h, int32_t on);
 int irbc_step_part1(irbc_handle* h);
 int irbc_step_part2(irbc_handle* h);
 
@@ -196,6 +200,57 @@ int64_t irbc_launch_count(const irbc_handle* h);
  * out[9] = its launches; nout <= 10 values are written */
 int irbc_profile_begin(irbc_handle* h);
 int irbc_profile_end(irbc_handle* h, double* out, int32_t nout);
+/* ---- batches and the request server (not in the reference) -------------------
+ * A batch steps independent simulations (handles, on one device) together:
+ * nthreads host threads issue the members' steps so that their kernels
+ * overlap on the GPU.  irbc_batch_step(b, n) advances every member n steps
+ * and returns when their device work has finished.  Members stay owned by
+ * the caller.  For many members, set CUDA_DEVICE_MAX_CONNECTIONS=32 in the
+ * environment before the process first uses CUDA. */
+typedef struct irbc_batch irbc_batch;
+int irbc_batch_create(int32_t nthreads, irbc_batch** out);
+void irbc_batch_destroy(irbc_batch* b);
+int irbc_batch_add(irbc_batch* b, irbc_handle* h);
+int irbc_batch_remove(irbc_batch* b, irbc_handle* h);
+int32_t irbc_batch_size(const irbc_batch* b);
+int irbc_batch_step(irbc_batch* b, int64_t n);
+/* The server takes whole simulations as requests: parameters, mesh, knob
+ * count and step count.  Its loop admits a pending request when its
+ * footprint (irbc_footprint_bytes) fits in the device-memory budget
+ * (budget_bytes <= 0: 85% of the free memory at creation), creates and
+ * initialises it, and advances every admitted simulation in rounds of
+ * round_steps steps with a pool of nthreads host threads; requests that
+ * arrive meanwhile join at the next round.  A finished simulation yields an
+ * irbc_result: its times on the server clock (seconds since creation), its
+ * observables (irbc_observables) and, when submitted with keep = 1, its
+ * handle, which the caller then owns and destroys; otherwise the server
+ * frees it.  Each simulation computes exactly what it would alone. */
+typedef struct irbc_server irbc_server;
+typedef struct irbc_result {
+  int64_t id;
+  int32_t status;          /* 0, or the error of create / init / step */
+  int32_t pad_;
+  int64_t steps, ns;       /* steps run, solvent particles */
+  double t_submit, t_start, t_end;
+  double obs[8];           /* irbc_observables at the end */
+  irbc_handle* handle;     /* keep = 1: the finished simulation */
+} irbc_result;
+int irbc_server_create(int32_t device, int64_t budget_bytes, int32_t nthreads, int64_t round_steps,
+                       irbc_server** out);
+/* copies the mesh; *id identifies the request's result.  IRBC_ERR_CAPACITY
+ * if its footprint exceeds the whole budget */
+int irbc_server_submit(irbc_server* s, const irbc_params* p, const double* V, int32_t nv, const int32_t* E,
+                       int32_t ne, const int32_t* T, int32_t nt, int32_t nknobs, int64_t nsteps, int32_t keep,
+                       int64_t* id);
+/* up to max finished results, waiting up to wait_s seconds for the first;
+ * returns how many were written */
+int32_t irbc_server_poll(irbc_server* s, irbc_result* out, int32_t max, double wait_s);
+/* out: pending, active, unread results, bytes in use, budget, particle-steps done */
+int irbc_server_status(irbc_server* s, int64_t out[6]);
+double irbc_server_clock(irbc_server* s);
+/* stops the loop; simulations still pending or running are dropped */
+void irbc_server_destroy(irbc_server* s);
+
 /* page-locked host memory for fast state exchange */
 void* irbc_host_alloc(size_t bytes);
 void irbc_host_free(void* p);

@@ -15,7 +15,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-O2",
          "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["kernels.cu", "fast.cu", "binning.cu", "binning_noalloc.cu", "api.cu"]
+SOURCES = ["kernels.cu", "fast.cu", "binning.cu", "binning_noalloc.cu", "api.cu", "batch.cu"]
 # every header and included .cuh: a change to any of them rebuilds every source
 HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 

@@ -37,6 +37,18 @@ struct irbc_handle {
   bool snap_ready = false;     // snapshot/triangle prep of the next step done
   cudaEvent_t ev_snap = nullptr, ev_mem = nullptr, ev_coll = nullptr, ev_str[2] = {nullptr, nullptr};
   cudaEvent_t ev_vbin = nullptr;
+  uint64_t* ebase = nullptr;   // device: the draw epoch base of the current call (DevParams::ebase)
+  int64_t ebase_val = 0;       // its value as last written
+  // captured step sequences (irbc_step): one per starting configuration
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    int colsteps0 = 0, parity = 0;
+    double wallspeed = 0;
+    int64_t launches = 0, collisions = 0;
+  };
+  std::vector<StepGraph> graphs;
+  bool graphs_on = true;
+  bool capturing = false;
   std::string err;
   bool have_mesh = false;
   int64_t step = 0;
@@ -304,10 +316,13 @@ void build_gather(const HostMesh& M, const std::vector<int>& start, const std::v
   gstart[M.nv] = (int)gidx.size();
 }
 
+void invalidate_graphs(irbc_handle* h);
+
 // allocates the membrane and uploads the topology
 int upload_mesh(irbc_handle* h, const HostMesh& M) {
   Membrane& m = h->m;
   if (M.nv > 8192) return fail(h, IRBC_ERR_ARG, "at most 8192 membrane vertices");
+  invalidate_graphs(h);
   free_membrane(m);
   free_fast(h->fb);
   h->snap_ready = false;
@@ -362,14 +377,39 @@ int upload_mesh(irbc_handle* h, const HostMesh& M) {
 
 int64_t launches_in(const irbc_handle* h) { return g_launches.load() - h->launches0; }
 
+// epoch base for the launches that follow on the main stream (the side
+// stream joins after it through the usual events)
+cudaError_t set_epoch_base(irbc_handle* h, uint64_t base) {
+  h->ebase_val = (int64_t)base;
+  launch_set_u64(h->ebase, base, h->st);
+  return cudaGetLastError();
+}
+
+void invalidate_graphs(irbc_handle* h) {
+  for (auto& g : h->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  h->graphs.clear();
+}
+
 // the solvent kernels of the handle's precision
+// physical re-sort of the solvent by the latest collision's cells
+int resort_any(irbc_handle* h, cudaStream_t st) {
+  if (h->fp32) launch_resort_f(h->sf, h->s, st);
+  else launch_resort(h->s, st);
+  h->s.resorted = h->s.ncoll;
+  return h->s.n ? 2 : 0;
+}
+
 // returns the number of kernels launched: vbin, count, ghost flags, three
-// scan kernels, perm, cells, and the physical re-sort when due.  With a
-// side stream the vertex binning runs there (after whatever the side stream
-// already holds: the membrane of the previous step) while the solvent's cell
-// counts start at once on the main stream.
+// scan kernels, perm, cells, and the physical re-sort when due (never while
+// a step sequence is being captured; irbc_step re-sorts between captured
+// sequences).  With a side stream the vertex binning runs there (after
+// whatever the side stream already holds: the membrane of the previous
+// step) while the solvent's cell counts start at once on the main stream.
 int collide_any(irbc_handle* h, uint64_t epoch, cudaStream_t st, cudaStream_t side = nullptr) {
-  const int64_t before = h->s.ncoll;
+  h->s.ncoll += 1;
+  const bool resort = !h->capturing && h->s.ncoll - h->s.resorted >= kResortEvery;
+  if (resort) h->s.resorted = h->s.ncoll;
   launch_vbin(h->dp, h->m, h->c, epoch, side ? side : st);
   if (h->fp32) launch_collide_count_f(h->dp, h->sf, h->s, h->c, epoch, st);
   else launch_collide_count(h->dp, h->s, h->c, epoch, st);
@@ -377,9 +417,9 @@ int collide_any(irbc_handle* h, uint64_t epoch, cudaStream_t st, cudaStream_t si
     cudaEventRecord(h->ev_vbin, side);
     cudaStreamWaitEvent(st, h->ev_vbin, 0);
   }
-  if (h->fp32) launch_collide_finish_f(h->dp, h->sf, h->s, h->c, h->m, epoch, st);
-  else launch_collide_finish(h->dp, h->s, h->c, h->m, epoch, st);
-  return 8 + ((h->s.ncoll != before && h->s.ncoll % kResortEvery == 0) ? 1 : 0);
+  if (h->fp32) launch_collide_finish_f(h->dp, h->sf, h->s, h->c, h->m, epoch, st, resort);
+  else launch_collide_finish(h->dp, h->s, h->c, h->m, epoch, st, resort);
+  return 8 + (resort && h->s.n ? 2 : 0);
 }
 
 // profiling: a pair of events around a launch group of a category
@@ -396,15 +436,17 @@ struct ProfScope {
   irbc_handle* h;
   size_t mark;
   cudaStream_t st;
-  ProfScope(irbc_handle* hh, int cat, cudaStream_t s = nullptr) : h(hh), mark(0), st(s ? s : hh->st) {
-    if (!h->prof) return;
+  bool on;
+  ProfScope(irbc_handle* hh, int cat, cudaStream_t s = nullptr)
+      : h(hh), mark(0), st(s ? s : hh->st), on(hh->prof && !hh->capturing) {
+    if (!on) return;
     const size_t idx = h->ev_used;
     cudaEventRecord(next_event(h), st);
     mark = h->ev_marks.size();
     h->ev_marks.push_back({cat, idx, idx});
   }
   ~ProfScope() {
-    if (!h->prof) return;
+    if (!on) return;
     h->ev_marks[mark].end = h->ev_used;
     cudaEventRecord(next_event(h), st);
   }
@@ -414,7 +456,7 @@ struct ProfScope {
 // bracketed by a pair of events of its own
 void stream_any(irbc_handle* h, int buf, cudaStream_t st) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (h->prof) {
+  if (h->prof && !h->capturing) {
     h->ev_marks.push_back({PROF_STREAM_BULK, h->ev_used, h->ev_used + 1});
     e0 = next_event(h);
     e1 = next_event(h);
@@ -496,7 +538,7 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   A(dalloc(&c.start, c.n + 1));
   A(dalloc(&c.lstart, c.n + 1));
   A(dalloc(&c.lstart2, c.n + 1));
-  A(dalloc(&c.totals, 8));
+  A(dalloc(&c.totals, 12));
   c.scan_blocks = scan_part_blocks(c.n + 1);
   A(dalloc(&c.scan_part, c.scan_blocks * 3 + 3));
   c.lcap = c.lcap2 = std::max<int64_t>(1024, c.n / 16);
@@ -506,6 +548,8 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   A(dalloc(&h->m.xlig, h->dp.nlig));
   A(dalloc(&h->m.ylig, h->dp.nlig));
   A(dalloc(&h->m.sc, 1));
+  A(dalloc(&h->ebase, 1));
+  h->dp.ebase = h->ebase;
   A(dalloc(&h->obs, 64 + 4096));
   A(dalloc(&h->fb.queue, s.n));
   A(dalloc(&h->fb.qn, 4));
@@ -520,6 +564,7 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   cudaMemsetAsync(c.lstart, 0, sizeof(int) * (c.n + 1), h->st);
   cudaMemsetAsync(h->m.ligi, 0, sizeof(int) * h->dp.nlig, h->st);
   cudaMemsetAsync(h->m.sc, 0, sizeof(MemScalars), h->st);
+  cudaMemsetAsync(h->ebase, 0, sizeof(uint64_t), h->st);
   cudaMemsetAsync(s.pid, 0, sizeof(int) * std::max<int64_t>(1, s.n), h->st);
   cudaMemcpyAsync(h->m.xlig, h->xlig.data(), sizeof(double) * h->dp.nlig, cudaMemcpyHostToDevice, h->st);
   cudaMemcpyAsync(h->m.ylig, h->ylig.data(), sizeof(double) * h->dp.nlig, cudaMemcpyHostToDevice, h->st);
@@ -535,6 +580,7 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   cudaSetDevice(h->P.device);
   if (h->st) cudaStreamSynchronize(h->st);
   if (h->st2) cudaStreamSynchronize(h->st2);
+  invalidate_graphs(h);
   free_fast(h->fb);
   dfree(h->fb.queue); dfree(h->fb.qn); dfree(h->fb.bcnt); dfree(h->fb.bucket);
   for (float4** q : {&h->sf.pos, &h->sf.vel, &h->sf.pos2, &h->sf.vel2}) dfree(*q);
@@ -553,7 +599,7 @@ extern "C" void irbc_destroy(irbc_handle* h) {
                   &c.scan_part, &c.lidx, &c.lidx2})
     dfree(*q);
   free_membrane(h->m);
-  dfree(h->m.ligi); dfree(h->m.xlig); dfree(h->m.ylig); dfree(h->m.sc); dfree(h->obs);
+  dfree(h->m.ligi); dfree(h->m.xlig); dfree(h->m.ylig); dfree(h->ebase); dfree(h->m.sc); dfree(h->obs);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   if (h->ev_begin) cudaEventDestroy(h->ev_begin);
   if (h->ev_end) cudaEventDestroy(h->ev_end);
@@ -567,6 +613,7 @@ extern "C" int32_t irbc_nlig(const irbc_handle* h) { return h ? h->dp.nlig : -1;
 extern "C" int64_t irbc_launch_count(const irbc_handle* h) { return h ? launches_in(h) : -1; }
 extern "C" int irbc_sync(irbc_handle* h) {
   if (!h) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
   CK(cudaStreamSynchronize(h->st));
   return 0;
 }
@@ -581,6 +628,7 @@ static int refresh_listed(irbc_handle* h) {
   g_launches += k;
   FastBufs& f = h->fb;
   if (c.nact > f.bcap) {
+    invalidate_graphs(h);  // the buckets move
     dfree(f.bcnt);
     dfree(f.bucket);
     f.bcap = c.nact + c.nact / 2 + 64;
@@ -600,7 +648,19 @@ static int do_llist(irbc_handle* h) {
     c.lcap2 = need + need / 4 + 1024;
     CK(dalloc(&c.lidx2, c.lcap2));
   }
-  launch_llist_fill(h->dp, c, h->m, h->st);
+  if (need > c.lcap) {
+    // the live list moves: grow it keeping its entries (the stale tails)
+    invalidate_graphs(h);
+    int* grown = nullptr;
+    const int64_t cap = need + need / 4 + 1024;
+    CK(dalloc(&grown, cap));
+    CK(cudaMemcpyAsync(grown, c.lidx, sizeof(int) * c.lcap, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    dfree(c.lidx);
+    c.lidx = grown;
+    c.lcap = cap;
+  }
+  launch_llist_fill(h->dp, c, h->m, need, h->st);
   g_launches += 1;
   CK(cudaGetLastError());
   return refresh_listed(h);
@@ -860,6 +920,7 @@ extern "C" int irbc_set_state(irbc_handle* h, const irbc_view* v) {
     for (int64_t i = 0; i < c.n; ++i) { start[i] = (int)tot; tot += v->llen[i]; }
     start[c.n] = (int)tot;
     if (tot > c.lcap) {
+      invalidate_graphs(h);
       dfree(c.lidx);
       c.lcap = tot + 1024;
       CK(dalloc(&c.lidx, c.lcap));
@@ -956,7 +1017,8 @@ extern "C" int irbc_get_state(irbc_handle* h, irbc_view* v) {
 extern "C" int irbc_collide(irbc_handle* h, int64_t epoch) {
   if (!h) return IRBC_ERR_ARG;
   if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
-  g_launches += collide_any(h, (uint64_t)epoch, h->st);
+  CK(set_epoch_base(h, (uint64_t)epoch));
+  g_launches += collide_any(h, 0, h->st);
   CK(cudaGetLastError());
   return 0;
 }
@@ -992,7 +1054,8 @@ extern "C" int irbc_forces(irbc_handle* h) {
 }
 extern "C" int irbc_bond_dynamics(irbc_handle* h, int64_t epoch) {
   if (!h || !h->have_mesh) return IRBC_ERR_ARG;
-  launch_bonds(h->dp, h->m, (uint64_t)epoch, h->st);
+  CK(set_epoch_base(h, (uint64_t)epoch));
+  launch_bonds(h->dp, h->m, 0, h->st);
   g_launches += 2;
   CK(cudaGetLastError());
   return 0;
@@ -1007,9 +1070,10 @@ extern "C" int irbc_step_part1(irbc_handle* h) {
   h->dp.wallspeed = (s < p.warm_steps) ? p.warm_speed : p.walls;
   h->colsteps += 1; h->bbi += 1; h->upd += 1;
   if (s > 0) h->filecc += 1;
+  CK(set_epoch_base(h, (uint64_t)s));
   if (h->colsteps == h->csteps) {
     ProfScope ps(h, PROF_COLLIDE);
-    g_launches += collide_any(h, (uint64_t)s, h->st);
+    g_launches += collide_any(h, 0, h->st);
     h->colsteps = 0;
   }
   const int buf = (int)(s & 1);
@@ -1041,9 +1105,10 @@ extern "C" int irbc_step_part2(irbc_handle* h) {
   if (!h) return IRBC_ERR_ARG;
   if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
   const int64_t s = h->step;
+  CK(set_epoch_base(h, (uint64_t)s));
   {
     ProfScope ps(h, PROF_MEMBRANE);
-    g_launches += fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)s, 0, (int)((s + 1) & 1), h->st, false);
+    g_launches += fast_forces_tail(h->dp, h->m, h->fb, 0, 0, (int)((s + 1) & 1), h->st, false);
   }
   if (h->filecc == h->P.out_every) { h->filec += 1; h->filecc = 0; }
   h->step = s + 1;
@@ -1051,53 +1116,58 @@ extern "C" int irbc_step_part2(irbc_handle* h) {
   return 0;
 }
 
-// n timesteps with the membrane chain on its own stream: step s streams the
-// solvent (h->st) while the membrane drifts, computes forces and bonds for s
-// and prepares the snapshot of s+1 (h->st2).  Collisions, llist updates and
-// the snapshot buffers (two, by step parity) are ordered by events.  The
-// result equals n calls of part 1 + part 2.
-extern "C" int irbc_step(irbc_handle* h, int64_t n) {
-  if (!h || n < 0) return IRBC_ERR_ARG;
-  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
-  cudaSetDevice(h->P.device);
+// One timestep of the pipelined schedule: step s streams the solvent
+// (h->st) while the membrane drifts, computes forces and bonds for s and
+// prepares the snapshot of s+1 (h->st2).  Collisions, llist updates and the
+// snapshot buffers (two, by step parity) are ordered by events.  eoff is the
+// step's draw-epoch offset from the current base; last: the step ends a
+// call or a captured sequence (the next step's half-kick is not fused into
+// this one).  dry: advance the host counters only (the launches are in a
+// captured sequence being replayed).
+static int step_one(irbc_handle* h, int64_t eoff, bool last, bool dry) {
   const irbc_params& p = h->P;
   cudaStream_t ms = h->st, ss = h->st2;
-  // the side stream starts after everything already queued on the main one
-  CK(cudaEventRecord(h->ev_coll, ms));
-  CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
-  for (int64_t k = 0; k < n; ++k) {
-    const int64_t s = h->step;
-    h->dp.wallspeed = (s < p.warm_steps) ? p.warm_speed : p.walls;
-    h->colsteps += 1; h->bbi += 1; h->upd += 1;
-    if (s > 0) h->filecc += 1;
-    const int buf = (int)(s & 1);
-    if (h->colsteps == h->csteps) {
+  const int64_t s = h->step;
+  h->dp.wallspeed = (s < p.warm_steps) ? p.warm_speed : p.walls;
+  h->colsteps += 1; h->bbi += 1; h->upd += 1;
+  if (s > 0) h->filecc += 1;
+  const int buf = (int)(s & 1);
+  if (h->colsteps == h->csteps) {
+    if (dry) {
+      h->s.ncoll += 1;
+    } else {
       {
         ProfScope ps(h, PROF_COLLIDE, ms);
-        g_launches += collide_any(h, (uint64_t)s, ms, ss);
+        g_launches += collide_any(h, (uint64_t)eoff, ms, ss);
       }
-      h->colsteps = 0;
-      CK(cudaEventRecord(h->ev_coll, ms));
-      CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
-      h->snap_ready = false;
-    }
-    if (!h->snap_ready) {
-      CK(cudaStreamWaitEvent(ss, h->ev_str[buf], 0));
-      ProfScope ps(h, PROF_MEMBRANE, ss);
-      fast_kick_prep(h->dp, h->m, h->fb, buf, ss);
-      g_launches += 2;
-    }
-    if (h->upd == h->uplist) {
-      // positions of step s are final once the side stream reaches here;
-      // the side stream's drift of step s waits for the update
-      CK(cudaEventRecord(h->ev_snap, ss));
-      CK(cudaStreamWaitEvent(ms, h->ev_snap, 0));
-      int rc = do_llist(h);
-      if (rc) return rc;
-      h->upd = 0;
       CK(cudaEventRecord(h->ev_coll, ms));
       CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
     }
+    h->colsteps = 0;
+    h->snap_ready = false;
+  }
+  if (!h->snap_ready && !dry) {
+    CK(cudaStreamWaitEvent(ss, h->ev_str[buf], 0));
+    ProfScope ps(h, PROF_MEMBRANE, ss);
+    fast_kick_prep(h->dp, h->m, h->fb, buf, ss);
+    g_launches += 2;
+  }
+  if (h->upd == h->uplist) {
+    // never inside a captured sequence.  Positions of step s are final once
+    // the side stream reaches here; its drift of step s waits for the update
+    CK(cudaEventRecord(h->ev_snap, ss));
+    CK(cudaStreamWaitEvent(ms, h->ev_snap, 0));
+    int rc = do_llist(h);
+    if (rc) return rc;
+    h->upd = 0;
+    CK(cudaEventRecord(h->ev_coll, ms));
+    CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
+  }
+  // the next step's snapshot goes to the other buffer, read by the
+  // previous step's streaming
+  const bool next_collides = (h->colsteps + 1 == h->csteps);
+  const int next_kick = (!last && !next_collides) ? 1 : 0;
+  if (!dry) {
     CK(cudaEventRecord(h->ev_snap, ss));
     CK(cudaStreamWaitEvent(ms, h->ev_snap, 0));
     {
@@ -1106,24 +1176,166 @@ extern "C" int irbc_step(irbc_handle* h, int64_t n) {
     }
     g_launches += 2;
     CK(cudaEventRecord(h->ev_str[buf], ms));
-    // the next step's snapshot goes to the other buffer, read by the
-    // previous step's streaming
-    const bool last = (k == n - 1);
-    const bool next_collides = (h->colsteps + 1 == h->csteps);
-    const int next_kick = (!last && !next_collides) ? 1 : 0;
     CK(cudaStreamWaitEvent(ss, h->ev_str[buf ^ 1], 0));
     {
       ProfScope ps(h, PROF_MEMBRANE, ss);
       g_launches += fast_drift_va(h->dp, h->m, ss, false);
-      g_launches += fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)s, next_kick, buf ^ 1, ss, true);
+      g_launches += fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)eoff, next_kick, buf ^ 1, ss, true);
     }
     CK(cudaEventRecord(h->ev_mem, ss));
-    h->snap_ready = next_kick != 0;
-    if (h->filecc == p.out_every) { h->filec += 1; h->filecc = 0; }
-    h->step = s + 1;
+  }
+  h->snap_ready = next_kick != 0;
+  if (h->filecc == p.out_every) { h->filec += 1; h->filecc = 0; }
+  h->step = s + 1;
+  return 0;
+}
+
+constexpr int kGraphSteps = 24;  // two collision cycles per captured sequence
+
+// records every stream-ordering event on the main stream: after a capture
+// (whose records belong to the graph) and after each graph launch, so that
+// later waits refer to work outside any graph and follow the launch
+static cudaError_t rearm_events(irbc_handle* h) {
+  for (cudaEvent_t e : {h->ev_str[0], h->ev_str[1], h->ev_snap, h->ev_mem, h->ev_coll, h->ev_vbin}) {
+    cudaError_t r = cudaEventRecord(e, h->st);
+    if (r != cudaSuccess) return r;
+  }
+  return cudaSuccess;
+}
+
+// a captured sequence can stand for the next kGraphSteps steps when no list
+// update falls inside them, the wall speed is the same throughout, and the
+// previous step did not fuse this step's half-kick
+static bool graph_fits(const irbc_handle* h, int64_t remaining) {
+  if (!h->graphs_on || remaining < kGraphSteps || h->snap_ready) return false;
+  if (h->upd + kGraphSteps >= h->uplist) return false;
+  const int64_t s = h->step, w = h->P.warm_steps;
+  return (s + kGraphSteps <= w) || (s >= w);
+}
+
+// the kGraphSteps steps from the current configuration, captured once; the
+// host counters are left where they were
+static irbc_handle::StepGraph* graph_for(irbc_handle* h) {
+  const double ws = (h->step < h->P.warm_steps) ? h->P.warm_speed : h->P.walls;
+  const int parity = (int)(h->step & 1);
+  for (auto& g : h->graphs)
+    if (g.colsteps0 == h->colsteps && g.parity == parity && g.wallspeed == ws) return &g;
+  cudaStream_t ms = h->st, ss = h->st2;
+  // counters to restore after the capture
+  const int64_t step = h->step, ncoll = h->s.ncoll, resorted = h->s.resorted;
+  const int colsteps = h->colsteps, bbi = h->bbi, upd = h->upd, filecc = h->filecc, filec = h->filec;
+  const bool snap = h->snap_ready;
+  const double wsp = h->dp.wallspeed;
+  const int64_t l0 = g_launches.load();
+  h->capturing = true;
+  cudaGraph_t graph = nullptr;
+  bool ok = cudaStreamBeginCapture(ms, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  int rc = 0;
+  if (ok) {
+    // every event the steps wait on is first recorded inside the capture,
+    // so no wait reaches outside it; then the side stream forks off
+    for (cudaEvent_t e : {h->ev_str[0], h->ev_str[1], h->ev_snap, h->ev_mem, h->ev_coll})
+      ok = ok && cudaEventRecord(e, ms) == cudaSuccess;
+    ok = ok && cudaStreamWaitEvent(ss, h->ev_coll, 0) == cudaSuccess;
+    for (int k = 0; ok && k < kGraphSteps; ++k) {
+      rc = step_one(h, k, k == kGraphSteps - 1, false);
+      ok = rc == 0;
+    }
+    if (ok) ok = cudaStreamWaitEvent(ms, h->ev_mem, 0) == cudaSuccess;
+    cudaError_t e = cudaStreamEndCapture(ms, &graph);
+    ok = ok && e == cudaSuccess && graph != nullptr;
+  }
+  h->capturing = false;
+  cudaGetLastError();
+  rearm_events(h);
+  const int64_t launches = g_launches.load() - l0;
+  const int64_t collisions = h->s.ncoll - ncoll;
+  g_launches -= launches;
+  h->step = step; h->s.ncoll = ncoll; h->s.resorted = resorted;
+  h->colsteps = colsteps; h->bbi = bbi; h->upd = upd; h->filecc = filecc; h->filec = filec;
+  h->snap_ready = snap; h->dp.wallspeed = wsp;
+  if (ok) {
+    // the side stream's priority does not travel into the graph by itself:
+    // give the membrane chain's kernel nodes the high priority explicitly
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    size_t nn = 0;
+    cudaGraphGetNodes(graph, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) cudaGraphGetNodes(graph, nodes.data(), &nn);
+    for (cudaGraphNode_t nd : nodes) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
+      cudaKernelNodeParams kp{};
+      if (cudaGraphKernelNodeGetParams(nd, &kp) != cudaSuccess || !is_membrane_kernel(kp.func)) continue;
+      cudaKernelNodeAttrValue v{};
+      v.priority = hi;
+      cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributePriority, &v);
+    }
+    cudaGetLastError();
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();  // a refused capture leaves no sticky error
+  if (!ok) {
+    h->graphs_on = false;  // stay on plain launches from here on
+    return nullptr;
+  }
+  irbc_handle::StepGraph g;
+  g.exec = exec; g.colsteps0 = colsteps; g.parity = parity; g.wallspeed = ws;
+  g.launches = launches; g.collisions = collisions;
+  h->graphs.push_back(g);
+  return &h->graphs.back();
+}
+
+// n timesteps.  Whole sequences of kGraphSteps steps are launched as one
+// captured CUDA graph when they fit (graph_fits); the other steps, the list
+// updates among them, are launched one by one.  Either way the launches,
+// their order and their results are the same.
+extern "C" int irbc_step(irbc_handle* h, int64_t n) {
+  if (!h || n < 0) return IRBC_ERR_ARG;
+  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
+  cudaSetDevice(h->P.device);
+  cudaStream_t ms = h->st, ss = h->st2;
+  // epochs: base h->step; the side stream starts after everything already
+  // queued on the main one
+  CK(set_epoch_base(h, (uint64_t)h->step));
+  CK(cudaEventRecord(h->ev_coll, ms));
+  CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
+  int64_t k = 0;
+  while (k < n) {
+    if (graph_fits(h, n - k)) {
+      irbc_handle::StepGraph* g = graph_for(h);
+      if (g) {
+        // the side stream's earlier work ends before the base moves
+        CK(cudaStreamWaitEvent(ms, h->ev_mem, 0));
+        CK(set_epoch_base(h, (uint64_t)h->step));
+        CK(cudaGraphLaunch(g->exec, ms));
+        g_launches += g->launches;
+        for (int j = 0; j < kGraphSteps; ++j) step_one(h, j, j == kGraphSteps - 1, true);
+        if (h->s.ncoll - h->s.resorted >= kResortEvery) g_launches += resort_any(h, ms);
+        CK(rearm_events(h));
+        CK(cudaStreamWaitEvent(ss, h->ev_coll, 0));
+        k += kGraphSteps;
+        continue;
+      }
+    }
+    // a plain step; the step before a collision never fuses the next
+    // half-kick, so captured sequences start at collision steps
+    int rc = step_one(h, h->step - h->ebase_val, k == n - 1, false);
+    if (rc) return rc;
+    k += 1;
   }
   CK(cudaStreamWaitEvent(ms, h->ev_mem, 0));
   CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int irbc_set_graphs(irbc_handle* h, int32_t on) {
+  if (!h) return IRBC_ERR_ARG;
+  h->graphs_on = on != 0;
+  if (!h->graphs_on) invalidate_graphs(h);
   return 0;
 }
 

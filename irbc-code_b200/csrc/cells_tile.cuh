@@ -270,7 +270,8 @@ __device__ void cell_from_global(const DevParams& p, Solvent& s, SolventF& f, co
 
 template <bool F32>
 __global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Solvent s, SolventF f, Cells cl,
-                                                               Membrane m, uint64_t epoch) {
+                                                               Membrane m, uint64_t eoff) {
+  const uint64_t epoch = epoch_of(p, eoff);
   __shared__ CellTile tiles[kTileWarps];
   const int lane = threadIdx.x & 31;
   CellTile& t = tiles[threadIdx.x >> 5];

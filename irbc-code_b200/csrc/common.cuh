@@ -18,7 +18,13 @@ struct DevParams {
   int nligx, nligy, nlig;  // ligand grid 0.5 apart (maincode.cpp:77-93)
   int randno;
   uint64_t seed;
+  // the draw epoch (step index) of a launch is *ebase + its offset argument:
+  // the host writes the base once per step call, so that a captured
+  // sequence of steps replays with the right epochs
+  const uint64_t* ebase;
 };
+
+__device__ __forceinline__ uint64_t epoch_of(const DevParams& p, uint64_t off) { return *p.ebase + off; }
 
 // draw streams (counter word 3); the same numbering as the oracle's
 enum : uint32_t { STREAM_INIT = 1, STREAM_COLLIDE_U = 2, STREAM_COLLIDE_N = 3, STREAM_BOND = 4 };

@@ -322,16 +322,19 @@ __device__ __forceinline__ void heavy_particle(const DevParams& p, Solvent& s, S
 // from there (the walk's per-entry test reads no global memory).  The
 // bucket count is reset for the next step.  Blocks from nact on walk the
 // overflow queue (full buckets, lists longer than kHeavyList), a warp per
-// particle, from global memory.
+// particle, from global memory.  nact is read on the device and the grid
+// is sized by the bucket capacity, so a captured launch stays valid across
+// list updates.
 template <bool F32>
 __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, SolventF f,
                                                       const int* __restrict__ lstart, const int* __restrict__ lidx,
                                                       const int* __restrict__ acell, int* bcnt,
                                                       const int* __restrict__ bucket, Snap sn,
                                                       const TriPre* __restrict__ pre, const int* queue,
-                                                      const int* qn, int nact) {
+                                                      const int* qn, const int* __restrict__ nactp) {
   extern __shared__ double sh[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int nact = *nactp;
   if ((int)blockIdx.x >= nact) {
     const int nq = *qn;
     const int64_t gw = (int64_t)(blockIdx.x - nact) * nw + w;
@@ -756,7 +759,8 @@ __global__ void k_tail_a(DevParams p, Membrane m, int* __restrict__ vd, int* __r
 // order with the parasite kick (Src/memfuncs.cpp:469-482, maincode.cpp:736-744).
 __global__ void __launch_bounds__(kTailT) k_tail_b(DevParams p, Membrane m, const int* __restrict__ vd,
                                                    const int* __restrict__ vw, const double* __restrict__ vX,
-                                                   uint64_t epoch) {
+                                                   uint64_t eoff) {
+  const uint64_t epoch = epoch_of(p, eoff);
   __shared__ int s_d[kTailT], s_w[kTailT];
   __shared__ int s_wlist[kWcaList];
   __shared__ double s_wx[kWcaList * 3];
@@ -891,6 +895,18 @@ __global__ void k_snap(DevParams p, Membrane m, Snap sn) {
 }
 
 // ================================================================ launch ======
+// the membrane chain's kernels (the side stream's work): a captured graph
+// gives them the side stream's high priority
+bool is_membrane_kernel(const void* fn) {
+  const void* k[] = {(const void*)k_m_drift, (const void*)k_m_av, (const void*)k_m_sum,
+                     (const void*)k_sum_edges, (const void*)k_force_tri, (const void*)k_force_gather_w,
+                     (const void*)k_tail_a, (const void*)k_tail_b, (const void*)k_kick_snap,
+                     (const void*)k_tri_prep, (const void*)k_snap};
+  for (const void* q : k)
+    if (q == fn) return true;
+  return false;
+}
+
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st) {
   k_snap<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.snap[buf]);
   k_tri_prep<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.pre[buf]);
@@ -904,17 +920,12 @@ void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaS
 template <bool F32>
 static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
                                 cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_stream_cells<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kHeavyList * (int)(sizeof(TriPre) + sizeof(int)));
-    attr_set = true;
-  }
-  const int lmax = c.lmax < kHeavyList ? c.lmax : kHeavyList;
-  const size_t smem = (size_t)lmax * (sizeof(TriPre) + sizeof(int));
-  k_stream_cells<F32><<<c.nact + kOverflowBlocks, 256, smem, st>>>(p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt,
-                                                                  f.bucket, f.snap[buf], f.pre[buf], f.queue,
-                                                                  f.qn, c.nact);
+  const int smem = kHeavyList * (int)(sizeof(TriPre) + sizeof(int));
+  // per device and cheap: set on every call (from any host thread)
+  cudaFuncSetAttribute(k_stream_cells<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, 256, smem, st>>>(
+      p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
+      c.totals + 4);
 }
 
 void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,

@@ -45,6 +45,7 @@ void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, in
                  cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
 // these return the number of kernels they launched
 int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_sum);
+bool is_membrane_kernel(const void* fn);
 int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
                      cudaStream_t st, bool sum_pending);
 

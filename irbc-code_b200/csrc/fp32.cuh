@@ -47,7 +47,8 @@ __device__ __forceinline__ int shifted_cell_f(const DevParams& p, float4 q, cons
   return cell_of(p, fx, fy, fz);
 }
 
-__global__ void k_count_f(DevParams p, SolventF f, int* cnt, int* key, int* slot, uint64_t epoch) {
+__global__ void k_count_f(DevParams p, SolventF f, int* cnt, int* slot, uint64_t eoff) {
+  const uint64_t epoch = epoch_of(p, eoff);
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t o[4];
   draw_block(p.seed, STREAM_COLLIDE_U, epoch, 0, o);
@@ -63,7 +64,7 @@ __global__ void k_count_f(DevParams p, SolventF f, int* cnt, int* key, int* slot
   int base = 0;
   if (lane == leader) base = atomicAdd(&cnt[c], __popc(peers));
   base = __shfl_sync(peers, base, leader);
-  key[i] = c;
+  f.pid[i] = c;  // the cell of this collision
   slot[i] = base + rank;
 }
 
@@ -83,26 +84,36 @@ __global__ void k_gather_f(SolventF f, const int* __restrict__ perm) {
   f.vel2[j] = f.vel[i];
   f.pid2[j] = f.pid[i];
 }
+__global__ void k_copy_back_f(SolventF f) {
+  int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= f.n) return;
+  f.pos[j] = f.pos2[j];
+  f.vel[j] = f.vel2[j];
+  f.pid[j] = f.pid2[j];
+}
 
 void launch_collide_count_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, uint64_t epoch,
                             cudaStream_t st) {
   cudaMemsetAsync(c.cnt, 0, sizeof(int) * c.n, st);
-  if (f.n) k_count_f<<<nbf(f.n, 256), 256, 0, st>>>(p, f, c.cnt, s.key, s.slot, epoch);
+  if (f.n) k_count_f<<<nbf(f.n, 256), 256, 0, st>>>(p, f, c.cnt, s.slot, epoch);
 }
 
 // per-cell statistics (sums in double, reference particle order) and the
 // float rotation: k_cells_tile<true> (cells_tile.cuh)
 void launch_collide_finish_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
-                             cudaStream_t st) {
+                             cudaStream_t st, bool resort) {
   launch_ghost_flags(p, c, m, st);
   launch_scan3(c.cnt, c.wrank, c.mrank, c.start, c.wrank, c.mrank, c.totals, c.n, c.scan_part, st);
   cudaMemcpyAsync(c.start + c.n, c.totals + 0, sizeof(int), cudaMemcpyDeviceToDevice, st);
-  if (f.n) k_perm_f<<<nbf(f.n, 256), 256, 0, st>>>(s.key, s.slot, c.start, f.n, s.perm);
-  std::swap(f.pid, s.key);  // pid = cell of this collision, in place
+  if (f.n) k_perm_f<<<nbf(f.n, 256), 256, 0, st>>>(f.pid, s.slot, c.start, f.n, s.perm);
   k_cells_tile<true><<<cells_tile_blocks(c.n), 32 * kTileWarps, 0, st>>>(p, s, f, c, m, epoch);
-  if (f.n && (++s.ncoll % kResortEvery) == 0) {
+  if (resort) launch_resort_f(f, s, st);
+}
+
+void launch_resort_f(SolventF& f, Solvent& s, cudaStream_t st) {
+  if (f.n) {
     k_gather_f<<<nbf(f.n, 256), 256, 0, st>>>(f, s.perm);
-    std::swap(f.pos, f.pos2); std::swap(f.vel, f.vel2); std::swap(f.pid, f.pid2);
+    k_copy_back_f<<<nbf(f.n, 256), 256, 0, st>>>(f);
   }
 }
 

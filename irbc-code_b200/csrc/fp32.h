@@ -18,7 +18,8 @@ void f32_to_f64(SolventF& f, Solvent& s, cudaStream_t st);
 void launch_collide_count_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, uint64_t epoch,
                             cudaStream_t st);
 void launch_collide_finish_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
-                             cudaStream_t st);
+                             cudaStream_t st, bool resort);
+void launch_resort_f(SolventF& f, Solvent& s, cudaStream_t st);
 // ev0/ev1 (optional) are recorded around the bulk kernel k_stream_f
 void fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb, int buf, cudaStream_t st,
                    cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);

@@ -35,6 +35,9 @@ __global__ void k_init_solvent(DevParams p, Solvent s) {
   s.pid[i] = 0;
 }
 
+__global__ void k_set_u64(uint64_t* d, uint64_t v) { *d = v; }
+void launch_set_u64(uint64_t* d, uint64_t v, cudaStream_t st) { k_set_u64<<<1, 1, 0, st>>>(d, v); }
+
 void launch_init_solvent(const DevParams& p, Solvent& s, cudaStream_t st) {
   if (s.n) k_init_solvent<<<nblk(s.n, 256), 256, 0, st>>>(p, s);
 }
@@ -281,7 +284,8 @@ __device__ __forceinline__ int shifted_cell(const DevParams& p, double x, double
 
 // vertices and parasite into the shifted grid (:149-162); vertex keys sorted
 // by (cell, vertex) with a bitonic sort in shared memory
-__global__ void k_vbin(DevParams p, Membrane m, int* ncm, uint64_t epoch) {
+__global__ void k_vbin(DevParams p, Membrane m, int* ncm, uint64_t eoff) {
+  const uint64_t epoch = epoch_of(p, eoff);
   extern __shared__ uint64_t sk[];
   double r[3];
   grid_shift(p, epoch, r);
@@ -319,7 +323,8 @@ __global__ void k_vbin(DevParams p, Membrane m, int* ncm, uint64_t epoch) {
 }
 
 // cell of each particle in the shifted grid; warp-aggregated slot counters
-__global__ void k_count(DevParams p, Solvent s, int* cnt, uint64_t epoch) {
+__global__ void k_count(DevParams p, Solvent s, int* cnt, uint64_t eoff) {
+  const uint64_t epoch = epoch_of(p, eoff);
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double r[3];
   grid_shift(p, epoch, r);
@@ -334,7 +339,7 @@ __global__ void k_count(DevParams p, Solvent s, int* cnt, uint64_t epoch) {
     int base = 0;
     if (lane == leader) base = atomicAdd(&cnt[c], __popc(peers));
     base = __shfl_sync(peers, base, leader);
-    s.key[i] = c;
+    s.pid[i] = c;  // the cell of this collision (particle.pid)
     s.slot[i] = base + rank;
   }
 }
@@ -365,7 +370,9 @@ __global__ void k_perm(const int* __restrict__ key, const int* __restrict__ slot
 }
 
 // physical re-sort by collision cell (every few collisions, to keep the
-// particles of a cell close in memory): coalesced writes, gathered reads
+// particles of a cell close in memory): gathered into the second buffer set,
+// then copied back, so the arrays never change address (a captured step
+// sequence stays valid)
 __global__ void k_gather(Solvent s) {
   int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= s.n) return;
@@ -374,22 +381,20 @@ __global__ void k_gather(Solvent s) {
   s.v2[j] = s.v[i];
   s.indio2[j] = s.indio[i]; s.pid2[j] = s.pid[i];
 }
-
-
-static void swap_solvent(Solvent& s) {
-  std::swap(s.x, s.x2); std::swap(s.y, s.y2); std::swap(s.z, s.z2);
-  std::swap(s.v, s.v2);
-  std::swap(s.indio, s.indio2); std::swap(s.pid, s.pid2);
+__global__ void k_copy_back(Solvent s) {
+  int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= s.n) return;
+  s.x[j] = s.x2[j]; s.y[j] = s.y2[j]; s.z[j] = s.z2[j];
+  s.v[j] = s.v2[j];
+  s.indio[j] = s.indio2[j]; s.pid[j] = s.pid2[j];
 }
+
 
 void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cudaStream_t st) {
   int n2 = 1;
   while (n2 < p.nv) n2 <<= 1;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
-    attr_set = true;
-  }
+  // per device and cheap: set on every call (from any host thread)
+  cudaFuncSetAttribute(k_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
   cudaMemsetAsync(c.ncm, 0, sizeof(int) * c.n, st);
   k_vbin<<<1, 1024, sizeof(uint64_t) * n2, st>>>(p, m, c.ncm, epoch);
 }
@@ -404,18 +409,21 @@ void launch_collide_count(const DevParams& p, Solvent& s, Cells& c, uint64_t epo
 }
 
 void launch_collide_finish(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
-                           cudaStream_t st) {
+                           cudaStream_t st, bool resort) {
   // wrank/mrank hold the flags first, then their exclusive scans
   k_ghost_flags<<<nblk(c.n, 256), 256, 0, st>>>(p, c.cnt, c.ncm, m.sc, c.wrank, c.mrank);
   launch_scan3(c.cnt, c.wrank, c.mrank, c.start, c.wrank, c.mrank, c.totals, c.n, c.scan_part, st);
   // start[C] = Ns
   cudaMemcpyAsync(c.start + c.n, c.totals + 0, sizeof(int), cudaMemcpyDeviceToDevice, st);
-  if (s.n) k_perm<<<nblk(s.n, 256), 256, 0, st>>>(s.key, s.slot, c.start, s.n, s.perm);
-  std::swap(s.pid, s.key);  // pid = cell of this collision, in place
+  if (s.n) k_perm<<<nblk(s.n, 256), 256, 0, st>>>(s.pid, s.slot, c.start, s.n, s.perm);
   k_cells_tile<false><<<cells_tile_blocks(c.n), 32 * kTileWarps, 0, st>>>(p, s, SolventF{}, c, m, epoch);
-  if (s.n && (++s.ncoll % kResortEvery) == 0) {
+  if (resort) launch_resort(s, st);
+}
+
+void launch_resort(Solvent& s, cudaStream_t st) {
+  if (s.n) {
     k_gather<<<nblk(s.n, 256), 256, 0, st>>>(s);
-    swap_solvent(s);
+    k_copy_back<<<nblk(s.n, 256), 256, 0, st>>>(s);
   }
 }
 
@@ -697,19 +705,20 @@ __global__ void __launch_bounds__(kLTile) k_llist(DevParams p, Cells cl, Membran
 int64_t launch_llist_count(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st) {
   k_tri_centroid<<<nblk(p.nt, 128), 128, 0, st>>>(p, m);
   k_llist<false><<<nblk(c.n, kLTile), kLTile, 0, st>>>(p, c, m);
-  launch_scan3(c.lcnt, nullptr, nullptr, c.lstart2, nullptr, nullptr, c.totals + 3, c.n, c.scan_part, st);
+  launch_scan3(c.lcnt, nullptr, nullptr, c.lstart2, nullptr, nullptr, c.totals + 8, c.n, c.scan_part, st);
   int tot = 0;
-  cudaMemcpyAsync(&tot, c.totals + 3, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&tot, c.totals + 8, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaStreamSynchronize(st);
-  cudaMemcpyAsync(c.lstart2 + c.n, c.totals + 3, sizeof(int), cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(c.lstart2 + c.n, c.totals + 8, sizeof(int), cudaMemcpyDeviceToDevice, st);
   return tot;
 }
 
-void launch_llist_fill(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st) {
+// the new lists are built in the second buffers (the old ones give the
+// stale tails) and copied back, so the list arrays keep their addresses
+void launch_llist_fill(const DevParams& p, Cells& c, const Membrane& m, int64_t total, cudaStream_t st) {
   k_llist<true><<<nblk(c.n, kLTile), kLTile, 0, st>>>(p, c, m);
-  std::swap(c.lstart, c.lstart2);
-  std::swap(c.lidx, c.lidx2);
-  std::swap(c.lcap, c.lcap2);
+  cudaMemcpyAsync(c.lstart, c.lstart2, sizeof(int) * (c.n + 1), cudaMemcpyDeviceToDevice, st);
+  if (total > 0) cudaMemcpyAsync(c.lidx, c.lidx2, sizeof(int) * total, cudaMemcpyDeviceToDevice, st);
 }
 
 // cells with a non-empty list: their rank (lrank), the cell of each rank
@@ -1093,7 +1102,8 @@ __global__ void k_bond_prep(DevParams p, Membrane m, const double* xlig, const d
 
 // bond_dynamics (maincode.cpp:16-54): serial over vertices; draw k of the
 // BOND stream is the reference's k-th RanGen[0].Random() of the step
-__global__ void k_bond_dyn(DevParams p, Membrane m, uint64_t epoch) {
+__global__ void k_bond_dyn(DevParams p, Membrane m, uint64_t eoff) {
+  const uint64_t epoch = epoch_of(p, eoff);
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   uint64_t k = 0;
   for (int ii = 0; ii < p.nv; ++ii) {

@@ -32,7 +32,8 @@ struct Solvent {
   int *indio2 = nullptr, *pid2 = nullptr;
   int *key = nullptr, *slot = nullptr;
   int *perm = nullptr;          // particle indices grouped by collision cell
-  int64_t ncoll = 0;            // collisions so far (physical re-sort cadence)
+  int64_t ncoll = 0;            // collisions so far (host count)
+  int64_t resorted = 0;         // ncoll at the last physical re-sort
 };
 
 // every kResortEvery-th collision also re-sorts the particle arrays
@@ -42,8 +43,8 @@ constexpr int kResortEvery = 16;
 struct Cells {
   int64_t n = 0;
   int *cnt = nullptr, *start = nullptr, *ncm = nullptr, *wrank = nullptr, *mrank = nullptr;
-  int *totals = nullptr;        // [0] particles, [1] wall ghost cells, [2] membrane ghost cells, [3] llist
-                                // entries, [4] cells with a list, [7] longest list
+  int *totals = nullptr;        // [0] particles, [1] wall ghost cells, [2] membrane ghost cells,
+                                // [4] cells with a list, [7] longest list, [8] llist entries
   int *lstart = nullptr, *lidx = nullptr, *lstart2 = nullptr, *lidx2 = nullptr, *lcnt = nullptr;
   int64_t lcap = 0, lcap2 = 0;
   int *lrank = nullptr;         // rank among the cells with a non-empty list
@@ -84,6 +85,8 @@ constexpr int kMaxPairs = 64;        // bond candidates per vertex (<= 25 with d
 
 // ---- launchers (kernels.cu) ---------------------------------------------------
 void launch_init_solvent(const DevParams& p, Solvent& s, cudaStream_t st);
+// *d = v in stream order (no host staging, no host wait)
+void launch_set_u64(uint64_t* d, uint64_t v, cudaStream_t st);
 // velocity records from / to plain arrays (state exchange); a null vx keeps
 // the velocities, a null id keeps the indices
 void launch_pack_vel(Solvent& s, const double* vx, const double* vy, const double* vz, const int* id,
@@ -94,13 +97,17 @@ void launch_classify(const DevParams& p, Solvent& s, const Membrane& m, cudaStre
 // only) in any order or on two streams, then launch_collide_finish
 void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cudaStream_t st);
 void launch_collide_count(const DevParams& p, Solvent& s, Cells& c, uint64_t epoch, cudaStream_t st);
+// resort: also re-sort the arrays physically by this collision's cells
 void launch_collide_finish(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,
-                           cudaStream_t st);
+                           cudaStream_t st, bool resort);
+// physical re-sort by the cells of the latest collision (any time after it)
+void launch_resort(Solvent& s, cudaStream_t st);
 void launch_ghost_flags(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
 void launch_stream(const DevParams& p, Solvent& s, const Cells& c, const Membrane& m, cudaStream_t st);
 // returns the total list length the update needs (host sync inside)
 int64_t launch_llist_count(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
-void launch_llist_fill(const DevParams& p, Cells& c, const Membrane& m, cudaStream_t st);
+// total: the entry count launch_llist_count returned (both list buffers hold it)
+void launch_llist_fill(const DevParams& p, Cells& c, const Membrane& m, int64_t total, cudaStream_t st);
 // lrank / acell / nact / lmax of the current lists (host sync inside);
 // returns the kernels launched, -1 on a CUDA error
 int launch_llist_ranks(const DevParams& p, Cells& c, cudaStream_t st);

@@ -21,6 +21,13 @@ D = C.POINTER(C.c_double)
 I = C.POINTER(C.c_int32)
 
 
+class Result(C.Structure):
+    """irbc_result"""
+    _fields_ = [("id", C.c_int64), ("status", C.c_int32), ("pad_", C.c_int32), ("steps", C.c_int64),
+                ("ns", C.c_int64), ("t_submit", C.c_double), ("t_start", C.c_double), ("t_end", C.c_double),
+                ("obs", C.c_double * 8), ("handle", C.c_void_p)]
+
+
 class IrbcError(RuntimeError):
     pass
 
@@ -108,6 +115,7 @@ def lib():
     L.irbc_launch_count.restype = C.c_int64
     L.irbc_launch_count.argtypes = [H]
     L.irbc_profile_begin.argtypes = [H]
+    L.irbc_set_graphs.argtypes = [H, C.c_int32]
     L.irbc_profile_end.argtypes = [H, D, C.c_int32]
     L.irbc_host_alloc.restype = C.c_void_p
     L.irbc_host_alloc.argtypes = [C.c_size_t]
@@ -115,6 +123,23 @@ def lib():
     L.irbc_bin_particles.argtypes = [C.POINTER(Params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                      C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     L.irbc_bin_particles_noalloc.argtypes = L.irbc_bin_particles.argtypes
+    B = C.c_void_p
+    L.irbc_batch_create.argtypes = [C.c_int32, C.POINTER(B)]
+    L.irbc_batch_destroy.argtypes = [B]
+    L.irbc_batch_destroy.restype = None
+    L.irbc_batch_add.argtypes = [B, H]
+    L.irbc_batch_remove.argtypes = [B, H]
+    L.irbc_batch_size.argtypes = [B]
+    L.irbc_batch_step.argtypes = [B, C.c_int64]
+    L.irbc_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int64, C.POINTER(B)]
+    L.irbc_server_submit.argtypes = [B, C.POINTER(Params), D, C.c_int32, I, C.c_int32, I, C.c_int32, C.c_int32,
+                                     C.c_int64, C.c_int32, C.POINTER(C.c_int64)]
+    L.irbc_server_poll.argtypes = [B, C.POINTER(Result), C.c_int32, C.c_double]
+    L.irbc_server_status.argtypes = [B, C.POINTER(C.c_int64)]
+    L.irbc_server_clock.restype = C.c_double
+    L.irbc_server_clock.argtypes = [B]
+    L.irbc_server_destroy.argtypes = [B]
+    L.irbc_server_destroy.restype = None
     _lib = L
     return L
 
@@ -198,6 +223,18 @@ class Simulation:
         self.ncell = int(self.L.irbc_ncell(self.h))
         self.nlig = int(self.L.irbc_nlig(self.h))
         self.nv = 0
+
+    @classmethod
+    def adopt(cls, handle, params, nv):
+        """wraps a handle the library created (a server result with keep = 1)"""
+        sim = cls.__new__(cls)
+        sim.L = lib()
+        sim.params = params
+        sim.h = C.c_void_p(handle)
+        sim.ncell = int(sim.L.irbc_ncell(sim.h))
+        sim.nlig = int(sim.L.irbc_nlig(sim.h))
+        sim.nv = nv
+        return sim
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:
@@ -297,6 +334,10 @@ class Simulation:
     def launch_count(self):
         return int(self.L.irbc_launch_count(self.h))
 
+    def set_graphs(self, on):
+        """captured 24-step CUDA graphs in step() (default on)"""
+        self._ck(self.L.irbc_set_graphs(self.h, 1 if on else 0), "irbc_set_graphs")
+
     def profile_begin(self):
         self._ck(self.L.irbc_profile_begin(self.h), "irbc_profile_begin")
 
@@ -307,6 +348,102 @@ class Simulation:
         return dict(total_ms=out[0], stream_ms=out[1], stream_steps=int(out[2]), collide_ms=out[3],
                     collides=int(out[4]), membrane_ms=out[5], membrane_groups=int(out[6]),
                     launches=int(out[7]), bulk_ms=out[8], bulk_launches=int(out[9]))
+
+
+class Batch:
+    """Independent simulations stepped together (irbc_batch_*)."""
+
+    def __init__(self, nthreads=4):
+        self.L = lib()
+        self.b = C.c_void_p()
+        if self.L.irbc_batch_create(nthreads, C.byref(self.b)) != 0:
+            raise IrbcError("irbc_batch_create failed")
+        self.members = []
+
+    def add(self, sim):
+        if self.L.irbc_batch_add(self.b, sim.h) != 0:
+            raise IrbcError("irbc_batch_add failed")
+        self.members.append(sim)
+
+    def remove(self, sim):
+        if self.L.irbc_batch_remove(self.b, sim.h) != 0:
+            raise IrbcError("irbc_batch_remove failed")
+        self.members.remove(sim)
+
+    def step(self, n):
+        rc = self.L.irbc_batch_step(self.b, n)
+        if rc != 0:
+            raise IrbcError("irbc_batch_step failed (%d)" % rc)
+
+    def close(self):
+        if self.b.value:
+            self.L.irbc_batch_destroy(self.b)
+            self.b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request loop over whole simulations (irbc_server_*): admission by
+    device-memory footprint, rounds of round_steps steps, results as they
+    finish."""
+
+    def __init__(self, device=0, budget_bytes=0, nthreads=4, round_steps=240):
+        self.L = lib()
+        self.s = C.c_void_p()
+        rc = self.L.irbc_server_create(device, budget_bytes, nthreads, round_steps, C.byref(self.s))
+        if rc != 0:
+            raise IrbcError("irbc_server_create failed (%d)" % rc)
+        self.params = {}
+
+    def submit(self, params, V, E, T, nknobs, nsteps, keep=False):
+        V = np.ascontiguousarray(V, np.float64)
+        E = np.ascontiguousarray(E, np.int32)
+        T = np.ascontiguousarray(T, np.int32)
+        rid = C.c_int64()
+        rc = self.L.irbc_server_submit(self.s, C.byref(params), _p(V, D), len(V), _p(E, I), len(E), _p(T, I),
+                                       len(T), nknobs, nsteps, 1 if keep else 0, C.byref(rid))
+        if rc != 0:
+            raise IrbcError("irbc_server_submit failed (%d)" % rc)
+        self.params[rid.value] = (params, len(V))
+        return rid.value
+
+    def poll(self, max_results=64, wait=0.0):
+        buf = (Result * max_results)()
+        n = self.L.irbc_server_poll(self.s, buf, max_results, wait)
+        out = []
+        for r in buf[:max(0, n)]:
+            d = dict(id=r.id, status=r.status, steps=r.steps, ns=r.ns, t_submit=r.t_submit, t_start=r.t_start,
+                     t_end=r.t_end, obs=np.array(r.obs[:]), sim=None)
+            if r.handle:
+                params, nv = self.params[r.id]
+                d["sim"] = Simulation.adopt(r.handle, params, nv)
+            out.append(d)
+        return out
+
+    def status(self):
+        out = (C.c_int64 * 6)()
+        self.L.irbc_server_status(self.s, out)
+        return dict(pending=out[0], active=out[1], results=out[2], used=out[3], budget=out[4],
+                    particle_steps=out[5])
+
+    def clock(self):
+        return float(self.L.irbc_server_clock(self.s))
+
+    def close(self):
+        if self.s.value:
+            self.L.irbc_server_destroy(self.s)
+            self.s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class PinnedArray:

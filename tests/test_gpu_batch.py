@@ -1,0 +1,90 @@
+"""Batches and the request server: a simulation computes the same thing
+alone, in a batch, or admitted by the server in a mix with others (bit for
+bit: each keeps its own streams, memory and draw epochs)."""
+import numpy as np
+import pytest
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def _small(seed, ns=20000, precision=0, **over):
+    op, orc = H.make_oracle(ns=ns, seed=seed, **over)
+    import irbc_b200 as G
+    p = H.to_irbc_params(op, seed, precision)
+    return op, p
+
+
+def _run_alone(p, V, E, T, nknobs, steps):
+    import irbc_b200 as G
+    sim = G.Simulation(p)
+    sim.init(V, E, T, nknobs)
+    sim.step(steps)
+    st = sim.get_state()
+    sim.close()
+    return st
+
+
+def test_batch_equals_members_alone():
+    import irbc_b200 as G
+    V, E, T = H.troph()
+    cfgs = [(3, 0, {}), (4, 1, {}), (5, 0, dict(onrate=300.0, offrate=50.0))]
+    sims, params = [], []
+    for seed, prec, over in cfgs:
+        _, p = _small(seed, precision=prec, **over)
+        s = G.Simulation(p)
+        s.init(V, E, T, 300)
+        sims.append(s)
+        params.append(p)
+    b = G.Batch(nthreads=2)
+    for s in sims:
+        b.add(s)
+    b.step(37)
+    b.step(60)
+    for s, p in zip(sims, params):
+        ref = _run_alone(p, V, E, T, 300, 97)
+        assert H.compare(s.get_state(), ref, 0.0) == {}
+    b.close()
+    for s in sims:
+        s.close()
+
+
+def test_server_results_same_alone_and_in_mix():
+    """Six requests with different seeds, rates, precisions and lengths;
+    a budget for two at a time, so later ones wait for memory and join as
+    earlier ones finish.  Every kept result equals the same request run
+    alone, and at most two ran at once."""
+    import irbc_b200 as G
+    V, E, T = H.troph()
+    reqs = []
+    for k in range(6):
+        seed = 20 + k
+        _, p = _small(seed, precision=k % 2, onrate=0.005 * (k + 1), offrate=0.015)
+        reqs.append((p, 100 + 20 * k, 48 + 24 * k))
+    fp = max(G.lib().irbc_footprint_bytes(G.C.byref(p), len(V), len(E), len(T)) for p, _, _ in reqs)
+    srv = G.Server(budget_bytes=int(2.5 * fp), nthreads=2, round_steps=24)
+    ids = {}
+    for p, nk, steps in reqs[:3]:
+        ids[srv.submit(p, V, E, T, nk, steps, keep=True)] = (p, nk, steps)
+    got = srv.poll(8, wait=30.0)
+    for p, nk, steps in reqs[3:]:
+        ids[srv.submit(p, V, E, T, nk, steps, keep=True)] = (p, nk, steps)
+    while len(got) < len(reqs):
+        more = srv.poll(8, wait=60.0)
+        assert more, "server stalled"
+        got += more
+    spans = []
+    for r in got:
+        assert r["status"] == 0
+        p, nk, steps = ids[r["id"]]
+        assert r["steps"] == steps
+        assert r["t_submit"] <= r["t_start"] <= r["t_end"]
+        spans.append((r["t_start"], r["t_end"]))
+        ref = _run_alone(p, V, E, T, nk, steps)
+        assert H.compare(r["sim"].get_state(), ref, 0.0) == {}, r["id"]
+        r["sim"].close()
+    # never more than two admitted at the same time
+    for t, _ in spans:
+        assert sum(1 for a, b in spans if a <= t < b) <= 2
+    srv.close()

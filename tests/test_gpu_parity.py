@@ -234,6 +234,23 @@ def test_pipelined_steps_equal_split_steps():
         assert H.compare(ga, gb, 0.0) == {}, n
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_captured_graphs_equal_plain_launches(precision):
+    """irbc_step launches 24-step stretches as captured CUDA graphs; 250
+    steps (list update at step 83, physical re-sorts between graphs) with
+    graphs must equal the same steps launched one kernel at a time, bit for
+    bit, in both precisions."""
+    op, orc = H.make_oracle(ns=30000, seed=37, onrate=300.0, offrate=50.0)
+    st = orc.get_state()
+    a = H.gpu_like(op, orc, 37, precision=precision, state=st)
+    b = H.gpu_like(op, orc, 37, precision=precision, state=st)
+    b.set_graphs(False)
+    for n in (5, 60, 185):
+        a.step(n)
+        b.step(n)
+        assert H.compare(a.get_state(), b.get_state(), 0.0) == {}, n
+
+
 def test_pipelined_single_steps_match_oracle():
     """irbc_step(1) from the oracle's state, 24 times (two collisions)."""
     import irbc_b200 as G
