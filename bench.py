@@ -133,6 +133,9 @@ def make_params(G, seed, precision):
 
 
 def dist_setup():
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE); NCCL
+    when CUDA is there, gloo otherwise (the CPU tests of the N > 1 path).
+    Ranks run independent replicas: the process group only times them."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -140,9 +143,21 @@ def dist_setup():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
+
+
+def replica_seed(rank):
+    """each rank's replica draws from its own seed"""
+    return 1234 + 7919 * rank
+
+
+def aggregate(ns, steps, world, t_ms):
+    """whole-job particle-steps/s: every rank's particles over the slowest rank's time"""
+    return ns * steps * world / (t_ms * 1e-3)
 
 
 def reduce_max(x, world):
@@ -150,7 +165,8 @@ def reduce_max(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -204,7 +220,7 @@ def run_ours(args):
     import irbc_b200 as G
     from irbc_b200 import mesh
     precision = G.FP32 if args.precision == "fp32" else G.FP64
-    p = make_params(G, seed=1234 + 7919 * rank, precision=precision)
+    p = make_params(G, seed=replica_seed(rank), precision=precision)
     p.device = local
     sim = G.Simulation(p)
     V, E, T = mesh.discocyte()
@@ -220,17 +236,14 @@ def run_ours(args):
         prof = sim.profile_end()
     t_ms = reduce_max(prof["total_ms"], world)
     ns = WORKLOAD["Ns"]
-    value = ns * args.steps * world / (t_ms * 1e-3)
+    value = aggregate(ns, args.steps, world, t_ms)
     # the state must still be physical after the timed steps
     finite = bool(np.isfinite(sim.observables()[:6]).all())
-    # per-phase and per-kernel times: a short window launched kernel by
-    # kernel (the timed steps run as captured graphs, which carry no
-    # per-kernel events), right after the timed steps
-    sim.set_graphs(False)
+    # per-phase and per-kernel times: a short profiled window right after
+    # the timed steps
     sim.profile_begin()
     sim.step(48)
     kprof = sim.profile_end()
-    sim.set_graphs(True)
     # roofline of the dominant kernel, the bulk streaming kernel (one launch
     # per step over every particle): algorithmic bytes per particle = state
     # read + positions written (FP64: positions 3 x 8 and the 32-byte
@@ -266,7 +279,7 @@ def run_ours(args):
                      "kernel_ms_avg": bulk_avg_ms},
         "phase_ms_per_step": {"stream": kprof["stream_ms"] / 48, "collide": kprof["collide_ms"] / 48,
                               "membrane": kprof["membrane_ms"] / 48,
-                              "window": "48 steps launched kernel by kernel after the timed steps"},
+                              "window": "48 steps after the timed steps"},
         "gpu_launches": prof["launches"],
         "clocks": clocks.summary(),
         "state_finite": finite,

@@ -134,9 +134,10 @@ int32_t irbc_nlig(const irbc_handle* h);
  * entry points run the halves either side of the TotalVA call at
  * maincode.cpp:602 (part 1 = :462-602, part 2 = :603-762). */
 int irbc_step(irbc_handle* h, int64_t n);
-/* Not in the reference.  irbc_step launches whole 24-step stretches
- * between list updates as one captured CUDA graph (on by default); on = 0
- * launches every kernel separately.  The results are the same either way. */
+/* Not in the reference.  on = 1: irbc_step launches whole 24-step
+ * stretches between list updates as one captured CUDA graph; on = 0 (the
+ * default) launches every kernel on the two streams.  The results are the
+ * same either way. */
 int irbc_set_graphs(irbc_handle* h, int32_t on);
 int irbc_step_part1(irbc_handle* h);
 int irbc_step_part2(irbc_handle* h);

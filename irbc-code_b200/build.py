@@ -11,7 +11,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libirbc.so")
+MAIN = os.path.join(HERE, "MAIN")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CXX = os.environ.get("IRBC_CXX", "g++")
+CUDA_LIB = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-O2",
          "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
@@ -48,6 +51,15 @@ def build(verbose=False):
         if r.returncode:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link failed")
+    # MAIN: the reference's command line over the library
+    src = os.path.join(HERE, "main.cpp")
+    if _newer(MAIN, [src, LIB, os.path.join(ROOT, "include", "irbc.h")]):
+        cmd = [CXX, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), src, "-o", MAIN, "-L" + HERE,
+               "-lirbc", "-L" + CUDA_LIB, "-lcudart", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + CUDA_LIB]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("MAIN failed to build")
     return LIB
 
 

@@ -47,7 +47,7 @@ struct irbc_handle {
     int64_t launches = 0, collisions = 0;
   };
   std::vector<StepGraph> graphs;
-  bool graphs_on = true;
+  bool graphs_on = false;  // measured slower than stream launches on the large box: opt in
   bool capturing = false;
   std::string err;
   bool have_mesh = false;

@@ -247,29 +247,56 @@ __global__ void __launch_bounds__(256) k_stream_fast(DevParams p, Solvent s, con
   if (VX != VX0 || VY != VY0 || VZ != VZ0 || VX0 != VX0) { s.v[i].vx = VX; s.v[i].vy = VY; s.v[i].vz = VZ; }
 }
 
+// reflectionFed's crossing test on the precomputed normals (the use_pre
+// case of tri_visit, :461-517): whether the full test can hit
+__device__ __forceinline__ bool tri_crossing(const DevParams& p, const TriPre& q, double X, double Y, double Z,
+                                             double VX, double VY, double VZ, int indio) {
+  const double rstep = 0.0, dtmd = p.dtmd;
+  double PSt0 = X - q.A1[0], PSt1 = Y - q.A1[1], PSt2 = Z - q.A1[2];
+  double PD0 = (X + VX * (dtmd - rstep)) - q.A2[0];
+  double PD1 = (Y + VY * (dtmd - rstep)) - q.A2[1];
+  double PD2 = (Z + VZ * (dtmd - rstep)) - q.A2[2];
+  const double bt = q.X[0] * PSt0 + q.X[1] * PSt1 + q.X[2] * PSt2;
+  const double bdt = q.Xdt[0] * PD0 + q.Xdt[1] * PD1 + q.Xdt[2] * PD2;
+  int flg = 0;
+  if ((indio == 1) && (bt < 0)) flg = 1;
+  if ((indio == 0) && (bt > 0)) flg = 1;
+  return (bt * bdt <= 0) && (flg == 0);
+}
+
 // The triangle walk of reflectionFed for one particle, by a whole warp:
-// lanes test 32 list entries at a time on copies of the particle state; the
-// first entry that would hit (lowest list position) is applied on every lane
-// and testing resumes after it with the updated state -- the same sequence
-// of states as the reference's sequential loop.  tri(e) gives the TriPre of
-// list entry e, jj(e) its triangle.
+// lanes run the crossing test on 32 list entries at a time; the crossing
+// candidates, lowest list position first, get the full test (contact time,
+// barycentric test) on every lane; the first hit is applied and testing
+// resumes after it with the updated state -- the same sequence of states as
+// the reference's sequential loop.  Inside the periodic stencil bands every
+// entry gets the full test (its shifted corners are not precomputed).
+// tri(e) gives the TriPre of list entry e, jj(e) its triangle.
 template <class TriAt, class IdAt>
 __device__ __forceinline__ void heavy_walk(const DevParams& p, const Snap& sn, TriAt tri, IdAt jj, int len, int lane,
                                            int indio, double& X, double& Y, double& Z, double& VX, double& VY,
                                            double& VZ, double& fulldt) {
   int cur = 0;
   while (cur < len) {
-    bool found = false;
+    const bool pre = !in_stencil(p, X, Y);
     const int e = cur + lane;
-    if (e < len) {
+    bool cand = false;
+    if (e < len) cand = pre ? tri_crossing(p, tri(e), X, Y, Z, VX, VY, VZ, indio) : true;
+    unsigned ball = __ballot_sync(0xffffffffu, cand);
+    bool hit = false;
+    while (ball) {
+      const int k = cur + __ffs(ball) - 1;
       double x = X, y = Y, z = Z, vx = VX, vy = VY, vz = VZ, fd = 0.0;
-      found = tri_visit(p, sn, tri(e), jj(e), x, y, z, vx, vy, vz, indio, fd, !in_stencil(p, X, Y));
+      if (tri_visit(p, sn, tri(k), jj(k), x, y, z, vx, vy, vz, indio, fd, pre)) {
+        X = x; Y = y; Z = z; VX = vx; VY = vy; VZ = vz;
+        fulldt += fd;
+        cur = k + 1;
+        hit = true;
+        break;
+      }
+      ball &= ball - 1;
     }
-    const unsigned ball = __ballot_sync(0xffffffffu, found);
-    if (ball == 0) { cur += 32; continue; }
-    const int first = cur + __ffs(ball) - 1;
-    tri_visit(p, sn, tri(first), jj(first), X, Y, Z, VX, VY, VZ, indio, fulldt, !in_stencil(p, X, Y));
-    cur = first + 1;
+    if (!hit) cur += 32;
   }
 }
 

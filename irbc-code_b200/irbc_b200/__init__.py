@@ -335,7 +335,7 @@ class Simulation:
         return int(self.L.irbc_launch_count(self.h))
 
     def set_graphs(self, on):
-        """captured 24-step CUDA graphs in step() (default on)"""
+        """captured 24-step CUDA graphs in step() (default off)"""
         self._ck(self.L.irbc_set_graphs(self.h, 1 if on else 0), "irbc_set_graphs")
 
     def profile_begin(self):

@@ -244,6 +244,7 @@ def test_captured_graphs_equal_plain_launches(precision):
     st = orc.get_state()
     a = H.gpu_like(op, orc, 37, precision=precision, state=st)
     b = H.gpu_like(op, orc, 37, precision=precision, state=st)
+    a.set_graphs(True)
     b.set_graphs(False)
     for n in (5, 60, 185):
         a.step(n)
