@@ -461,6 +461,9 @@ void stream_any(irbc_handle* h, int buf, cudaStream_t st) {
     e0 = next_event(h);
     e1 = next_event(h);
   }
+  // the staging capacity follows the longest list; captured steps keep the
+  // largest, so that a replay stays valid after the lists grow
+  h->fb.hcap = (h->graphs_on || h->capturing) ? kHeavyList : heavy_cap(h->c.lmax);
   if (h->fp32) fast_stream_f(h->dp, h->sf, h->c, h->fb, buf, st, e0, e1);
   else fast_stream(h->dp, h->s, h->c, h->fb, buf, st, e0, e1);
 }
@@ -953,30 +956,22 @@ extern "C" int irbc_get_state(irbc_handle* h, irbc_view* v) {
   CK(cudaStreamSynchronize(h->st));
   const int64_t n = s.n;
   if (v->sx && n) {
-    std::vector<int> id(n);
-    std::vector<double> buf(n);
-    std::vector<int> ibuf(n);
-    launch_unpack_vel(s, s.x2, s.y2, s.z2, s.key, h->st);
+    // un-permuted on the device into the second buffer set, then copied
+    // straight into the caller's arrays
+    int* bad = h->c.totals + 11;
+    CK(cudaMemsetAsync(bad, 0, sizeof(int), h->st));
+    launch_unpermute(s, 0, bad, h->st);
     g_launches += 1;
-    if (down(h, id.data(), s.key, n)) return IRBC_ERR_CUDA;
-    CK(cudaStreamSynchronize(h->st));
-    for (int64_t i = 0; i < n; ++i)
-      if (id[i] < 0 || id[i] >= n) return fail(h, IRBC_ERR_STATE, "corrupt particle ids");
-    auto pull = [&](double* dst, const double* src) -> int {
-      if (down(h, buf.data(), src, n)) return IRBC_ERR_CUDA;
-      if (cudaStreamSynchronize(h->st) != cudaSuccess) return IRBC_ERR_CUDA;
-      for (int64_t i = 0; i < n; ++i) dst[id[i]] = buf[i];
-      return 0;
-    };
-    auto pulli = [&](int* dst, const int* src) -> int {
-      if (down(h, ibuf.data(), src, n)) return IRBC_ERR_CUDA;
-      if (cudaStreamSynchronize(h->st) != cudaSuccess) return IRBC_ERR_CUDA;
-      for (int64_t i = 0; i < n; ++i) dst[id[i]] = ibuf[i];
-      return 0;
-    };
-    if (pull(v->sx, s.x) || pull(v->sy, s.y) || pull(v->sz, s.z) || pull(v->svx, s.x2) || pull(v->svy, s.y2) ||
-        pull(v->svz, s.z2) || pulli(v->spid, s.pid) || pulli(v->sindio, s.indio))
+    if (down(h, v->sx, s.x2, n) || down(h, v->sy, s.y2, n) || down(h, v->sz, s.z2, n) ||
+        down(h, v->spid, s.pid2, n) || down(h, v->sindio, s.indio2, n))
       return IRBC_ERR_CUDA;
+    launch_unpermute(s, 1, bad, h->st);
+    g_launches += 1;
+    if (down(h, v->svx, s.x2, n) || down(h, v->svy, s.y2, n) || down(h, v->svz, s.z2, n)) return IRBC_ERR_CUDA;
+    int nbad = 0;
+    CK(cudaMemcpyAsync(&nbad, bad, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (nbad) return fail(h, IRBC_ERR_STATE, "corrupt particle ids");
   }
   const int nv = m.nv;
   if (v->x && nv) {

@@ -48,9 +48,24 @@ __device__ __forceinline__ float4 rotate_f(float4 v, const double* P, float cosa
 // particles in reference order (vel_at(q, v) yields the q-th); rotates the
 // cell's vertices and the parasite.  Sums in the order of :164-258: solvent,
 // wall ghost, vertices in vertex order, parasite, membrane ghost.
+// the per-cell values cell_par reads besides the velocities; loaded before
+// the tile's gather so that their latency overlaps it
+struct CellLook {
+  int nmem, wrank, mrank, para, nwall;
+};
+__device__ __forceinline__ CellLook look_cell(const Cells& cl, const Membrane& m, int64_t c) {
+  CellLook k;
+  k.nmem = cl.ncm[c];
+  k.wrank = cl.wrank[c];
+  k.mrank = cl.mrank[c];
+  k.para = (c == m.sc->paraid) ? 1 : 0;
+  k.nwall = cl.totals[1];
+  return k;
+}
+
 template <class VelAt>
 __device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, const Membrane& m, uint64_t epoch,
-                                         int64_t c, int n, VelAt vel_at, double P[7]) {
+                                         int64_t c, int n, const CellLook& look, VelAt vel_at, double P[7]) {
   const MemScalars* sc = m.sc;
   double vcm[3] = {0.0, 0.0, 0.0}, ncc = 0.0;
   int nc = 0;
@@ -63,13 +78,13 @@ __device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, co
     ncc += (1 * p.mass);
     nc += 1;
   }
-  const int k = (int)(c % p.nz);
+  const int k = c < 0x7fffffff ? (int)((unsigned)c % (unsigned)p.nz) : (int)(c % p.nz);
   const double zmin = -1.0 + (double)k * p.a, zmax = -1.0 + (double)k * p.a + p.a;
   {
     // wall ghost particle (:185-204): mean (navg - n) * wallspeed in x at the top
     int nn = nc;
     if ((zmax >= p.Lz || zmin <= 0) && nn < p.navg) {
-      const uint64_t g = 3 * (uint64_t)cl.wrank[c];
+      const uint64_t g = 3 * (uint64_t)look.wrank;
       const double sd = sqrt((p.navg - nn) * p.Theta / p.mass);
       const double mx = zmax >= p.Lz ? (p.navg - nn) * p.wallspeed : 0.0;
       vcm[0] += p.mass * (draw_normal(p.seed, STREAM_COLLIDE_N, epoch, g + 0) * sd + mx);
@@ -79,7 +94,7 @@ __device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, co
     }
   }
   // vertices of this cell: their range in the sorted (cell, vertex) keys
-  const int nmem = cl.ncm[c];
+  const int nmem = look.nmem;
   int v0 = 0;
   if (nmem > 0) {
     int lo = 0, hi = p.nv;
@@ -95,7 +110,7 @@ __device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, co
       nc += 1;
     }
   }
-  const bool has_para = (c == sc->paraid);
+  const bool has_para = look.para != 0;
   if (has_para) {
     vcm[0] += p.PRmass * sc->paraV[0];
     vcm[1] += p.PRmass * sc->paraV[1];
@@ -107,7 +122,7 @@ __device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, co
     // membrane ghost (:236-244)
     int nn = nc;
     if ((nn < p.navg) && (nmem > 0)) {
-      const uint64_t g = 3 * ((uint64_t)cl.totals[1] + (uint64_t)cl.mrank[c]);
+      const uint64_t g = 3 * ((uint64_t)look.nwall + (uint64_t)look.mrank);
       const double sd = sqrt((p.navg - nn) * p.Theta / p.mass);
       vcm[0] += p.mass * (draw_normal(p.seed, STREAM_COLLIDE_N, epoch, g + 0) * sd + 0);
       vcm[1] += p.mass * (draw_normal(p.seed, STREAM_COLLIDE_N, epoch, g + 1) * sd + 0);
@@ -175,7 +190,7 @@ __device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, co
 constexpr int kTileCells = 32;   // cells per warp (one per lane)
 constexpr int kTileCap = 400;    // particles a tile holds in shared memory (mean 32 * navg)
 constexpr int kTileWarps = 2;    // warps per block
-constexpr int kTileBatch = 8;    // gathers in flight per lane
+constexpr int kTilePer = (kTileCap + 31) / 32;  // gathers in flight per lane (the whole tile)
 constexpr int kMaxSeg = 48;      // fallback: cells up to this size sort in registers
 
 // one warp's tile, in perm order; ord lists each cell's particles in
@@ -259,7 +274,8 @@ __device__ void cell_from_global(const DevParams& p, Solvent& s, SolventF& f, co
     return cur_at;
   };
   double P[7];
-  cell_par(p, cl, m, epoch, c, n, [&](int q, double v[3]) { int id; load_particle<F32>(s, f, nth(q), id, v); }, P);
+  cell_par(p, cl, m, epoch, c, n, look_cell(cl, m, c),
+           [&](int q, double v[3]) { int id; load_particle<F32>(s, f, nth(q), id, v); }, P);
   for (int q = 0; q < n; ++q) {
     int id;
     double v[3];
@@ -296,21 +312,27 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Sol
     const int e = t.st[lane + 1];
     for (int j = stl; j < e; ++j) t.cell[j] = (unsigned char)lane;
   }
-  // gather: one record per particle, kTileBatch independent loads per lane
-  for (int j0 = 0; j0 < total; j0 += 32 * kTileBatch) {
-    int qv[kTileBatch], idv[kTileBatch];
-    double vv[kTileBatch][3];
+  // this lane's cell values, in flight during the gather
+  CellLook look{};
+  if (lane < ncl) look = look_cell(cl, m, c0 + lane);
+  // gather: one record per particle; every perm entry of the tile is
+  // loaded first (coalesced), then every record, so the tile waits for
+  // two memory latencies, not two per batch.  Each lane keeps its slots'
+  // particle indices and reference indices for the write-back.
+  int qv[kTilePer], idv[kTilePer];
+  {
+    double vv[kTilePer][3];
 #pragma unroll
-    for (int u = 0; u < kTileBatch; ++u) {
-      const int j = j0 + u * 32 + lane;
+    for (int u = 0; u < kTilePer; ++u) {
+      const int j = u * 32 + lane;
       qv[u] = j < total ? perm[S0 + j] : -1;
     }
 #pragma unroll
-    for (int u = 0; u < kTileBatch; ++u)
+    for (int u = 0; u < kTilePer; ++u)
       if (qv[u] >= 0) load_particle<F32>(s, f, qv[u], idv[u], vv[u]);
 #pragma unroll
-    for (int u = 0; u < kTileBatch; ++u) {
-      const int j = j0 + u * 32 + lane;
+    for (int u = 0; u < kTilePer; ++u) {
+      const int j = u * 32 + lane;
       if (qv[u] >= 0) {
         t.id[j] = idv[u];
         t.vx[j] = vv[u][0]; t.vy[j] = vv[u][1]; t.vz[j] = vv[u][2];
@@ -331,7 +353,7 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Sol
   if (lane < ncl) {
     const int b = stl, n = t.st[lane + 1] - stl;
     double P[7];
-    cell_par(p, cl, m, epoch, c0 + lane, n,
+    cell_par(p, cl, m, epoch, c0 + lane, n, look,
              [&](int q, double v[3]) {
                const int j = t.ord[b + q];
                v[0] = t.vx[j]; v[1] = t.vy[j]; v[2] = t.vz[j];
@@ -340,11 +362,14 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Sol
     for (int e = 0; e < 7; ++e) t.P[lane][e] = P[e];
   }
   __syncwarp();
-  // rotation and write-back, in perm order (perm is read again from L2)
-#pragma unroll 2
-  for (int j = lane; j < total; j += 32) {
-    const double v[3] = {t.vx[j], t.vy[j], t.vz[j]};
-    store_rotated<F32>(p, s, f, perm[S0 + j], t.id[j], v, t.P[t.cell[j]]);
+  // rotation and write-back of this lane's slots
+#pragma unroll
+  for (int u = 0; u < kTilePer; ++u) {
+    const int j = u * 32 + lane;
+    if (qv[u] >= 0) {
+      const double v[3] = {t.vx[j], t.vy[j], t.vz[j]};
+      store_rotated<F32>(p, s, f, qv[u], idv[u], v, t.P[t.cell[j]]);
+    }
   }
 }
 

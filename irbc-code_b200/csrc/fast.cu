@@ -5,6 +5,7 @@
 // the solvent kernels.
 //
 // Results equal the one-kernel-per-phase path (kernels.cu) bit for bit.
+#include <algorithm>
 #include <cstdio>
 #include "fast.h"
 #include "fp32.h"
@@ -210,9 +211,9 @@ __device__ __forceinline__ bool in_stencil(const DevParams& p, double x, double 
 // cell (rank lrank among the listed cells) when the list fits the shared
 // staging of k_stream_cells and the bucket has room, else onto the overflow
 // queue
-__device__ __forceinline__ void hand_off(const int* __restrict__ lrank, int pid, int len, int i, int* bcnt,
-                                         int* bucket, int* queue, int* qn) {
-  if (len <= kHeavyList) {
+__device__ __forceinline__ void hand_off(const int* __restrict__ lrank, int pid, int len, int hcap, int i,
+                                         int* bcnt, int* bucket, int* queue, int* qn) {
+  if (len <= hcap) {
     const int a = lrank[pid];
     const int slot = atomicAdd(bcnt + a, 1);
     if (slot < kBucket) { bucket[(int64_t)a * kBucket + slot] = i; return; }
@@ -226,7 +227,7 @@ __device__ __forceinline__ void hand_off(const int* __restrict__ lrank, int pid,
 // untouched here
 __global__ void __launch_bounds__(256) k_stream_fast(DevParams p, Solvent s, const int* __restrict__ lstart,
                                                      const int* __restrict__ lrank, int* bcnt, int* bucket,
-                                                     int* queue, int* qn) {
+                                                     int* queue, int* qn, int hcap) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.n) return;
   double X = s.x[i], Y = s.y[i], Z = s.z[i];
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(256) k_stream_fast(DevParams p, Solvent s, con
   int pid = cell_of(p, fx, fy, fz);
   const int l0 = __ldg(lstart + pid), l1 = __ldg(lstart + pid + 1);
   if (l1 > l0) {
-    hand_off(lrank, pid, l1 - l0, (int)i, bcnt, bucket, queue, qn);
+    hand_off(lrank, pid, l1 - l0, hcap, (int)i, bcnt, bucket, queue, qn);
     return;
   }
   finish_stream(p, 0.0, X, Y, Z, VX, VY, VZ);
@@ -265,13 +266,15 @@ __device__ __forceinline__ bool tri_crossing(const DevParams& p, const TriPre& q
 }
 
 // The triangle walk of reflectionFed for one particle, by a whole warp:
-// lanes run the crossing test on 32 list entries at a time; the crossing
-// candidates, lowest list position first, get the full test (contact time,
-// barycentric test) on every lane; the first hit is applied and testing
+// lanes run the crossing test on 32 list entries at a time, and every
+// crossing candidate gets the full test (contact time, barycentric test) on
+// its own lane, all from the same particle state.  The reference's loop
+// changes the state only at a hit, so up to and including the first hit of
+// the 32 these are exactly its tests: the lowest hit is applied and the walk
 // resumes after it with the updated state -- the same sequence of states as
-// the reference's sequential loop.  Inside the periodic stencil bands every
-// entry gets the full test (its shifted corners are not precomputed).
-// tri(e) gives the TriPre of list entry e, jj(e) its triangle.
+// the sequential loop.  Inside the periodic stencil bands every entry gets
+// the full test (its shifted corners are not precomputed).  tri(e) gives the
+// TriPre of list entry e, jj(e) its triangle.
 template <class TriAt, class IdAt>
 __device__ __forceinline__ void heavy_walk(const DevParams& p, const Snap& sn, TriAt tri, IdAt jj, int len, int lane,
                                            int indio, double& X, double& Y, double& Z, double& VX, double& VY,
@@ -282,21 +285,22 @@ __device__ __forceinline__ void heavy_walk(const DevParams& p, const Snap& sn, T
     const int e = cur + lane;
     bool cand = false;
     if (e < len) cand = pre ? tri_crossing(p, tri(e), X, Y, Z, VX, VY, VZ, indio) : true;
-    unsigned ball = __ballot_sync(0xffffffffu, cand);
-    bool hit = false;
-    while (ball) {
-      const int k = cur + __ffs(ball) - 1;
-      double x = X, y = Y, z = Z, vx = VX, vy = VY, vz = VZ, fd = 0.0;
-      if (tri_visit(p, sn, tri(k), jj(k), x, y, z, vx, vy, vz, indio, fd, pre)) {
-        X = x; Y = y; Z = z; VX = vx; VY = vy; VZ = vz;
-        fulldt += fd;
-        cur = k + 1;
-        hit = true;
-        break;
-      }
-      ball &= ball - 1;
+    double x = X, y = Y, z = Z, vx = VX, vy = VY, vz = VZ, fd = 0.0;
+    const bool hit = cand && tri_visit(p, sn, tri(e), jj(e), x, y, z, vx, vy, vz, indio, fd, pre);
+    const unsigned hb = __ballot_sync(0xffffffffu, hit);
+    if (hb == 0u) {
+      cur += 32;
+      continue;
     }
-    if (!hit) cur += 32;
+    const int src = __ffs(hb) - 1;
+    X = __shfl_sync(0xffffffffu, x, src);
+    Y = __shfl_sync(0xffffffffu, y, src);
+    Z = __shfl_sync(0xffffffffu, z, src);
+    VX = __shfl_sync(0xffffffffu, vx, src);
+    VY = __shfl_sync(0xffffffffu, vy, src);
+    VZ = __shfl_sync(0xffffffffu, vz, src);
+    fulldt += __shfl_sync(0xffffffffu, fd, src);
+    cur += src + 1;
   }
 }
 
@@ -391,7 +395,7 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
   const int n = s_n;
   if (n == 0) return;
   const int c = acell[a];
-  const int l0 = lstart[c], len = lstart[c + 1] - l0;  // len <= kHeavyList (hand_off)
+  const int l0 = lstart[c], len = lstart[c + 1] - l0;  // len <= hcap (hand_off)
   TriPre* st = reinterpret_cast<TriPre*>(sh);
   int* sj = reinterpret_cast<int*>(st + len);
   for (int e = threadIdx.x; e < len; e += blockDim.x) {
@@ -553,8 +557,7 @@ constexpr int kTailT = 1024, kTailDraws = 4096, kWcaList = 512;
 // reading shared memory.
 
 // drift + image counters (maincode.cpp:566-574) and parasite drift (:576-598)
-__global__ void k_m_drift(DevParams p, Membrane m) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void m_drift_item(const DevParams& p, Membrane& m, int i) {
   if (i < p.nv) {
     double x = m.x[i], y = m.y[i], z = m.z[i];
     x += (m.vx[i] * p.dtmd);
@@ -576,10 +579,10 @@ __global__ void k_m_drift(DevParams p, Membrane m) {
     else if (sc->para[1] < 0) { sc->para[1] += p.Ly; sc->parady -= 1; }
   }
 }
+__global__ void k_m_drift(DevParams p, Membrane m) { m_drift_item(p, m, blockIdx.x * blockDim.x + threadIdx.x); }
 
 // Areatri / Voltri terms per triangle (Src/memfuncs.cpp:124-157)
-__global__ void k_m_av(DevParams p, Membrane m) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void m_av_item(const DevParams& p, Membrane& m, int i) {
   if (i >= p.nt) return;
   int l1 = m.t1[i], l2 = m.t2[i], l3 = m.t3[i];
   double A[3], B[3], eta[3], Cn[3];
@@ -592,6 +595,7 @@ __global__ void k_m_av(DevParams p, Membrane m) {
   Cn[2] = (m.z[l1] + m.z[l2] + m.z[l3]) / 3.0;
   m.vol[i] = (1.0 / 6.0) * ((eta[0] * Cn[0]) + (eta[1] * Cn[1]) + (eta[2] * Cn[2]));
 }
+__global__ void k_m_av(DevParams p, Membrane m) { m_av_item(p, m, blockIdx.x * blockDim.x + threadIdx.x); }
 
 // TotalVA's sums, left to right in triangle order, from shared memory
 constexpr int kSumSmemT = 12288;
@@ -631,95 +635,12 @@ __global__ void __launch_bounds__(1024) k_m_sum(DevParams p, Membrane m) {
   else if (threadIdx.x == 32) m.sc->Volume = ordered_sum(v, p.nt);
 }
 
-// Block 0: TotalVA's two ordered sums (as k_m_sum).  Blocks 1..: the edge
-// and bending terms, which do not depend on Sarea / Volume, so they overlap
-// the sums.  The triangle terms follow in k_force_tri.
-__global__ void __launch_bounds__(1024) k_sum_edges(DevParams p, Membrane m, double* __restrict__ slot, int do_sum) {
-  if (blockIdx.x == 0) {
-    if (!do_sum) return;
-    extern __shared__ double sh[];
-    const bool staged = p.nt <= kSumSmemT;
-    if (staged) {
-      for (int i = threadIdx.x; i < p.nt; i += blockDim.x) { sh[i] = m.area[i]; sh[p.nt + i] = m.vol[i]; }
-      __syncthreads();
-    }
-    const double* a = staged ? sh : m.area;
-    const double* v = staged ? sh + p.nt : m.vol;
-    if (threadIdx.x == 0) m.sc->Sarea = ordered_sum(a, p.nt);
-    else if (threadIdx.x == 32) m.sc->Volume = ordered_sum(v, p.nt);
-    return;
-  }
-  const int k = (blockIdx.x - 1) * blockDim.x + threadIdx.x;  // 0 .. 2E
-  if (k < p.ne) force_item(p, m, slot, k);
-  else if (k < 2 * p.ne) force_item(p, m, slot, p.nt + k);  // dihedral k - E
-}
-__global__ void k_force_tri(DevParams p, Membrane m, double* __restrict__ slot) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < p.nt) force_item(p, m, slot, p.ne + k);
-}
-
-// warp per vertex: lanes stage the vertex's force slots in shared memory,
-// lanes 0-2 add them up component-wise in the reference's order, lane 0
-// applies pfdt's -X first and the external forces after (maincode.cpp:603-665)
-constexpr int kGW = 4, kGSlots = 64;
-__global__ void __launch_bounds__(32 * kGW) k_force_gather_w(DevParams p, Membrane m, const double* __restrict__ slot,
-                                                           const int* __restrict__ gstart,
-                                                           const int* __restrict__ gidx) {
-  __shared__ double sh[kGW][kGSlots * 3];
-  __shared__ double ffs[kGW][3];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int i = blockIdx.x * kGW + w;
-  if (i >= p.nv) return;
-  const int q0 = gstart[i], q1 = gstart[i + 1];
-  double acc = 0.0;
-  for (int c0 = q0; c0 < q1; c0 += kGSlots) {
-    const int nc = min(kGSlots, q1 - c0);
-    for (int e = lane; e < nc * 3; e += 32) {
-      const int q = e / 3, k = e - 3 * q;
-      sh[w][e] = slot[3 * (int64_t)gidx[c0 + q] + k];
-    }
-    __syncwarp();
-    if (lane < 3)
-      for (int q = 0; q < nc; ++q) acc += sh[w][3 * q + lane];
-    __syncwarp();
-  }
-  if (lane < 3) ffs[w][lane] = acc;
-  __syncwarp();
-  if (lane != 0) return;
-  const MemScalars* sc = m.sc;
-  double f[3] = {m.fx[i], m.fy[i], m.fz[i]};
-  double X[3];
-  if (wca_f(p, m, sc, i, X)) { f[0] -= X[0]; f[1] -= X[1]; f[2] -= X[2]; }
-  f[0] += ffs[w][0]; f[1] += ffs[w][1]; f[2] += ffs[w][2];
-  f[2] += -p.Fg / (double)p.nv;
-  if (m.bondi[i] == 1) {
-    int jj = m.bondl[i];
-    double A[3];
-    A[0] = m.x[i] - m.xlig[jj];
-    A[1] = m.y[i] - m.ylig[jj];
-    A[2] = m.z[i];
-    A[0] -= p.Lx * round(A[0] / p.Lx);
-    A[1] -= p.Ly * round(A[1] / p.Ly);
-    double aa = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
-    A[0] /= aa; A[1] /= aa; A[2] /= aa;
-    if (aa > p.el0) {
-      f[0] += -p.ks * (aa - p.el0) * A[0];
-      f[1] += -p.ks * (aa - p.el0) * A[1];
-      f[2] += -p.ks * (aa - p.el0) * A[2];
-    }
-  }
-  double cc = m.z[i];
-  if (cc < 0.5) f[2] += 300.0 * exp(-50.0 * cc);
-  cc = p.Lz - m.z[i];
-  if (cc < 0.5) f[2] -= 300.0 * exp(-50.0 * cc);
-  m.fx[i] = f[0]; m.fy[i] = f[1]; m.fz[i] = f[2];
-}
-
-// per vertex: bond preparation (maincode.cpp:668-723), second half-kick
-// (:727-733), the number of bond draws and the WCA flag for k_tail_b
-__global__ void k_tail_a(DevParams p, Membrane m, int* __restrict__ vd, int* __restrict__ vw,
-                         double* __restrict__ vX) {
-  int ii = blockIdx.x * blockDim.x + threadIdx.x;
+// per vertex: bond preparation (maincode.cpp:668-723), the number of bond
+// draws and the WCA flag for k_tail_b.  It reads positions (after the
+// drift) and bond states only, so it runs beside the force terms; the
+// second half-kick (:727-733) is applied by the force gather.
+__device__ __forceinline__ void bond_prep_item(const DevParams& p, Membrane& m, int* __restrict__ vd,
+                                            int* __restrict__ vw, double* __restrict__ vX, int ii) {
   if (ii >= p.nv) return;
   double A[3], B[3];
   int nd = 0;
@@ -774,26 +695,131 @@ __global__ void k_tail_a(DevParams p, Membrane m, int* __restrict__ vd, int* __r
   vw[ii] = in_wca ? 1 : 0;
   if (in_wca) { vX[3 * ii] = X[0]; vX[3 * ii + 1] = X[1]; vX[3 * ii + 2] = X[2]; }
   vd[ii] = nd;
-  m.vx[ii] += (m.fx[ii] * p.dtmd / (2.0 * p.pmass));
-  m.vy[ii] += (m.fy[ii] * p.dtmd / (2.0 * p.pmass));
-  m.vz[ii] += (m.fz[ii] * p.dtmd / (2.0 * p.pmass));
 }
+// Block 0: TotalVA's two ordered sums (as k_m_sum).  Blocks 1..: the edge
+// and bending terms and the bond preparation, which do not depend on
+// Sarea / Volume, so they overlap the sums.  The triangle terms follow in
+// k_force_tri.
+__global__ void __launch_bounds__(1024) k_sum_edges(DevParams p, Membrane m, double* __restrict__ slot, int do_sum,
+                                                    int* __restrict__ vd, int* __restrict__ vw,
+                                                    double* __restrict__ vX) {
+  if (blockIdx.x == 0) {
+    if (!do_sum) return;
+    extern __shared__ double sh[];
+    const bool staged = p.nt <= kSumSmemT;
+    if (staged) {
+      for (int i = threadIdx.x; i < p.nt; i += blockDim.x) { sh[i] = m.area[i]; sh[p.nt + i] = m.vol[i]; }
+      __syncthreads();
+    }
+    const double* a = staged ? sh : m.area;
+    const double* v = staged ? sh + p.nt : m.vol;
+    if (threadIdx.x == 0) m.sc->Sarea = ordered_sum(a, p.nt);
+    else if (threadIdx.x == 32) m.sc->Volume = ordered_sum(v, p.nt);
+    return;
+  }
+  const int k = (blockIdx.x - 1) * blockDim.x + threadIdx.x;  // 0 .. 2E + V
+  if (k < p.ne) force_item(p, m, slot, k);
+  else if (k < 2 * p.ne) force_item(p, m, slot, p.nt + k);  // dihedral k - E
+  else bond_prep_item(p, m, vd, vw, vX, k - 2 * p.ne);
+}
+__global__ void k_force_tri(DevParams p, Membrane m, double* __restrict__ slot) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < p.nt) force_item(p, m, slot, p.ne + k);
+}
+
+// warp per vertex: lanes stage the vertex's force slots in shared memory,
+// lanes 0-2 add them up component-wise in the reference's order, lane 0
+// applies pfdt's -X first and the external forces after (maincode.cpp:603-665)
+constexpr int kGW = 4, kGSlots = 64;
+// vertex i by one warp; shw: kGSlots * 3 + 3 doubles of this warp's shared memory
+__device__ __forceinline__ void gather_vertex(const DevParams& p, Membrane& m, const double* __restrict__ slot,
+                                              const int* __restrict__ gstart, const int* __restrict__ gidx, int i,
+                                              int lane, double* shw) {
+  double* ffsw = shw + kGSlots * 3;
+  const int q0 = gstart[i], q1 = gstart[i + 1];
+  double acc = 0.0;
+  for (int c0 = q0; c0 < q1; c0 += kGSlots) {
+    const int nc = min(kGSlots, q1 - c0);
+    for (int e = lane; e < nc * 3; e += 32) {
+      const int q = e / 3, k = e - 3 * q;
+      shw[e] = slot[3 * (int64_t)gidx[c0 + q] + k];
+    }
+    __syncwarp();
+    if (lane < 3)
+      for (int q = 0; q < nc; ++q) acc += shw[3 * q + lane];
+    __syncwarp();
+  }
+  if (lane < 3) ffsw[lane] = acc;
+  __syncwarp();
+  if (lane != 0) return;
+  const MemScalars* sc = m.sc;
+  double f[3] = {m.fx[i], m.fy[i], m.fz[i]};
+  double X[3];
+  if (wca_f(p, m, sc, i, X)) { f[0] -= X[0]; f[1] -= X[1]; f[2] -= X[2]; }
+  f[0] += ffsw[0]; f[1] += ffsw[1]; f[2] += ffsw[2];
+  f[2] += -p.Fg / (double)p.nv;
+  if (m.bondi[i] == 1) {
+    int jj = m.bondl[i];
+    double A[3];
+    A[0] = m.x[i] - m.xlig[jj];
+    A[1] = m.y[i] - m.ylig[jj];
+    A[2] = m.z[i];
+    A[0] -= p.Lx * round(A[0] / p.Lx);
+    A[1] -= p.Ly * round(A[1] / p.Ly);
+    double aa = sqrt(A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+    A[0] /= aa; A[1] /= aa; A[2] /= aa;
+    if (aa > p.el0) {
+      f[0] += -p.ks * (aa - p.el0) * A[0];
+      f[1] += -p.ks * (aa - p.el0) * A[1];
+      f[2] += -p.ks * (aa - p.el0) * A[2];
+    }
+  }
+  double cc = m.z[i];
+  if (cc < 0.5) f[2] += 300.0 * exp(-50.0 * cc);
+  cc = p.Lz - m.z[i];
+  if (cc < 0.5) f[2] -= 300.0 * exp(-50.0 * cc);
+  m.fx[i] = f[0]; m.fy[i] = f[1]; m.fz[i] = f[2];
+  // second half-kick (maincode.cpp:727-733)
+  m.vx[i] += (f[0] * p.dtmd / (2.0 * p.pmass));
+  m.vy[i] += (f[1] * p.dtmd / (2.0 * p.pmass));
+  m.vz[i] += (f[2] * p.dtmd / (2.0 * p.pmass));
+}
+__global__ void __launch_bounds__(32 * kGW) k_force_gather_w(DevParams p, Membrane m, const double* __restrict__ slot,
+                                                           const int* __restrict__ gstart,
+                                                           const int* __restrict__ gidx) {
+  __shared__ double sh[kGW][kGSlots * 3 + 3];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * kGW + w;
+  if (i >= p.nv) return;
+  gather_vertex(p, m, slot, gstart, gidx, i, lane, sh[w]);
+
+}
+
 
 // One CTA: exclusive scans of the per-vertex draw counts and WCA flags (each
 // thread owns a contiguous run of vertices, so order is kept), the bond
 // draws marked as events in parallel and applied in draw order by one warp
 // (bond_dynamics, maincode.cpp:16-54), and pfdt's parasite sum in vertex
 // order with the parasite kick (Src/memfuncs.cpp:469-482, maincode.cpp:736-744).
-__global__ void __launch_bounds__(kTailT) k_tail_b(DevParams p, Membrane m, const int* __restrict__ vd,
-                                                   const int* __restrict__ vw, const double* __restrict__ vX,
-                                                   uint64_t eoff) {
-  const uint64_t epoch = epoch_of(p, eoff);
-  __shared__ int s_d[kTailT], s_w[kTailT];
-  __shared__ int s_wlist[kWcaList];
-  __shared__ double s_wx[kWcaList * 3];
-  __shared__ int s_evv[kTailDraws];
-  __shared__ short s_evr[kTailDraws];
-  __shared__ int s_tot[2];
+struct TailSmem {
+  double s_wx[kWcaList * 3];
+  int s_d[kTailT], s_w[kTailT];
+  int s_wlist[kWcaList];
+  int s_evv[kTailDraws];
+  short s_evr[kTailDraws];
+  int s_tot[2];
+};
+
+// the whole block (at most kTailT threads); S in shared memory
+__device__ void tail_b_block(const DevParams& p, Membrane& m, const int* __restrict__ vd, const int* __restrict__ vw,
+                             const double* __restrict__ vX, uint64_t epoch, TailSmem& S) {
+  int* s_d = S.s_d;
+  int* s_w = S.s_w;
+  int* s_wlist = S.s_wlist;
+  double* s_wx = S.s_wx;
+  int* s_evv = S.s_evv;
+  short* s_evr = S.s_evr;
+  int* s_tot = S.s_tot;
   const int T = blockDim.x, tid = threadIdx.x;
   MemScalars* sc = m.sc;
   const int chunk = (p.nv + T - 1) / T;
@@ -895,11 +921,16 @@ __global__ void __launch_bounds__(kTailT) k_tail_b(DevParams p, Membrane m, cons
     }
   }
 }
+__global__ void __launch_bounds__(kTailT) k_tail_b(DevParams p, Membrane m, const int* __restrict__ vd,
+                                                   const int* __restrict__ vw, const double* __restrict__ vX,
+                                                   uint64_t eoff) {
+  __shared__ TailSmem S;
+  tail_b_block(p, m, vd, vw, vX, epoch_of(p, eoff), S);
+}
 
 // half-kick + snapshot + triangle prep as separate launches (after a
 // collision, or at the first step)
-__global__ void k_kick_snap(DevParams p, Membrane m, Snap sn) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void kick_snap_item(const DevParams& p, Membrane& m, const Snap& sn, int i) {
   if (i >= p.nv) return;
   double vx = m.vx[i] + (m.fx[i] * p.dtmd / (2.0 * p.pmass));
   double vy = m.vy[i] + (m.fy[i] * p.dtmd / (2.0 * p.pmass));
@@ -908,6 +939,9 @@ __global__ void k_kick_snap(DevParams p, Membrane m, Snap sn) {
   m.fx[i] = 0.0; m.fy[i] = 0.0; m.fz[i] = 0.0;
   sn.x[i] = m.x[i]; sn.y[i] = m.y[i]; sn.z[i] = m.z[i];
   sn.vx[i] = vx; sn.vy[i] = vy; sn.vz[i] = vz;
+}
+__global__ void k_kick_snap(DevParams p, Membrane m, Snap sn) {
+  kick_snap_item(p, m, sn, blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void k_tri_prep(DevParams p, Membrane m, TriPre* pre) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -927,7 +961,7 @@ __global__ void k_snap(DevParams p, Membrane m, Snap sn) {
 bool is_membrane_kernel(const void* fn) {
   const void* k[] = {(const void*)k_m_drift, (const void*)k_m_av, (const void*)k_m_sum,
                      (const void*)k_sum_edges, (const void*)k_force_tri, (const void*)k_force_gather_w,
-                     (const void*)k_tail_a, (const void*)k_tail_b, (const void*)k_kick_snap,
+                     (const void*)k_tail_b, (const void*)k_kick_snap,
                      (const void*)k_tri_prep, (const void*)k_snap};
   for (const void* q : k)
     if (q == fn) return true;
@@ -947,7 +981,7 @@ void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaS
 template <bool F32>
 static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
                                 cudaStream_t st) {
-  const int smem = kHeavyList * (int)(sizeof(TriPre) + sizeof(int));
+  const int smem = f.hcap * (int)(sizeof(TriPre) + sizeof(int));
   // per device and cheap: set on every call (from any host thread)
   cudaFuncSetAttribute(k_stream_cells<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, 256, smem, st>>>(
@@ -960,7 +994,8 @@ void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, in
   cudaMemsetAsync(f.qn, 0, sizeof(int), st);
   if (s.n) {
     if (ev0) cudaEventRecord(ev0, st);
-    k_stream_fast<<<nb(s.n, 256), 256, 0, st>>>(p, s, c.lstart, c.lrank, f.bcnt, f.bucket, f.queue, f.qn);
+    k_stream_fast<<<nb(s.n, 256), 256, 0, st>>>(p, s, c.lstart, c.lrank, f.bcnt, f.bucket, f.queue, f.qn,
+                                                 f.hcap);
     if (ev1) cudaEventRecord(ev1, st);
     SolventF none;
     launch_stream_cells<false>(p, s, none, c, f, buf, st);
@@ -992,13 +1027,12 @@ int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoc
                      cudaStream_t st, bool sum_pending) {
   set_sum_attrs();
   const size_t sm = (sum_pending && p.nt <= kSumSmemT) ? 2 * (size_t)p.nt * sizeof(double) : 0;
-  k_sum_edges<<<1 + nb(2 * p.ne, 1024), 1024, sm, st>>>(p, m, f.slot, sum_pending ? 1 : 0);
+  k_sum_edges<<<1 + nb(2 * p.ne + p.nv, 1024), 1024, sm, st>>>(p, m, f.slot, sum_pending ? 1 : 0, f.vd, f.vw, f.vX);
   k_force_tri<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.slot);
   k_force_gather_w<<<nb(p.nv, kGW), 32 * kGW, 0, st>>>(p, m, f.slot, f.gstart, f.gidx);
-  k_tail_a<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.vd, f.vw, f.vX);
   k_tail_b<<<1, kTailT, 0, st>>>(p, m, f.vd, f.vw, f.vX, epoch);
   if (next_kick) fast_kick_prep(p, m, f, next_buf, st);
-  return 5 + (next_kick ? 2 : 0);
+  return 4 + (next_kick ? 2 : 0);
 }
 
 

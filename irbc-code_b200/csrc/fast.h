@@ -30,6 +30,8 @@ struct FastBufs {
   int* bcnt = nullptr;    // particles handed to each listed cell this step (reset by k_stream_cells)
   int* bucket = nullptr;  // kBucket particle slots per listed cell
   int64_t bcap = 0;       // listed cells the buckets have room for
+  int hcap = kHeavyList;  // list entries k_stream_cells stages (its shared memory); longer lists go
+                          // to the overflow queue
   double* slot = nullptr; // force terms: 3 doubles per slot, 4E + 9T + 4E slots
   int* gstart = nullptr;  // per-vertex slot lists in the reference's order
   int* gidx = nullptr;
@@ -40,6 +42,12 @@ struct FastBufs {
 
 void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
+// the staging capacity for lists of at most lmax entries: lmax rounded up
+// to 64, at least 64, at most kHeavyList
+inline int heavy_cap(int lmax) {
+  int c = ((lmax + 63) / 64) * 64;
+  return c < 64 ? 64 : (c > kHeavyList ? kHeavyList : c);
+}
 // ev0/ev1 (optional) are recorded around the bulk kernel k_stream_fast
 void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
                  cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);

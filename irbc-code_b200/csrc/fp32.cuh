@@ -122,7 +122,7 @@ void launch_resort_f(SolventF& f, Solvent& s, cudaStream_t st) {
 // cells with triangles are handed to k_stream_cells<true> (double precision)
 __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const int* __restrict__ lstart,
                                                   const int* __restrict__ lrank, int* bcnt, int* bucket,
-                                                  int* queue, int* qn) {
+                                                  int* queue, int* qn, int hcap) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= f.n) return;
   const float Lx = (float)p.Lx, Ly = (float)p.Ly, Lz = (float)p.Lz, dt = (float)p.dtmd;
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const
   int pid = cell_of(p, fx, fy, fz);
   const int l0 = __ldg(lstart + pid), l1 = __ldg(lstart + pid + 1);
   if (l1 > l0) {
-    hand_off(lrank, pid, l1 - l0, (int)i, bcnt, bucket, queue, qn);
+    hand_off(lrank, pid, l1 - l0, hcap, (int)i, bcnt, bucket, queue, qn);
     return;
   }
   float X = q.x + v.x * dt, Y = q.y + v.y * dt, Z = q.z + v.z * dt;
@@ -159,7 +159,8 @@ void fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb
   cudaMemsetAsync(fb.qn, 0, sizeof(int), st);
   if (f.n) {
     if (ev0) cudaEventRecord(ev0, st);
-    k_stream_f<<<nbf(f.n, 256), 256, 0, st>>>(p, f, c.lstart, c.lrank, fb.bcnt, fb.bucket, fb.queue, fb.qn);
+    k_stream_f<<<nbf(f.n, 256), 256, 0, st>>>(p, f, c.lstart, c.lrank, fb.bcnt, fb.bucket, fb.queue, fb.qn,
+                                              fb.hcap);
     if (ev1) cudaEventRecord(ev1, st);
     Solvent none;
     none.n = f.n;

@@ -66,6 +66,30 @@ void launch_unpack_vel(const Solvent& s, double* vx, double* vy, double* vz, int
   if (s.n) k_unpack_vel<<<nblk(s.n, 256), 256, 0, st>>>(s, vx, vy, vz, id);
 }
 
+// the solvent in reference order (get_state): particle i goes to position
+// id of the second buffer set; velocities = 0 moves positions, cell and
+// flag, velocities = 1 moves the velocities into x2, y2, z2.  Ids out of
+// range are counted in *bad and skipped.
+__global__ void k_unpermute(Solvent s, int velocities, int* bad) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const SolVel r = s.v[i];
+  const int id = r.id;
+  if (id < 0 || id >= s.n) {
+    atomicAdd(bad, 1);
+    return;
+  }
+  if (velocities) {
+    s.x2[id] = r.vx; s.y2[id] = r.vy; s.z2[id] = r.vz;
+  } else {
+    s.x2[id] = s.x[i]; s.y2[id] = s.y[i]; s.z2[id] = s.z[i];
+    s.pid2[id] = s.pid[i]; s.indio2[id] = s.indio[i];
+  }
+}
+void launch_unpermute(const Solvent& s, int velocities, int* bad, cudaStream_t st) {
+  if (s.n) k_unpermute<<<nblk(s.n, 256), 256, 0, st>>>(s, velocities, bad);
+}
+
 // inside/outside ray test, sortsolvent_initial1 (Src/solfuncs.cpp:31-94).
 // Triangle data staged in shared memory tiles: normal X (Normaldt), the
 // three corners and the centroid x (tries[].cmx).

@@ -44,7 +44,8 @@ struct Cells {
   int64_t n = 0;
   int *cnt = nullptr, *start = nullptr, *ncm = nullptr, *wrank = nullptr, *mrank = nullptr;
   int *totals = nullptr;        // [0] particles, [1] wall ghost cells, [2] membrane ghost cells,
-                                // [4] cells with a list, [7] longest list, [8] llist entries
+                                // [4] cells with a list, [7] longest list, [8] llist entries,
+                                // [11] bad particle ids seen by get_state
   int *lstart = nullptr, *lidx = nullptr, *lstart2 = nullptr, *lidx2 = nullptr, *lcnt = nullptr;
   int64_t lcap = 0, lcap2 = 0;
   int *lrank = nullptr;         // rank among the cells with a non-empty list
@@ -92,6 +93,7 @@ void launch_set_u64(uint64_t* d, uint64_t v, cudaStream_t st);
 void launch_pack_vel(Solvent& s, const double* vx, const double* vy, const double* vz, const int* id,
                      cudaStream_t st);
 void launch_unpack_vel(const Solvent& s, double* vx, double* vy, double* vz, int* id, cudaStream_t st);
+void launch_unpermute(const Solvent& s, int velocities, int* bad, cudaStream_t st);
 void launch_classify(const DevParams& p, Solvent& s, const Membrane& m, cudaStream_t st);
 // a collision = launch_vbin (membrane only) + launch_collide_count (solvent
 // only) in any order or on two streams, then launch_collide_finish

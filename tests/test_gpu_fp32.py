@@ -100,3 +100,28 @@ def test_fp32_long_run_stays_physical(base):
     v2r = np.mean(r.a["svx"] ** 2 + r.a["svy"] ** 2 + r.a["svz"] ** 2)
     assert np.isfinite(v2g) and abs(v2g - v2r) / v2r < 0.05
     assert abs(g.s["Sarea"] - r.s["Sarea"]) / r.s["Sarea"] < 0.02
+
+
+def test_precision_study_within_one_percent():
+    """The precision study on the reference's own configuration (define.h
+    box, the shipped mesh, 500 knobs) in developed Couette flow: FP64 and
+    FP32-bulk runs for four seeds, 16,000 steps each, sampled every 160.
+    Temperature, membrane area and volume and the shear rate of the FP32
+    ensemble within 1% of the FP64 ensemble.  The velocity profile and the
+    centre-of-mass velocity are sampling-noise limited over this window:
+    FP32's difference must be within 1%, or within three standard errors
+    of the difference of the ensemble means."""
+    import irbc_b200 as G
+    from irbc_b200 import precision
+    V, E, T = H.troph()
+    p = G.default_params(onrate=0.005, offrate=0.015, Nt=600)
+    study = precision.run_study(p, V, E, T, 500, 16000, 160, seeds=(71, 72, 73, 74))
+    err = precision.compare(study)
+    print(err)
+    for k, v in err.items():
+        assert np.isfinite(v), k
+    assert err["temperature_rel"] < 0.01
+    assert err["area_rel"] < 0.01 and err["volume_rel"] < 0.01
+    assert err["shear_rel"] < max(0.01, 3.0 * err["noise_shear_rel"])
+    assert err["profile_l2_rel"] < max(0.01, 3.0 * err["noise_profile_l2_rel"])
+    assert err["com_velocity_abs"] < max(0.01, 3.0 * err["noise_com_velocity_abs"])
