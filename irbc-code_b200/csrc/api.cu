@@ -454,7 +454,7 @@ struct ProfScope {
 
 // the streaming kernels; in a profiling window the bulk kernel alone is
 // bracketed by a pair of events of its own
-void stream_any(irbc_handle* h, int buf, cudaStream_t st) {
+void stream_any(irbc_handle* h, int buf, cudaStream_t st, cudaEvent_t snap = nullptr) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->prof && !h->capturing) {
     h->ev_marks.push_back({PROF_STREAM_BULK, h->ev_used, h->ev_used + 1});
@@ -464,8 +464,8 @@ void stream_any(irbc_handle* h, int buf, cudaStream_t st) {
   // the staging capacity follows the longest list; captured steps keep the
   // largest, so that a replay stays valid after the lists grow
   h->fb.hcap = (h->graphs_on || h->capturing) ? kHeavyList : heavy_cap(h->c.lmax);
-  if (h->fp32) fast_stream_f(h->dp, h->sf, h->c, h->fb, buf, st, e0, e1);
-  else fast_stream(h->dp, h->s, h->c, h->fb, buf, st, e0, e1);
+  if (h->fp32) fast_stream_f(h->dp, h->sf, h->c, h->fb, buf, st, e0, e1, snap);
+  else fast_stream(h->dp, h->s, h->c, h->fb, buf, st, e0, e1, snap);
 }
 
 }  // namespace
@@ -1163,19 +1163,23 @@ static int step_one(irbc_handle* h, int64_t eoff, bool last, bool dry) {
   const bool next_collides = (h->colsteps + 1 == h->csteps);
   const int next_kick = (!last && !next_collides) ? 1 : 0;
   if (!dry) {
+    // The streams meet only where they share data.  The bulk streaming
+    // kernel reads no membrane data and starts at once; the near-membrane
+    // kernel waits for the snapshot `buf` (ev_snap: the side stream so far).
+    // The membrane step runs on, and only its writing of the next snapshot
+    // (buf ^ 1) waits for the streaming that last read that buffer.
     CK(cudaEventRecord(h->ev_snap, ss));
-    CK(cudaStreamWaitEvent(ms, h->ev_snap, 0));
     {
       ProfScope ps(h, PROF_STREAM, ms);
-      stream_any(h, buf, ms);
+      stream_any(h, buf, ms, h->ev_snap);
     }
     g_launches += 2;
     CK(cudaEventRecord(h->ev_str[buf], ms));
-    CK(cudaStreamWaitEvent(ss, h->ev_str[buf ^ 1], 0));
     {
       ProfScope ps(h, PROF_MEMBRANE, ss);
       g_launches += fast_drift_va(h->dp, h->m, ss, false);
-      g_launches += fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)eoff, next_kick, buf ^ 1, ss, true);
+      g_launches += fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)eoff, next_kick, buf ^ 1, ss, true,
+                                     h->ev_str[buf ^ 1]);
     }
     CK(cudaEventRecord(h->ev_mem, ss));
   }

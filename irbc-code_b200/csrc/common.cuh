@@ -72,6 +72,16 @@ __device__ inline double draw_normal(uint64_t seed, uint32_t stream, uint64_t ep
   return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
 }
 
+// the collision grid's random shift (Src/solfuncs.cpp:116-118): uniforms 0, 1, 2 of the
+// COLLIDE_U stream, times a
+__device__ __forceinline__ void grid_shift(const DevParams& p, uint64_t epoch, double r[3]) {
+  uint32_t o[4];
+  draw_block(p.seed, STREAM_COLLIDE_U, epoch, 0, o);
+  r[0] = p.a * ((double)o[0] * (1.0 / 4294967296.0));
+  r[1] = p.a * ((double)o[1] * (1.0 / 4294967296.0));
+  r[2] = p.a * ((double)o[2] * (1.0 / 4294967296.0));
+}
+
 // periodic wrap by repeated subtraction (bbound, Src/solfuncs.cpp:603-622).
 // The reference's loop never ends for an infinite coordinate and runs for
 // ages for a huge one (reachable only through a degenerate contact time);

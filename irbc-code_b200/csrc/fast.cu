@@ -990,13 +990,14 @@ static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, co
 }
 
 void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
-                 cudaEvent_t ev0, cudaEvent_t ev1) {
+                 cudaEvent_t ev0, cudaEvent_t ev1, cudaEvent_t snap) {
   cudaMemsetAsync(f.qn, 0, sizeof(int), st);
   if (s.n) {
     if (ev0) cudaEventRecord(ev0, st);
     k_stream_fast<<<nb(s.n, 256), 256, 0, st>>>(p, s, c.lstart, c.lrank, f.bcnt, f.bucket, f.queue, f.qn,
                                                  f.hcap);
     if (ev1) cudaEventRecord(ev1, st);
+    if (snap) cudaStreamWaitEvent(st, snap, 0);
     SolventF none;
     launch_stream_cells<false>(p, s, none, c, f, buf, st);
   }
@@ -1024,14 +1025,17 @@ int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_su
 }
 
 int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
-                     cudaStream_t st, bool sum_pending) {
+                     cudaStream_t st, bool sum_pending, cudaEvent_t readers) {
   set_sum_attrs();
   const size_t sm = (sum_pending && p.nt <= kSumSmemT) ? 2 * (size_t)p.nt * sizeof(double) : 0;
   k_sum_edges<<<1 + nb(2 * p.ne + p.nv, 1024), 1024, sm, st>>>(p, m, f.slot, sum_pending ? 1 : 0, f.vd, f.vw, f.vX);
   k_force_tri<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.slot);
   k_force_gather_w<<<nb(p.nv, kGW), 32 * kGW, 0, st>>>(p, m, f.slot, f.gstart, f.gidx);
   k_tail_b<<<1, kTailT, 0, st>>>(p, m, f.vd, f.vw, f.vX, epoch);
-  if (next_kick) fast_kick_prep(p, m, f, next_buf, st);
+  if (next_kick) {
+    if (readers) cudaStreamWaitEvent(st, readers, 0);
+    fast_kick_prep(p, m, f, next_buf, st);
+  }
   return 4 + (next_kick ? 2 : 0);
 }
 

@@ -48,13 +48,17 @@ inline int heavy_cap(int lmax) {
   int c = ((lmax + 63) / 64) * 64;
   return c < 64 ? 64 : (c > kHeavyList ? kHeavyList : c);
 }
-// ev0/ev1 (optional) are recorded around the bulk kernel k_stream_fast
+// ev0/ev1 (optional) are recorded around the bulk kernel k_stream_fast.  The
+// bulk kernel reads no membrane data; the near-membrane kernel reads the
+// snapshot `buf` and first waits for `snap` (optional: its producer)
 void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
-                 cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr);
+                 cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr, cudaEvent_t snap = nullptr);
 // these return the number of kernels they launched
 int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_sum);
 bool is_membrane_kernel(const void* fn);
+// next_kick: also the next step's half-kick and snapshot into next_buf,
+// after waiting for `readers` (optional: the last streaming that read it)
 int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
-                     cudaStream_t st, bool sum_pending);
+                     cudaStream_t st, bool sum_pending, cudaEvent_t readers = nullptr);
 
 }  // namespace irbc

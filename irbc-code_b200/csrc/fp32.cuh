@@ -50,10 +50,11 @@ __device__ __forceinline__ int shifted_cell_f(const DevParams& p, float4 q, cons
 __global__ void k_count_f(DevParams p, SolventF f, int* cnt, int* slot, uint64_t eoff) {
   const uint64_t epoch = epoch_of(p, eoff);
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t o[4];
-  draw_block(p.seed, STREAM_COLLIDE_U, epoch, 0, o);
-  const double r[3] = {p.a * ((double)o[0] * (1.0 / 4294967296.0)), p.a * ((double)o[1] * (1.0 / 4294967296.0)),
-                       p.a * ((double)o[2] * (1.0 / 4294967296.0))};
+  // the grid shift, drawn once per block
+  __shared__ double sr[3];
+  if (threadIdx.x == 0) grid_shift(p, epoch, sr);
+  __syncthreads();
+  const double r[3] = {sr[0], sr[1], sr[2]};
   unsigned act = __ballot_sync(0xffffffffu, i < f.n);
   if (i >= f.n) return;
   int c = shifted_cell_f(p, f.pos[i], r);
@@ -155,13 +156,14 @@ __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const
 }
 
 void fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb, int buf, cudaStream_t st,
-                   cudaEvent_t ev0, cudaEvent_t ev1) {
+                   cudaEvent_t ev0, cudaEvent_t ev1, cudaEvent_t snap) {
   cudaMemsetAsync(fb.qn, 0, sizeof(int), st);
   if (f.n) {
     if (ev0) cudaEventRecord(ev0, st);
     k_stream_f<<<nbf(f.n, 256), 256, 0, st>>>(p, f, c.lstart, c.lrank, fb.bcnt, fb.bucket, fb.queue, fb.qn,
                                               fb.hcap);
     if (ev1) cudaEventRecord(ev1, st);
+    if (snap) cudaStreamWaitEvent(st, snap, 0);
     Solvent none;
     none.n = f.n;
     launch_stream_cells<true>(p, none, f, c, fb, buf, st);

@@ -291,14 +291,6 @@ void launch_scan3(const int* a, const int* b, const int* c, int* oa, int* ob, in
 // tile of 32 cells for the cell statistics in reference order and the
 // rotation (CollisionDyn, :700-736; cells_tile.cuh).
 
-__device__ __forceinline__ void grid_shift(const DevParams& p, uint64_t epoch, double r[3]) {
-  uint32_t o[4];
-  draw_block(p.seed, STREAM_COLLIDE_U, epoch, 0, o);
-  r[0] = p.a * ((double)o[0] * (1.0 / 4294967296.0));
-  r[1] = p.a * ((double)o[1] * (1.0 / 4294967296.0));
-  r[2] = p.a * ((double)o[2] * (1.0 / 4294967296.0));
-}
-
 __device__ __forceinline__ int shifted_cell(const DevParams& p, double x, double y, double z, const double r[3]) {
   int fx = (int)floor(bbound(x - r[0], p.Lx));
   int fy = (int)floor(bbound(y - r[1], p.Ly));
@@ -350,8 +342,11 @@ __global__ void k_vbin(DevParams p, Membrane m, int* ncm, uint64_t eoff) {
 __global__ void k_count(DevParams p, Solvent s, int* cnt, uint64_t eoff) {
   const uint64_t epoch = epoch_of(p, eoff);
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  double r[3];
-  grid_shift(p, epoch, r);
+  // the grid shift, drawn once per block
+  __shared__ double sr[3];
+  if (threadIdx.x == 0) grid_shift(p, epoch, sr);
+  __syncthreads();
+  const double r[3] = {sr[0], sr[1], sr[2]};
   int c = -1;
   if (i < s.n) c = shifted_cell(p, s.x[i], s.y[i], s.z[i], r);
   unsigned act = __ballot_sync(0xffffffffu, i < s.n);
