@@ -139,6 +139,18 @@ int irbc_step(irbc_handle* h, int64_t n);
  * default) launches every kernel on the two streams.  The results are the
  * same either way. */
 int irbc_set_graphs(irbc_handle* h, int32_t on);
+/* Not in the reference.  n = 2 (the default): the membrane kernels run on a
+ * second, high-priority stream beside the solvent kernels; n = 1: every
+ * kernel of the handle runs on its one stream.  One stream suits many small
+ * simulations sharing a GPU (fewer streams contend for the device's
+ * hardware queues); the results are the same either way. */
+int irbc_set_streams(irbc_handle* h, int32_t n);
+/* Not in the reference.  How irbc_step launches the membrane step: mode 1
+ * (the default) as wide kernels over many SMs; mode 2 as one block per
+ * launch, two kernels per step instead of eight, for meshes up to 1024
+ * vertices (IRBC_ERR_CAPACITY for a larger mesh; a mesh set later keeps
+ * the wide kernels).  The results are the same either way. */
+int irbc_set_membrane_kernels(irbc_handle* h, int32_t mode);
 int irbc_step_part1(irbc_handle* h);
 int irbc_step_part2(irbc_handle* h);
 

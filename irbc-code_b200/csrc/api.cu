@@ -29,7 +29,9 @@ struct irbc_handle {
   Cells c;
   Membrane m;
   cudaStream_t st = nullptr;   // solvent kernels; every public call orders on it
-  cudaStream_t st2 = nullptr;  // membrane kernels, run beside the solvent ones
+  cudaStream_t st2 = nullptr;  // membrane kernels, run beside the solvent ones (== st with one stream)
+  cudaStream_t st2_own = nullptr;  // the side stream this handle created
+  int mem_mode = 1;                // membrane step: 1 wide kernels, 2 one block
   FastBufs fb;
   bool fp32 = false;           // solvent held in sf (float4) between exchanges
   SolventF sf;
@@ -372,6 +374,7 @@ int upload_mesh(irbc_handle* h, const HostMesh& M) {
   h->dp.cth0 = cos(M.theta0 * h->P.Pi / 180.0);
   h->dp.sth0 = sin(M.theta0 * h->P.Pi / 180.0);
   h->have_mesh = true;
+  h->fb.one_block = h->mem_mode == 2 && one_block_fits(h->dp);
   return 0;
 }
 
@@ -520,6 +523,7 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
       delete h;
       return IRBC_ERR_CUDA;
     }
+    h->st2_own = h->st2;
     for (cudaEvent_t* e : {&h->ev_snap, &h->ev_mem, &h->ev_coll, &h->ev_str[0], &h->ev_str[1], &h->ev_vbin})
       cudaEventCreateWithFlags(e, cudaEventDisableTiming);
   }
@@ -582,15 +586,15 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   if (!h) return;
   cudaSetDevice(h->P.device);
   if (h->st) cudaStreamSynchronize(h->st);
-  if (h->st2) cudaStreamSynchronize(h->st2);
+  if (h->st2_own) cudaStreamSynchronize(h->st2_own);
   invalidate_graphs(h);
   free_fast(h->fb);
-  dfree(h->fb.queue); dfree(h->fb.qn); dfree(h->fb.bcnt); dfree(h->fb.bucket);
+  dfree(h->fb.queue); dfree(h->fb.qn); dfree(h->fb.bcnt); dfree(h->fb.bucket); dfree(h->fb.border);
   for (float4** q : {&h->sf.pos, &h->sf.vel, &h->sf.pos2, &h->sf.vel2}) dfree(*q);
   dfree(h->sf.pid); dfree(h->sf.pid2);
   for (cudaEvent_t e : {h->ev_snap, h->ev_mem, h->ev_coll, h->ev_str[0], h->ev_str[1], h->ev_vbin})
     if (e) cudaEventDestroy(e);
-  if (h->st2) cudaStreamDestroy(h->st2);
+  if (h->st2_own) cudaStreamDestroy(h->st2_own);
   Solvent& s = h->s;
   Cells& c = h->c;
   for (double** q : {&s.x, &s.y, &s.z, &s.x2, &s.y2, &s.z2}) dfree(*q);
@@ -634,10 +638,25 @@ static int refresh_listed(irbc_handle* h) {
     invalidate_graphs(h);  // the buckets move
     dfree(f.bcnt);
     dfree(f.bucket);
+    dfree(f.border);
     f.bcap = c.nact + c.nact / 2 + 64;
     CK(dalloc(&f.bcnt, f.bcap));
     CK(dalloc(&f.bucket, f.bcap * kBucket));
+    CK(dalloc(&f.border, f.bcap));
     CK(cudaMemsetAsync(f.bcnt, 0, sizeof(int) * f.bcap, h->st));
+  }
+  // the near-membrane streaming takes the listed cells longest list first,
+  // so that the heaviest blocks do not start last (order of work only)
+  if (c.nact > 0) {
+    std::vector<int> len(c.nact), order(c.nact);
+    launch_rank_lengths(c, f.border, h->st);
+    g_launches += 1;
+    CK(cudaMemcpyAsync(len.data(), f.border, sizeof(int) * c.nact, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int a = 0; a < c.nact; ++a) order[a] = a;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return len[x] > len[y]; });
+    CK(cudaMemcpyAsync(f.border, order.data(), sizeof(int) * c.nact, cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
   }
   return 0;
 }
@@ -1074,8 +1093,7 @@ extern "C" int irbc_step_part1(irbc_handle* h) {
   const int buf = (int)(s & 1);
   {
     ProfScope ps(h, PROF_MEMBRANE);
-    fast_kick_prep(h->dp, h->m, h->fb, buf, h->st);
-    g_launches += 2;
+    g_launches += fast_kick_prep(h->dp, h->m, h->fb, buf, h->st);
   }
   if (h->upd == h->uplist) {
     int rc = do_llist(h);
@@ -1144,8 +1162,7 @@ static int step_one(irbc_handle* h, int64_t eoff, bool last, bool dry) {
   if (!h->snap_ready && !dry) {
     CK(cudaStreamWaitEvent(ss, h->ev_str[buf], 0));
     ProfScope ps(h, PROF_MEMBRANE, ss);
-    fast_kick_prep(h->dp, h->m, h->fb, buf, ss);
-    g_launches += 2;
+    g_launches += fast_kick_prep(h->dp, h->m, h->fb, buf, ss);
   }
   if (h->upd == h->uplist) {
     // never inside a captured sequence.  Positions of step s are final once
@@ -1177,9 +1194,8 @@ static int step_one(irbc_handle* h, int64_t eoff, bool last, bool dry) {
     CK(cudaEventRecord(h->ev_str[buf], ms));
     {
       ProfScope ps(h, PROF_MEMBRANE, ss);
-      g_launches += fast_drift_va(h->dp, h->m, ss, false);
-      g_launches += fast_forces_tail(h->dp, h->m, h->fb, (uint64_t)eoff, next_kick, buf ^ 1, ss, true,
-                                     h->ev_str[buf ^ 1]);
+      g_launches += fast_membrane_step(h->dp, h->m, h->fb, (uint64_t)eoff, next_kick, buf ^ 1, ss,
+                                       h->ev_str[buf ^ 1]);
     }
     CK(cudaEventRecord(h->ev_mem, ss));
   }
@@ -1328,6 +1344,34 @@ extern "C" int irbc_step(irbc_handle* h, int64_t n) {
   }
   CK(cudaStreamWaitEvent(ms, h->ev_mem, 0));
   CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int irbc_set_streams(irbc_handle* h, int32_t n) {
+  if (!h || (n != 1 && n != 2)) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaStreamSynchronize(h->st2_own));
+  cudaStream_t want = n == 1 ? h->st : h->st2_own;
+  if (want != h->st2) {
+    invalidate_graphs(h);  // captured with the other stream layout
+    h->st2 = want;
+  }
+  return 0;
+}
+
+extern "C" int irbc_set_membrane_kernels(irbc_handle* h, int32_t mode) {
+  if (!h || mode < 1 || mode > 2) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaStreamSynchronize(h->st2_own));
+  h->mem_mode = mode;
+  if (h->have_mesh) {
+    const bool ob = mode == 2;
+    if (ob && !one_block_fits(h->dp)) return fail(h, IRBC_ERR_CAPACITY, "mesh too large for the one-block membrane step");
+    if (ob != h->fb.one_block) invalidate_graphs(h);
+    h->fb.one_block = ob;
+  }
   return 0;
 }
 

@@ -82,6 +82,35 @@ __device__ __forceinline__ void grid_shift(const DevParams& p, uint64_t epoch, d
   r[2] = p.a * ((double)o[2] * (1.0 / 4294967296.0));
 }
 
+// counting-sort slots: particle i0 + u * stride (u < K) of cell c[u] (-1:
+// none) gets a slot in its cell's counter.  Lanes of a warp with the same
+// cell share one atomic (the leader adds the group's size); the K claims
+// of a thread are issued before any result is used.
+constexpr int kCountPer = 4;
+template <int K>
+__device__ __forceinline__ void claim_slots(int* cnt, const int c[K], int64_t i0, int stride, int64_t n,
+                                            int slot[K]) {
+  const int lane = threadIdx.x & 31;
+  unsigned peers[K];
+  int leader[K], rank[K], base[K];
+#pragma unroll
+  for (int u = 0; u < K; ++u) {
+    const bool in = i0 + (int64_t)u * stride < n;
+    const unsigned act = __ballot_sync(0xffffffffu, in);
+    peers[u] = 0u; leader[u] = 0; rank[u] = 0; base[u] = 0;
+    if (in) {
+      peers[u] = __match_any_sync(act, c[u]);
+      leader[u] = __ffs(peers[u]) - 1;
+      rank[u] = __popc(peers[u] & ((1u << lane) - 1));
+      if (lane == leader[u]) base[u] = atomicAdd(&cnt[c[u]], __popc(peers[u]));
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < K; ++u) {
+    if (i0 + (int64_t)u * stride < n) slot[u] = __shfl_sync(peers[u], base[u], leader[u]) + rank[u];
+  }
+}
+
 // periodic wrap by repeated subtraction (bbound, Src/solfuncs.cpp:603-622).
 // The reference's loop never ends for an infinite coordinate and runs for
 // ages for a huge one (reachable only through a degenerate contact time);

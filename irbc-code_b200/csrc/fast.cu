@@ -362,7 +362,8 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
                                                       const int* __restrict__ acell, int* bcnt,
                                                       const int* __restrict__ bucket, Snap sn,
                                                       const TriPre* __restrict__ pre, const int* queue,
-                                                      const int* qn, const int* __restrict__ nactp) {
+                                                      const int* qn, const int* __restrict__ nactp,
+                                                      const int* __restrict__ border) {
   extern __shared__ double sh[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int nact = *nactp;
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
     }
     return;
   }
-  const int a = blockIdx.x;
+  const int a = border[blockIdx.x];
   __shared__ int s_n;
   if (threadIdx.x == 0) {
     s_n = min(bcnt[a], kBucket);
@@ -958,14 +959,30 @@ __global__ void k_snap(DevParams p, Membrane m, Snap sn) {
 // ================================================================ launch ======
 // the membrane chain's kernels (the side stream's work): a captured graph
 // gives them the side stream's high priority
+constexpr int kBlockT = 512;      // threads of the one-block membrane kernels
+constexpr int kBlockMaxV = 1024;  // meshes up to this many vertices use them
+__global__ void __launch_bounds__(kBlockT) k_membrane_block(DevParams p, Membrane m, FastBufs f, uint64_t eoff);
+__global__ void __launch_bounds__(kBlockT) k_kick_prep_block(DevParams p, Membrane m, Snap sn, TriPre* pre);
+
 bool is_membrane_kernel(const void* fn) {
   const void* k[] = {(const void*)k_m_drift, (const void*)k_m_av, (const void*)k_m_sum,
                      (const void*)k_sum_edges, (const void*)k_force_tri, (const void*)k_force_gather_w,
-                     (const void*)k_tail_b, (const void*)k_kick_snap,
+                     (const void*)k_tail_b, (const void*)k_kick_snap, (const void*)k_membrane_block,
+                     (const void*)k_kick_prep_block,
                      (const void*)k_tri_prep, (const void*)k_snap};
   for (const void* q : k)
     if (q == fn) return true;
   return false;
+}
+
+__global__ void k_rank_lengths(Cells c, int nact, int* len) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= nact) return;
+  const int cell = c.acell[a];
+  len[a] = c.lstart[cell + 1] - c.lstart[cell];
+}
+void launch_rank_lengths(const Cells& c, int* len, cudaStream_t st) {
+  if (c.nact > 0) k_rank_lengths<<<nb(c.nact, 256), 256, 0, st>>>(c, c.nact, len);
 }
 
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st) {
@@ -973,9 +990,21 @@ void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaS
   k_tri_prep<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.pre[buf]);
 }
 
-void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st) {
+// half-kick, snapshot and triangle prep of a small mesh in one block
+__global__ void __launch_bounds__(kBlockT) k_kick_prep_block(DevParams p, Membrane m, Snap sn, TriPre* pre) {
+  for (int i = threadIdx.x; i < p.nv; i += blockDim.x) kick_snap_item(p, m, sn, i);
+  __syncthreads();
+  for (int j = threadIdx.x; j < p.nt; j += blockDim.x) tri_prep_one(p, m, j, m.vx, m.vy, m.vz, pre);
+}
+
+int fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st) {
+  if (f.one_block) {
+    k_kick_prep_block<<<1, kBlockT, 0, st>>>(p, m, f.snap[buf], f.pre[buf]);
+    return 1;
+  }
   k_kick_snap<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.snap[buf]);
   k_tri_prep<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.pre[buf]);
+  return 2;
 }
 
 template <bool F32>
@@ -986,7 +1015,7 @@ static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, co
   cudaFuncSetAttribute(k_stream_cells<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, 256, smem, st>>>(
       p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
-      c.totals + 4);
+      c.totals + 4, f.border);
 }
 
 void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
@@ -1024,6 +1053,71 @@ int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_su
   return 3;
 }
 
+// ================================================= membrane step, one block ===
+// The membrane step of a small mesh in one block: the phases of the wide
+// kernels separated by __syncthreads instead of kernel boundaries.  A
+// simulation then launches two kernels for its membrane per step instead
+// of eight, which is what limits many small simulations sharing a GPU.
+// Each phase calls the same per-item functions in the same order as the
+// wide kernels, so results are bit for bit the same.
+__global__ void __launch_bounds__(kBlockT) k_membrane_block(DevParams p, Membrane m, FastBufs f, uint64_t eoff) {
+  extern __shared__ double shb[];
+  const int T = blockDim.x, t = threadIdx.x;
+  for (int i = t; i < p.nv; i += T) m_drift_item(p, m, i);
+  __syncthreads();
+  for (int i = t; i < p.nt; i += T) {
+    m_av_item(p, m, i);
+    shb[i] = m.area[i];
+    shb[p.nt + i] = m.vol[i];
+  }
+  __syncthreads();
+  // warps 0 and 1: Sarea and Volume left to right; the others: edge and
+  // bending terms and the bond preparation
+  if (t == 0) m.sc->Sarea = ordered_sum(shb, p.nt);
+  else if (t == 32) m.sc->Volume = ordered_sum(shb + p.nt, p.nt);
+  else if (t >= 64) {
+    const int n = 2 * p.ne + p.nv;
+    for (int k = t - 64; k < n; k += T - 64) {
+      if (k < p.ne) force_item(p, m, f.slot, k);
+      else if (k < 2 * p.ne) force_item(p, m, f.slot, p.nt + k);
+      else bond_prep_item(p, m, f.vd, f.vw, f.vX, k - 2 * p.ne);
+    }
+  }
+  __syncthreads();
+  for (int k = t; k < p.nt; k += T) force_item(p, m, f.slot, p.ne + k);
+  __syncthreads();
+  {
+    const int lane = t & 31;
+    double* shw = shb + (t >> 5) * (kGSlots * 3 + 3);
+    for (int i = t >> 5; i < p.nv; i += T >> 5) gather_vertex(p, m, f.slot, f.gstart, f.gidx, i, lane, shw);
+  }
+  __syncthreads();
+  tail_b_block(p, m, f.vd, f.vw, f.vX, epoch_of(p, eoff), *reinterpret_cast<TailSmem*>(shb));
+}
+
+static size_t block_smem(const DevParams& p) {
+  size_t b = std::max((size_t)(kBlockT / 32) * (kGSlots * 3 + 3) * sizeof(double), sizeof(TailSmem));
+  return std::max(b, 2 * (size_t)p.nt * sizeof(double));
+}
+
+bool one_block_fits(const DevParams& p) { return p.nv <= kBlockMaxV && 2 * (size_t)p.nt * sizeof(double) <= 96 * 1024; }
+
+int fast_membrane_step(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
+                       cudaStream_t st, cudaEvent_t readers) {
+  if (!f.one_block)
+    return fast_drift_va(p, m, st, false) + fast_forces_tail(p, m, f, epoch, next_kick, next_buf, st, true, readers);
+  const size_t smem = block_smem(p);
+  // per device and cheap: set on every call (from any host thread)
+  cudaFuncSetAttribute(k_membrane_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_membrane_block<<<1, kBlockT, smem, st>>>(p, m, f, epoch);
+  int n = 1;
+  if (next_kick) {
+    if (readers) cudaStreamWaitEvent(st, readers, 0);
+    n += fast_kick_prep(p, m, f, next_buf, st);
+  }
+  return n;
+}
+
 int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
                      cudaStream_t st, bool sum_pending, cudaEvent_t readers) {
   set_sum_attrs();
@@ -1032,11 +1126,12 @@ int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoc
   k_force_tri<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.slot);
   k_force_gather_w<<<nb(p.nv, kGW), 32 * kGW, 0, st>>>(p, m, f.slot, f.gstart, f.gidx);
   k_tail_b<<<1, kTailT, 0, st>>>(p, m, f.vd, f.vw, f.vX, epoch);
+  int n = 4;
   if (next_kick) {
     if (readers) cudaStreamWaitEvent(st, readers, 0);
-    fast_kick_prep(p, m, f, next_buf, st);
+    n += fast_kick_prep(p, m, f, next_buf, st);
   }
-  return 4 + (next_kick ? 2 : 0);
+  return n;
 }
 
 

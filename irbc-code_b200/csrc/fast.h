@@ -30,6 +30,8 @@ struct FastBufs {
   int* bcnt = nullptr;    // particles handed to each listed cell this step (reset by k_stream_cells)
   int* bucket = nullptr;  // kBucket particle slots per listed cell
   int64_t bcap = 0;       // listed cells the buckets have room for
+  int* border = nullptr;  // the listed cell (rank) of each k_stream_cells block: longest lists first
+  bool one_block = false; // the membrane step as one block per launch (small meshes)
   int hcap = kHeavyList;  // list entries k_stream_cells stages (its shared memory); longer lists go
                           // to the overflow queue
   double* slot = nullptr; // force terms: 3 doubles per slot, 4E + 9T + 4E slots
@@ -40,8 +42,11 @@ struct FastBufs {
   double* vX = nullptr;   // its WCA force (3 per vertex)
 };
 
-void fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
+// these return the number of kernels they launched
+int fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
+// list length of each listed cell (rank a < nact) into len[a]
+void launch_rank_lengths(const Cells& c, int* len, cudaStream_t st);
 // the staging capacity for lists of at most lmax entries: lmax rounded up
 // to 64, at least 64, at most kHeavyList
 inline int heavy_cap(int lmax) {
@@ -60,5 +65,12 @@ bool is_membrane_kernel(const void* fn);
 // after waiting for `readers` (optional: the last streaming that read it)
 int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
                      cudaStream_t st, bool sum_pending, cudaEvent_t readers = nullptr);
+// the whole membrane step of irbc_step (drift .. bond_dynamics, then the
+// next half-kick and snapshot as fast_forces_tail): in one block per launch
+// when f.one_block, else fast_drift_va + fast_forces_tail
+int fast_membrane_step(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
+                       cudaStream_t st, cudaEvent_t readers = nullptr);
+// whether a mesh suits the one-block membrane step
+bool one_block_fits(const DevParams& p);
 
 }  // namespace irbc

@@ -47,26 +47,30 @@ __device__ __forceinline__ int shifted_cell_f(const DevParams& p, float4 q, cons
   return cell_of(p, fx, fy, fz);
 }
 
-__global__ void k_count_f(DevParams p, SolventF f, int* cnt, int* slot, uint64_t eoff) {
+__global__ void __launch_bounds__(256) k_count_f(DevParams p, SolventF f, int* cnt, int* slot, uint64_t eoff) {
   const uint64_t epoch = epoch_of(p, eoff);
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   // the grid shift, drawn once per block
   __shared__ double sr[3];
   if (threadIdx.x == 0) grid_shift(p, epoch, sr);
   __syncthreads();
   const double r[3] = {sr[0], sr[1], sr[2]};
-  unsigned act = __ballot_sync(0xffffffffu, i < f.n);
-  if (i >= f.n) return;
-  int c = shifted_cell_f(p, f.pos[i], r);
-  unsigned peers = __match_any_sync(act, c);
-  int leader = __ffs(peers) - 1;
-  int lane = threadIdx.x & 31;
-  int rank = __popc(peers & ((1u << lane) - 1));
-  int base = 0;
-  if (lane == leader) base = atomicAdd(&cnt[c], __popc(peers));
-  base = __shfl_sync(peers, base, leader);
-  f.pid[i] = c;  // the cell of this collision
-  slot[i] = base + rank;
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x * kCountPer + threadIdx.x;
+  int c[kCountPer];
+#pragma unroll
+  for (int u = 0; u < kCountPer; ++u) {
+    const int64_t i = i0 + (int64_t)u * blockDim.x;
+    c[u] = i < f.n ? shifted_cell_f(p, f.pos[i], r) : -1;
+  }
+  int sl[kCountPer];
+  claim_slots<kCountPer>(cnt, c, i0, blockDim.x, f.n, sl);
+#pragma unroll
+  for (int u = 0; u < kCountPer; ++u) {
+    const int64_t i = i0 + (int64_t)u * blockDim.x;
+    if (i < f.n) {
+      f.pid[i] = c[u];  // the cell of this collision
+      slot[i] = sl[u];
+    }
+  }
 }
 
 __global__ void k_perm_f(const int* __restrict__ key, const int* __restrict__ slot, const int* __restrict__ start,
@@ -96,7 +100,7 @@ __global__ void k_copy_back_f(SolventF f) {
 void launch_collide_count_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, uint64_t epoch,
                             cudaStream_t st) {
   cudaMemsetAsync(c.cnt, 0, sizeof(int) * c.n, st);
-  if (f.n) k_count_f<<<nbf(f.n, 256), 256, 0, st>>>(p, f, c.cnt, s.slot, epoch);
+  if (f.n) k_count_f<<<nbf(f.n, 256 * kCountPer), 256, 0, st>>>(p, f, c.cnt, s.slot, epoch);
 }
 
 // per-cell statistics (sums in double, reference particle order) and the

@@ -339,27 +339,32 @@ __global__ void k_vbin(DevParams p, Membrane m, int* ncm, uint64_t eoff) {
 }
 
 // cell of each particle in the shifted grid; warp-aggregated slot counters
-__global__ void k_count(DevParams p, Solvent s, int* cnt, uint64_t eoff) {
+__global__ void __launch_bounds__(256) k_count(DevParams p, Solvent s, int* cnt, uint64_t eoff) {
   const uint64_t epoch = epoch_of(p, eoff);
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   // the grid shift, drawn once per block
   __shared__ double sr[3];
   if (threadIdx.x == 0) grid_shift(p, epoch, sr);
   __syncthreads();
   const double r[3] = {sr[0], sr[1], sr[2]};
-  int c = -1;
-  if (i < s.n) c = shifted_cell(p, s.x[i], s.y[i], s.z[i], r);
-  unsigned act = __ballot_sync(0xffffffffu, i < s.n);
-  if (i < s.n) {
-    unsigned peers = __match_any_sync(act, c);
-    int leader = __ffs(peers) - 1;
-    int lane = threadIdx.x & 31;
-    int rank = __popc(peers & ((1u << lane) - 1));
-    int base = 0;
-    if (lane == leader) base = atomicAdd(&cnt[c], __popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    s.pid[i] = c;  // the cell of this collision (particle.pid)
-    s.slot[i] = base + rank;
+  // kCountPer particles per thread, a block's particles contiguous: every
+  // thread's loads first, then the slot claims, so that the memory
+  // latencies overlap
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x * kCountPer + threadIdx.x;
+  int c[kCountPer];
+#pragma unroll
+  for (int u = 0; u < kCountPer; ++u) {
+    const int64_t i = i0 + (int64_t)u * blockDim.x;
+    c[u] = i < s.n ? shifted_cell(p, s.x[i], s.y[i], s.z[i], r) : -1;
+  }
+  int slot[kCountPer];
+  claim_slots<kCountPer>(cnt, c, i0, blockDim.x, s.n, slot);
+#pragma unroll
+  for (int u = 0; u < kCountPer; ++u) {
+    const int64_t i = i0 + (int64_t)u * blockDim.x;
+    if (i < s.n) {
+      s.pid[i] = c[u];  // the cell of this collision (particle.pid)
+      s.slot[i] = slot[u];
+    }
   }
 }
 
@@ -424,7 +429,7 @@ void launch_ghost_flags(const DevParams& p, Cells& c, const Membrane& m, cudaStr
 
 void launch_collide_count(const DevParams& p, Solvent& s, Cells& c, uint64_t epoch, cudaStream_t st) {
   cudaMemsetAsync(c.cnt, 0, sizeof(int) * c.n, st);
-  if (s.n) k_count<<<nblk(s.n, 256), 256, 0, st>>>(p, s, c.cnt, epoch);
+  if (s.n) k_count<<<nblk(s.n, 256 * kCountPer), 256, 0, st>>>(p, s, c.cnt, epoch);
 }
 
 void launch_collide_finish(const DevParams& p, Solvent& s, Cells& c, Membrane& m, uint64_t epoch,

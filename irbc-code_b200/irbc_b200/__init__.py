@@ -116,6 +116,8 @@ def lib():
     L.irbc_launch_count.argtypes = [H]
     L.irbc_profile_begin.argtypes = [H]
     L.irbc_set_graphs.argtypes = [H, C.c_int32]
+    L.irbc_set_streams.argtypes = [H, C.c_int32]
+    L.irbc_set_membrane_kernels.argtypes = [H, C.c_int32]
     L.irbc_profile_end.argtypes = [H, D, C.c_int32]
     L.irbc_host_alloc.restype = C.c_void_p
     L.irbc_host_alloc.argtypes = [C.c_size_t]
@@ -337,6 +339,14 @@ class Simulation:
     def set_graphs(self, on):
         """captured 24-step CUDA graphs in step() (default off)"""
         self._ck(self.L.irbc_set_graphs(self.h, 1 if on else 0), "irbc_set_graphs")
+
+    def set_streams(self, n):
+        """2 (default): membrane kernels on a second stream; 1: one stream"""
+        self._ck(self.L.irbc_set_streams(self.h, int(n)), "irbc_set_streams")
+
+    def set_membrane_kernels(self, mode):
+        """1: wide kernels (default); 2: one block (meshes up to 1024 vertices)"""
+        self._ck(self.L.irbc_set_membrane_kernels(self.h, int(mode)), "irbc_set_membrane_kernels")
 
     def profile_begin(self):
         self._ck(self.L.irbc_profile_begin(self.h), "irbc_profile_begin")

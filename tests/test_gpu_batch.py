@@ -88,3 +88,40 @@ def test_server_results_same_alone_and_in_mix():
     for t, _ in spans:
         assert sum(1 for a, b in spans if a <= t < b) <= 2
     srv.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_one_stream_equals_two(precision):
+    """irbc_set_streams(1) puts the membrane kernels on the solvent's stream:
+    the same state, bit for bit, across collisions and a list update."""
+    import irbc_b200 as G
+    V, E, T = H.troph()
+    _, p = _small(9, precision=precision, onrate=300.0, offrate=50.0)
+    a = G.Simulation(p)
+    a.init(V, E, T, 300)
+    a.set_streams(1)
+    a.step(50)
+    a.set_streams(2)
+    a.step(47)
+    ref = _run_alone(p, V, E, T, 300, 97)
+    assert H.compare(a.get_state(), ref, 0.0) == {}
+    a.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_one_block_membrane_equals_wide_kernels(precision):
+    """The one-block membrane step (the default for this 600-vertex mesh)
+    and the wide kernels give the same state, bit for bit, across
+    collisions, bond events and a list update."""
+    import irbc_b200 as G
+    V, E, T = H.troph()
+    _, p = _small(13, precision=precision, onrate=300.0, offrate=50.0)
+    out = []
+    for mode in (1, 2):
+        s = G.Simulation(p)
+        s.init(V, E, T, 300)
+        s.set_membrane_kernels(mode)
+        s.step(97)
+        out.append(s.get_state())
+        s.close()
+    assert H.compare(out[0], out[1], 0.0) == {}
