@@ -194,6 +194,16 @@ int irbc_bin_particles_noalloc(const irbc_params* p, const double* x, const doub
 /* ---- output (formats of maincode.cpp:749-753 and Src/memfuncs.cpp:590-626) ---- */
 int irbc_write_rbcdata(irbc_handle* h, const char* path, int32_t append);
 int irbc_write_stl(irbc_handle* h, const char* path);
+/* Not in the reference: the fields of the RBCdata record (vertex x, y, z,
+ * ix, iy, bondi; maincode.cpp:749-753) copied to a host buffer without
+ * waiting.  The layout is x[nv], y[nv], z[nv] (double) then ix[nv], iy[nv],
+ * bondi[nv] (int32): irbc_record_bytes(h) bytes.  The copy is queued on
+ * the handle's stream after the steps queued so far and the call returns
+ * at once; the buffer holds the record once irbc_sync(h) returns.  `host`
+ * should be page-locked (irbc_host_alloc) for the copy to run
+ * asynchronously. */
+int64_t irbc_record_bytes(const irbc_handle* h);
+int irbc_record_async(irbc_handle* h, void* host, int64_t bytes);
 /* observables not in the reference: out[0..] = mean solvent kT, centre of
  * mass x,y,z (unwrapped), Sarea, Volume, bond count */
 int irbc_observables(irbc_handle* h, double* out, int32_t nout);
@@ -211,6 +221,11 @@ int64_t irbc_launch_count(const irbc_handle* h);
  * membrane launch groups, out[7] = kernel launches in the window, out[8] =
  * ms in the bulk streaming kernel alone (k_stream_fast / k_stream_f),
  * out[9] = its launches; nout <= 10 values are written */
+/* device time (ms) between irbc_timer_begin and irbc_timer_end: two CUDA
+ * events on the handle's stream and no per-phase events in between (what
+ * irbc_step queues is joined back to that stream before it returns) */
+int irbc_timer_begin(irbc_handle* h);
+int irbc_timer_end(irbc_handle* h, double* ms);
 int irbc_profile_begin(irbc_handle* h);
 int irbc_profile_end(irbc_handle* h, double* out, int32_t nout);
 /* ---- batches and the request server (not in the reference) -------------------

@@ -23,6 +23,7 @@ std::atomic<int64_t> g_launches{0};
 }
 
 struct irbc_handle {
+  void* rec = nullptr;     // device staging of irbc_record_async
   irbc_params P{};
   DevParams dp{};
   Solvent s;
@@ -590,6 +591,7 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   invalidate_graphs(h);
   free_fast(h->fb);
   dfree(h->fb.queue); dfree(h->fb.qn); dfree(h->fb.bcnt); dfree(h->fb.bucket); dfree(h->fb.border);
+  if (h->rec) cudaFree(h->rec);
   for (float4** q : {&h->sf.pos, &h->sf.vel, &h->sf.pos2, &h->sf.vel2}) dfree(*q);
   dfree(h->sf.pid); dfree(h->sf.pid2);
   for (cudaEvent_t e : {h->ev_snap, h->ev_mem, h->ev_coll, h->ev_str[0], h->ev_str[1], h->ev_vbin})
@@ -1400,6 +1402,35 @@ int pull_vertices(irbc_handle* h, VertexCopy& V) {
 }  // namespace
 
 // RBCdata record (maincode.cpp:749-753)
+namespace {
+__global__ void k_pack_record(Membrane m, int nv, double* d, int32_t* q) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  d[i] = m.x[i]; d[nv + i] = m.y[i]; d[2 * nv + i] = m.z[i];
+  q[i] = m.ix[i]; q[nv + i] = m.iy[i]; q[2 * nv + i] = m.bondi[i];
+}
+}  // namespace
+
+extern "C" int64_t irbc_record_bytes(const irbc_handle* h) {
+  return h ? (int64_t)h->m.nv * (3 * (int64_t)sizeof(double) + 3 * (int64_t)sizeof(int32_t)) : -1;
+}
+
+extern "C" int irbc_record_async(irbc_handle* h, void* host, int64_t bytes) {
+  if (!h || !host) return IRBC_ERR_ARG;
+  if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
+  const int64_t need = irbc_record_bytes(h);
+  if (bytes < need) return fail(h, IRBC_ERR_CAPACITY, "record buffer too small");
+  cudaSetDevice(h->P.device);
+  if (!h->rec) CK(cudaMalloc(&h->rec, (size_t)need));
+  const int nv = h->m.nv;
+  double* d = static_cast<double*>(h->rec);
+  int32_t* q = reinterpret_cast<int32_t*>(d + 3 * (size_t)nv);
+  k_pack_record<<<(nv + 255) / 256, 256, 0, h->st>>>(h->m, nv, d, q);
+  g_launches += 1;
+  CK(cudaMemcpyAsync(host, h->rec, (size_t)need, cudaMemcpyDeviceToHost, h->st));
+  return 0;
+}
+
 extern "C" int irbc_write_rbcdata(irbc_handle* h, const char* path, int32_t append) {
   if (!h || !path || !h->have_mesh) return IRBC_ERR_ARG;
   VertexCopy V;
@@ -1504,6 +1535,26 @@ extern "C" int irbc_bin_particles(const irbc_params* p, const double* x, const d
 }
 
 // ---- profiling window and host buffers ------------------------------------------------
+// device time of a stretch of calls with two events on the handle's
+// stream and nothing in between (no per-phase events)
+extern "C" int irbc_timer_begin(irbc_handle* h) {
+  if (!h) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
+  if (!h->ev_begin) { CK(cudaEventCreate(&h->ev_begin)); CK(cudaEventCreate(&h->ev_end)); }
+  CK(cudaEventRecord(h->ev_begin, h->st));
+  return 0;
+}
+extern "C" int irbc_timer_end(irbc_handle* h, double* ms) {
+  if (!h || !ms || !h->ev_begin) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
+  CK(cudaEventRecord(h->ev_end, h->st));
+  CK(cudaEventSynchronize(h->ev_end));
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, h->ev_begin, h->ev_end));
+  *ms = t;
+  return 0;
+}
+
 extern "C" int irbc_profile_begin(irbc_handle* h) {
   if (!h) return IRBC_ERR_ARG;
   cudaSetDevice(h->P.device);

@@ -6,6 +6,7 @@
 //
 // Results equal the one-kernel-per-phase path (kernels.cu) bit for bit.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include "fast.h"
 #include "fp32.h"
@@ -985,6 +986,14 @@ void launch_rank_lengths(const Cells& c, int* len, cudaStream_t st) {
   if (c.nact > 0) k_rank_lengths<<<nb(c.nact, 256), 256, 0, st>>>(c, c.nact, len);
 }
 
+bool first_on_device(int key) {
+  static std::atomic<uint64_t> done[8] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || key < 0 || key >= 8) return true;
+  const uint64_t bit = 1ull << dev;
+  return (done[key].fetch_or(bit) & bit) == 0;
+}
+
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st) {
   k_snap<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.snap[buf]);
   k_tri_prep<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.pre[buf]);
@@ -1011,8 +1020,10 @@ template <bool F32>
 static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
                                 cudaStream_t st) {
   const int smem = f.hcap * (int)(sizeof(TriPre) + sizeof(int));
-  // per device and cheap: set on every call (from any host thread)
-  cudaFuncSetAttribute(k_stream_cells<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  // the limit for the largest staging, once per device
+  if (first_on_device(F32 ? 1 : 0))
+    cudaFuncSetAttribute(k_stream_cells<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kHeavyList * (int)(sizeof(TriPre) + sizeof(int)));
   k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, 256, smem, st>>>(
       p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
       c.totals + 4, f.border);
@@ -1107,8 +1118,9 @@ int fast_membrane_step(const DevParams& p, Membrane& m, FastBufs& f, uint64_t ep
   if (!f.one_block)
     return fast_drift_va(p, m, st, false) + fast_forces_tail(p, m, f, epoch, next_kick, next_buf, st, true, readers);
   const size_t smem = block_smem(p);
-  // per device and cheap: set on every call (from any host thread)
-  cudaFuncSetAttribute(k_membrane_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the limit for the largest mesh this kernel takes, once per device
+  if (first_on_device(2))
+    cudaFuncSetAttribute(k_membrane_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   k_membrane_block<<<1, kBlockT, smem, st>>>(p, m, f, epoch);
   int n = 1;
   if (next_kick) {

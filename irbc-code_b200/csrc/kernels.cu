@@ -417,8 +417,8 @@ __global__ void k_copy_back(Solvent s) {
 void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cudaStream_t st) {
   int n2 = 1;
   while (n2 < p.nv) n2 <<= 1;
-  // per device and cheap: set on every call (from any host thread)
-  cudaFuncSetAttribute(k_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
+  if (first_on_device(3))
+    cudaFuncSetAttribute(k_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
   cudaMemsetAsync(c.ncm, 0, sizeof(int) * c.n, st);
   k_vbin<<<1, 1024, sizeof(uint64_t) * n2, st>>>(p, m, c.ncm, epoch);
 }

@@ -117,6 +117,11 @@ def lib():
     L.irbc_profile_begin.argtypes = [H]
     L.irbc_set_graphs.argtypes = [H, C.c_int32]
     L.irbc_set_streams.argtypes = [H, C.c_int32]
+    L.irbc_timer_begin.argtypes = [H]
+    L.irbc_timer_end.argtypes = [H, D]
+    L.irbc_record_bytes.restype = C.c_int64
+    L.irbc_record_bytes.argtypes = [H]
+    L.irbc_record_async.argtypes = [H, C.c_void_p, C.c_int64]
     L.irbc_set_membrane_kernels.argtypes = [H, C.c_int32]
     L.irbc_profile_end.argtypes = [H, D, C.c_int32]
     L.irbc_host_alloc.restype = C.c_void_p
@@ -339,6 +344,23 @@ class Simulation:
     def set_graphs(self, on):
         """captured 24-step CUDA graphs in step() (default off)"""
         self._ck(self.L.irbc_set_graphs(self.h, 1 if on else 0), "irbc_set_graphs")
+
+    def record_async(self, pinned):
+        """queue the RBCdata record (x, y, z, ix, iy, bondi of every vertex)
+        into a PinnedArray of irbc_record_bytes bytes; valid after sync()"""
+        self._ck(self.L.irbc_record_async(self.h, C.c_void_p(pinned.ptr), pinned.array.nbytes), "irbc_record_async")
+
+    def record_bytes(self):
+        return int(self.L.irbc_record_bytes(self.h))
+
+    def timer_begin(self):
+        self._ck(self.L.irbc_timer_begin(self.h), "irbc_timer_begin")
+
+    def timer_end(self):
+        """device ms since timer_begin (two events on the handle's stream)"""
+        out = np.zeros(1)
+        self._ck(self.L.irbc_timer_end(self.h, _p(out, D)), "irbc_timer_end")
+        return float(out[0])
 
     def set_streams(self, n):
         """2 (default): membrane kernels on a second stream; 1: one stream"""

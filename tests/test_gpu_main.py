@@ -44,3 +44,26 @@ def test_main_writes_the_reference_files(tmp_path):
     sim.write_rbcdata(str(ref), False)
     assert ref.read_text().splitlines() == text[:601]
     sim.close()
+
+
+def test_record_async_matches_state():
+    """irbc_record_async packs x, y, z, ix, iy, bondi of every vertex into a
+    page-locked buffer; after sync it equals the state's vertex fields."""
+    import numpy as np
+    import irbc_b200 as G
+    op, orc = H.make_oracle(ns=20000, seed=5, onrate=300.0, offrate=50.0)
+    sim = H.gpu_like(op, orc, 5)
+    sim.step(7)
+    buf = G.PinnedArray(sim.record_bytes(), np.uint8)
+    sim.record_async(buf)
+    sim.sync()
+    st = sim.get_state()
+    nv = sim.nv
+    a = buf.array
+    d = a[:24 * nv].view(np.float64)
+    q = a[24 * nv:].view(np.int32)
+    for k, name in enumerate(("x", "y", "z")):
+        assert np.array_equal(d[k * nv:(k + 1) * nv], st.a[name]), name
+    for k, name in enumerate(("ix", "iy", "bondi")):
+        assert np.array_equal(q[k * nv:(k + 1) * nv], st.a[name]), name
+    sim.close()
