@@ -77,6 +77,7 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.start = 0
 
     def __enter__(self):
         try:
@@ -85,6 +86,13 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
+            # nvidia-smi's start-up (NVML initialisation) stalls the
+            # driver: wait for its first sample before the timed region
+            # begins, and keep only the samples taken inside it
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.start = len(self.lines)
         except Exception:
             self.proc = None
         return self
@@ -105,7 +113,8 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
+        inside = self.lines[self.start:] or self.lines
+        for l in inside:
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
                 continue
