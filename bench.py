@@ -246,7 +246,9 @@ def run_ours(args):
     launches0 = int(sim.L.irbc_launch_count(sim.h))
     with ClockSampler(local) as clocks:
         sim.timer_begin()
+        h0 = time.perf_counter()
         sim.step(args.steps)
+        host_enqueue_s = time.perf_counter() - h0
         t_local = sim.timer_end()
     launches = int(sim.L.irbc_launch_count(sim.h)) - launches0
     t_ms = reduce_max(t_local, world)
@@ -296,6 +298,7 @@ def run_ours(args):
                               "membrane": kprof["membrane_ms"] / 48,
                               "window": "48 steps after the timed steps"},
         "gpu_launches": launches,
+        "host_enqueue_ms_per_step": 1e3 * host_enqueue_s / args.steps,
         "clocks": clocks.summary(),
         "state_finite": finite,
     }

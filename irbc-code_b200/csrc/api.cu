@@ -1292,7 +1292,9 @@ static irbc_handle::StepGraph* graph_for(irbc_handle* h) {
     cudaGetLastError();
   }
   cudaGraphExec_t exec = nullptr;
-  if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  // the kernel nodes' priorities apply only when the graph is instantiated
+  // to use them
+  if (ok) ok = cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority) == cudaSuccess;
   if (graph) cudaGraphDestroy(graph);
   cudaGetLastError();  // a refused capture leaves no sticky error
   if (!ok) {
