@@ -611,20 +611,32 @@ __device__ __forceinline__ double ordered_sum(const double* a, int n) {
   if ((reinterpret_cast<uintptr_t>(a) & 15) == 0) {
     const double2* a2 = reinterpret_cast<const double2*>(a);
     const int n16 = n & ~15;
-#pragma unroll 2
+    // the next 16 terms are loaded while the current 16 are added (32
+    // registers of terms: the kernels calling this run <= 256 threads)
+    double2 cur[8], nxt[8];
+    if (n16 > 0) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) cur[k] = a2[k];
+    }
     for (; i < n16; i += 16) {
-      double2 r[8];
+      const bool more = i + 16 < n16;
+      if (more) {
 #pragma unroll
-      for (int k = 0; k < 8; ++k) r[k] = a2[(i >> 1) + k];
+        for (int k = 0; k < 8; ++k) nxt[k] = a2[((i + 16) >> 1) + k];
+      }
 #pragma unroll
-      for (int k = 0; k < 8; ++k) { t += r[k].x; t += r[k].y; }
+      for (int k = 0; k < 8; ++k) { t += cur[k].x; t += cur[k].y; }
+      if (more) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) cur[k] = nxt[k];
+      }
     }
   }
   for (; i < n; ++i) t += a[i];
   return t;
 }
 
-__global__ void __launch_bounds__(1024) k_m_sum(DevParams p, Membrane m) {
+__global__ void __launch_bounds__(256) k_m_sum(DevParams p, Membrane m) {
   extern __shared__ double sh[];
   const bool staged = p.nt <= kSumSmemT;
   if (staged) {
@@ -702,7 +714,7 @@ __device__ __forceinline__ void bond_prep_item(const DevParams& p, Membrane& m, 
 // and bending terms and the bond preparation, which do not depend on
 // Sarea / Volume, so they overlap the sums.  The triangle terms follow in
 // k_force_tri.
-__global__ void __launch_bounds__(1024) k_sum_edges(DevParams p, Membrane m, double* __restrict__ slot, int do_sum,
+__global__ void __launch_bounds__(256) k_sum_edges(DevParams p, Membrane m, double* __restrict__ slot, int do_sum,
                                                     int* __restrict__ vd, int* __restrict__ vw,
                                                     double* __restrict__ vX) {
   if (blockIdx.x == 0) {
@@ -1060,7 +1072,7 @@ int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_su
   k_m_av<<<nb(p.nt, 128), 128, 0, st>>>(p, m);
   if (!with_sum) return 2;
   const size_t sm = p.nt <= kSumSmemT ? 2 * (size_t)p.nt * sizeof(double) : 0;
-  k_m_sum<<<1, 1024, sm, st>>>(p, m);
+  k_m_sum<<<1, 256, sm, st>>>(p, m);
   return 3;
 }
 
@@ -1134,7 +1146,7 @@ int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoc
                      cudaStream_t st, bool sum_pending, cudaEvent_t readers) {
   set_sum_attrs();
   const size_t sm = (sum_pending && p.nt <= kSumSmemT) ? 2 * (size_t)p.nt * sizeof(double) : 0;
-  k_sum_edges<<<1 + nb(2 * p.ne + p.nv, 1024), 1024, sm, st>>>(p, m, f.slot, sum_pending ? 1 : 0, f.vd, f.vw, f.vX);
+  k_sum_edges<<<1 + nb(2 * p.ne + p.nv, 256), 256, sm, st>>>(p, m, f.slot, sum_pending ? 1 : 0, f.vd, f.vw, f.vX);
   k_force_tri<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.slot);
   k_force_gather_w<<<nb(p.nv, kGW), 32 * kGW, 0, st>>>(p, m, f.slot, f.gstart, f.gidx);
   k_tail_b<<<1, kTailT, 0, st>>>(p, m, f.vd, f.vw, f.vX, epoch);
