@@ -40,6 +40,9 @@ import os
 # many replicas' streams need more than the default 8 hardware queues;
 # read by CUDA when the process first uses it
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+# every kernel loaded when the context is created, so that no first use
+# (a list update, a re-sort) loads one inside the timed steps
+os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
 import subprocess
 import sys
 import tempfile
