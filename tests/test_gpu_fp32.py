@@ -125,3 +125,4 @@ def test_precision_study_within_one_percent():
     assert err["shear_rel"] < max(0.01, 3.0 * err["noise_shear_rel"])
     assert err["profile_l2_rel"] < max(0.01, 3.0 * err["noise_profile_l2_rel"])
     assert err["com_velocity_abs"] < max(0.01, 3.0 * err["noise_com_velocity_abs"])
+
