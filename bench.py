@@ -264,19 +264,23 @@ def run_ours(args):
     sim.sync()
     # the end-to-end leg below replays the same steps from this state
     start = sim.get_state() if args.e2e else None
-    barrier(world)
-    # the timed steps: two CUDA events on the simulation's stream (the
-    # per-phase profile is taken in a separate window below)
     # keep the GPU busy for a second before the timed steps (memory and SM
     # clocks leave their idle states), without advancing the simulation
     gpu_warm(local, 1.0)
     launches0 = int(sim.L.irbc_launch_count(sim.h))
+    # the timed steps: two CUDA events on the simulation's stream, bracketed
+    # by a synchronize and a barrier over the ranks on both sides (the
+    # per-phase profile is taken in a separate window below)
     with ClockSampler(local) as clocks:
+        sim.sync()
+        barrier(world)
         sim.timer_begin()
         h0 = time.perf_counter()
         sim.step(args.steps)
         host_enqueue_s = time.perf_counter() - h0
         t_local = sim.timer_end()
+        sim.sync()
+        barrier(world)
     launches = int(sim.L.irbc_launch_count(sim.h)) - launches0
     t_ms = reduce_max(t_local, world)
     ns = WORKLOAD["Ns"]
