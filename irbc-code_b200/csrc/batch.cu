@@ -52,7 +52,6 @@ class StepPool {
     steps_ = nullptr;
     return first_error_;
   }
-  int threads() const { return n_; }
 
  private:
   void run(int t) {

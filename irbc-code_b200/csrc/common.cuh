@@ -33,7 +33,9 @@ enum : uint32_t { STREAM_INIT = 1, STREAM_COLLIDE_U = 2, STREAM_COLLIDE_N = 3, S
 // multiply/xor round with the Weyl key schedule.
 __host__ __device__ inline void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
                                               uint32_t k0, uint32_t k1, uint32_t out[4]) {
+#ifdef __CUDA_ARCH__
 #pragma unroll
+#endif
   for (int r = 0; r < 10; ++r) {
     uint64_t p0 = (uint64_t)0xD2511F53u * c0;
     uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
