@@ -242,6 +242,48 @@ int irbc_batch_add(irbc_batch* b, irbc_handle* h);
 int irbc_batch_remove(irbc_batch* b, irbc_handle* h);
 int32_t irbc_batch_size(const irbc_batch* b);
 int irbc_batch_step(irbc_batch* b, int64_t n);
+/* ---- launch schedules and their autotuner (not in the reference) --------------
+ * How a batch launches its members' steps.  No field changes what a member
+ * computes; each is checked bit for bit against its default:
+ *   streams   irbc_set_streams for every member (1 or 2; default 2)
+ *   membrane  irbc_set_membrane_kernels for every member (1 wide kernels,
+ *             2 one block; default 1)
+ *   graphs    irbc_set_graphs for every member (0 or 1; default 0)
+ *   chunk     steps a pool thread issues to one member before it turns to
+ *             its next member (a multiple of 24 in 24..2400; default 24) */
+typedef struct irbc_schedule {
+  int32_t streams, membrane, graphs, chunk;
+} irbc_schedule;
+/* Applies s to every member now and to every member added later.  On an
+ * error (IRBC_ERR_CAPACITY: a member's mesh is too large for membrane = 2)
+ * every member goes back to the batch's previous schedule (the defaults if
+ * none was set) and the error is returned. */
+int irbc_batch_set_schedule(irbc_batch* b, const irbc_schedule* s);
+int irbc_batch_get_schedule(const irbc_batch* b, irbc_schedule* s);
+/* Picks the fastest of n candidates.  measure(i, ctx, &seconds) runs
+ * candidate i once and returns 0 with its time, IRBC_ERR_CAPACITY when the
+ * candidate cannot run (it is skipped), or another error, which ends the
+ * search and is returned.  Candidates run one after another: each once
+ * untimed, then `repeats` (1..64) timed runs, scored by their median.
+ * Candidate 0 is the incumbent: a later candidate displaces the best so far
+ * only when its median is below (1 - margin) times the best's (margin in
+ * [0, 1)).  medians (n entries, or null) receives each score, -1 for a
+ * skipped candidate.  IRBC_ERR_CAPACITY when every candidate was skipped. */
+typedef int (*irbc_tune_measure)(int32_t candidate, void* ctx, double* seconds);
+int irbc_tune_select(int32_t n, irbc_tune_measure measure, void* ctx, int32_t repeats, double margin,
+                     double* medians, int32_t* best);
+/* Tunes the batch's schedule on its own members, one field at a time in
+ * the order membrane, streams, graphs, chunk (24, 96, 240): the current
+ * value against the others, each candidate scored by irbc_tune_select as
+ * the host time of trial_steps batch steps with their device work waited
+ * for.  Ends with the winner applied (to members added later too) and
+ * written to *best.  The trial steps are ordinary steps of the members, and
+ * no field changes results, so they simply advance the simulations:
+ * *steps_taken receives how far every member advanced.  The tuner sets the
+ * members' stream, membrane and graph options itself, replacing settings
+ * made on the handles before. */
+int irbc_batch_autotune(irbc_batch* b, int64_t trial_steps, int32_t repeats, double margin, irbc_schedule* best,
+                        int64_t* steps_taken);
 /* The server takes whole simulations as requests: parameters, mesh, knob
  * count and step count.  Its loop admits a pending request when its
  * footprint (irbc_footprint_bytes) fits in the device-memory budget

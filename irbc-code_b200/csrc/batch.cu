@@ -116,8 +116,24 @@ double now_s(std::chrono::steady_clock::time_point t0) {
 struct irbc_batch {
   std::vector<irbc_handle*> members;
   StepPool pool;
+  irbc_schedule sched{2, 1, 0, 24};  // the handles' defaults and the pool's chunk
+  bool scheduled = false;             // set explicitly: members added later get it too
   explicit irbc_batch(int nthreads) : pool(nthreads) {}
 };
+
+namespace {
+bool valid_schedule(const irbc_schedule& s) {
+  return (s.streams == 1 || s.streams == 2) && (s.membrane == 1 || s.membrane == 2) &&
+         (s.graphs == 0 || s.graphs == 1) && s.chunk >= 24 && s.chunk <= 2400 && s.chunk % 24 == 0;
+}
+
+int apply_schedule(irbc_handle* h, const irbc_schedule& s) {
+  int rc = irbc_set_streams(h, s.streams);
+  if (!rc) rc = irbc_set_membrane_kernels(h, s.membrane);
+  if (!rc) rc = irbc_set_graphs(h, s.graphs);
+  return rc;
+}
+}  // namespace
 
 extern "C" int irbc_batch_create(int32_t nthreads, irbc_batch** out) {
   if (!out || nthreads < 1 || nthreads > 256) return IRBC_ERR_ARG;
@@ -130,6 +146,10 @@ extern "C" void irbc_batch_destroy(irbc_batch* b) { delete b; }
 extern "C" int irbc_batch_add(irbc_batch* b, irbc_handle* h) {
   if (!b || !h) return IRBC_ERR_ARG;
   if (std::find(b->members.begin(), b->members.end(), h) != b->members.end()) return IRBC_ERR_ARG;
+  if (b->scheduled) {
+    const int rc = apply_schedule(h, b->sched);
+    if (rc) return rc;
+  }
   b->members.push_back(h);
   return 0;
 }
@@ -147,7 +167,128 @@ extern "C" int32_t irbc_batch_size(const irbc_batch* b) { return b ? (int32_t)b-
 extern "C" int irbc_batch_step(irbc_batch* b, int64_t n) {
   if (!b || n < 0) return IRBC_ERR_ARG;
   std::vector<int64_t> steps(b->members.size(), n);
-  return b->pool.step(b->members, steps, 24);
+  return b->pool.step(b->members, steps, b->sched.chunk);
+}
+
+// ---- launch schedules and the autotuner --------------------------------------
+extern "C" int irbc_batch_set_schedule(irbc_batch* b, const irbc_schedule* s) {
+  if (!b || !s || !valid_schedule(*s)) return IRBC_ERR_ARG;
+  for (irbc_handle* h : b->members) {
+    const int rc = apply_schedule(h, *s);
+    if (rc) {
+      for (irbc_handle* g : b->members) apply_schedule(g, b->sched);
+      return rc;
+    }
+  }
+  b->sched = *s;
+  b->scheduled = true;
+  return 0;
+}
+
+extern "C" int irbc_batch_get_schedule(const irbc_batch* b, irbc_schedule* s) {
+  if (!b || !s) return IRBC_ERR_ARG;
+  *s = b->sched;
+  return 0;
+}
+
+extern "C" int irbc_tune_select(int32_t n, irbc_tune_measure measure, void* ctx, int32_t repeats, double margin,
+                                double* medians, int32_t* best) {
+  if (n < 1 || !measure || !best || repeats < 1 || repeats > 64 || !(margin >= 0.0 && margin < 1.0))
+    return IRBC_ERR_ARG;
+  int32_t win = -1;
+  double win_t = 0.0;
+  std::vector<double> t;
+  for (int32_t i = 0; i < n; ++i) {
+    t.clear();
+    int rc = 0;
+    for (int32_t r = 0; r <= repeats && !rc; ++r) {
+      double sec = 0.0;
+      rc = measure(i, ctx, &sec);
+      if (rc) break;
+      if (!(sec >= 0.0 && sec < 1e30)) return IRBC_ERR_ARG;  // not a time
+      if (r > 0) t.push_back(sec);                          // run 0 warms up
+    }
+    if (rc && rc != IRBC_ERR_CAPACITY) return rc;
+    double med = -1.0;
+    if (!rc) {
+      std::sort(t.begin(), t.end());
+      const size_t m = t.size();
+      med = (m % 2) ? t[m / 2] : 0.5 * (t[m / 2 - 1] + t[m / 2]);
+      if (win < 0 || med < (1.0 - margin) * win_t) {
+        win = i;
+        win_t = med;
+      }
+    }
+    if (medians) medians[i] = med;
+  }
+  if (win < 0) return IRBC_ERR_CAPACITY;
+  *best = win;
+  return 0;
+}
+
+namespace {
+struct TuneRun {
+  irbc_batch* b = nullptr;
+  std::vector<irbc_schedule> cands;
+  int64_t trial = 0, taken = 0;
+};
+
+// one timed stretch of trial steps of every member under candidate i; the
+// schedule is applied first (a no-op for the one already in place, so
+// captured graphs survive between the runs of one candidate)
+int measure_schedule(int32_t i, void* ctx, double* seconds) {
+  TuneRun* run = static_cast<TuneRun*>(ctx);
+  irbc_batch* b = run->b;
+  const irbc_schedule& s = run->cands[i];
+  const int rc = irbc_batch_set_schedule(b, &s);
+  if (rc) return rc;
+  std::vector<int64_t> steps(b->members.size(), run->trial);
+  const auto t0 = std::chrono::steady_clock::now();
+  const int e = b->pool.step(b->members, steps, s.chunk);
+  *seconds = now_s(t0);
+  if (!e) run->taken += run->trial;
+  return e;
+}
+}  // namespace
+
+extern "C" int irbc_batch_autotune(irbc_batch* b, int64_t trial_steps, int32_t repeats, double margin,
+                                   irbc_schedule* best, int64_t* steps_taken) {
+  if (!b || trial_steps < 1 || repeats < 1 || repeats > 64 || !(margin >= 0.0 && margin < 1.0))
+    return IRBC_ERR_ARG;
+  if (b->members.empty()) return IRBC_ERR_STATE;
+  TuneRun run;
+  run.b = b;
+  run.trial = trial_steps;
+  irbc_schedule cur = b->sched;
+  static const int32_t kChunks[] = {24, 96, 240};
+  int rc = 0;
+  for (int field = 0; field < 4 && !rc; ++field) {
+    run.cands.assign(1, cur);
+    irbc_schedule alt = cur;
+    if (field == 0) {
+      alt.membrane = 3 - cur.membrane;
+      run.cands.push_back(alt);
+    } else if (field == 1) {
+      alt.streams = 3 - cur.streams;
+      run.cands.push_back(alt);
+    } else if (field == 2) {
+      alt.graphs = 1 - cur.graphs;
+      run.cands.push_back(alt);
+    } else {
+      for (int32_t k : kChunks)
+        if (k != cur.chunk) {
+          alt.chunk = k;
+          run.cands.push_back(alt);
+        }
+    }
+    int32_t w = 0;
+    rc = irbc_tune_select((int32_t)run.cands.size(), measure_schedule, &run, repeats, margin, nullptr, &w);
+    if (!rc) cur = run.cands[w];
+  }
+  if (!rc) rc = irbc_batch_set_schedule(b, &cur);
+  if (!rc && best) *best = cur;
+  if (steps_taken) *steps_taken = run.taken;
+  return rc;
 }
 
 // ---- server -------------------------------------------------------------------

@@ -65,6 +65,49 @@ class View(C.Structure):
          ("filec", C.c_int32)]
 
 
+class Schedule(C.Structure):
+    """irbc_schedule: how a batch launches its members' steps."""
+    _fields_ = [("streams", C.c_int32), ("membrane", C.c_int32), ("graphs", C.c_int32), ("chunk", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# int (*)(int32_t candidate, void* ctx, double* seconds)
+TUNE_MEASURE = C.CFUNCTYPE(C.c_int, C.c_int32, C.c_void_p, C.POINTER(C.c_double))
+ERR_ARG, ERR_CAPACITY = -1, -4
+
+
+def tune_select(n, measure, repeats=3, margin=0.02):
+    """irbc_tune_select over n candidates.  measure(i) runs candidate i once
+    and returns its time in seconds, or None when it cannot run (skipped).
+    Returns (best index, medians with -1 for skipped candidates)."""
+    raised = []
+
+    def cb(i, _ctx, out):
+        if raised:
+            return ERR_ARG
+        try:
+            t = measure(i)
+        except Exception as e:  # an exception cannot cross the C frame
+            raised.append(e)
+            return ERR_ARG
+        if t is None:
+            return ERR_CAPACITY
+        out[0] = float(t)
+        return 0
+
+    fn = TUNE_MEASURE(cb)
+    med = (C.c_double * n)()
+    best = C.c_int32(-1)
+    rc = lib().irbc_tune_select(n, fn, None, repeats, margin, med, C.byref(best))
+    if raised:
+        raise raised[0]
+    if rc != 0:
+        raise IrbcError("irbc_tune_select failed (%d)" % rc)
+    return best.value, list(med)
+
+
 def exported_names():
     """Function names declared in include/irbc.h."""
     import re
@@ -138,6 +181,11 @@ def lib():
     L.irbc_batch_remove.argtypes = [B, H]
     L.irbc_batch_size.argtypes = [B]
     L.irbc_batch_step.argtypes = [B, C.c_int64]
+    L.irbc_batch_set_schedule.argtypes = [B, C.POINTER(Schedule)]
+    L.irbc_batch_get_schedule.argtypes = [B, C.POINTER(Schedule)]
+    L.irbc_tune_select.argtypes = [C.c_int32, TUNE_MEASURE, C.c_void_p, C.c_int32, C.c_double, D, I]
+    L.irbc_batch_autotune.argtypes = [B, C.c_int64, C.c_int32, C.c_double, C.POINTER(Schedule),
+                                      C.POINTER(C.c_int64)]
     L.irbc_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int64, C.POINTER(B)]
     L.irbc_server_submit.argtypes = [B, C.POINTER(Params), D, C.c_int32, I, C.c_int32, I, C.c_int32, C.c_int32,
                                      C.c_int64, C.c_int32, C.POINTER(C.c_int64)]
@@ -406,6 +454,28 @@ class Batch:
         rc = self.L.irbc_batch_step(self.b, n)
         if rc != 0:
             raise IrbcError("irbc_batch_step failed (%d)" % rc)
+
+    def schedule(self):
+        s = Schedule()
+        if self.L.irbc_batch_get_schedule(self.b, C.byref(s)) != 0:
+            raise IrbcError("irbc_batch_get_schedule failed")
+        return s.as_dict()
+
+    def set_schedule(self, **fields):
+        s = Schedule(**{**self.schedule(), **fields})
+        rc = self.L.irbc_batch_set_schedule(self.b, C.byref(s))
+        if rc != 0:
+            raise IrbcError("irbc_batch_set_schedule failed (%d)" % rc)
+
+    def autotune(self, trial_steps=120, repeats=3, margin=0.02):
+        """Tunes the launch schedule on the members themselves; returns
+        (schedule dict, steps every member advanced while tuning)."""
+        s = Schedule()
+        taken = C.c_int64(0)
+        rc = self.L.irbc_batch_autotune(self.b, trial_steps, repeats, margin, C.byref(s), C.byref(taken))
+        if rc != 0:
+            raise IrbcError("irbc_batch_autotune failed (%d)" % rc)
+        return s.as_dict(), taken.value
 
     def close(self):
         if self.b.value:
