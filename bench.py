@@ -372,7 +372,9 @@ def run_batched(G, nrep=64, steps=240, alone=4, nthreads=8):
     """64 replicas of uneven box (Lx in 32..96, Ly = Lz = 32 cells, 10 per
     cell), the 600-vertex mesh, knobs in 100..1000, kon log-uniform in
     1e-4..1e-1, koff in 1e-3..1e-1, FP32 bulk: stepped together vs the
-    first `alone` of them stepped one at a time (the plain path)."""
+    first `alone` of them stepped one at a time (the plain path).  The
+    batch is timed under the default launch schedule and again after
+    irbc_batch_autotune has chosen one on the replicas themselves."""
     import numpy as np
     from irbc_b200 import mesh
     V, E, T = mesh.read_reference_files(*TROPH)
@@ -402,6 +404,14 @@ def run_batched(G, nrep=64, steps=240, alone=4, nthreads=8):
     b.step(48)  # past the first collision: every member's graphs are captured
     t = time.perf_counter()
     b.step(steps)
+    dt0 = time.perf_counter() - t
+    # the launch schedule tuned on the replicas themselves (its trial steps
+    # advance them like any other), then the same stretch timed again
+    t = time.perf_counter()
+    sched, tune_steps = b.autotune(trial_steps=48, repeats=2)
+    tune_s = time.perf_counter() - t
+    t = time.perf_counter()
+    b.step(steps)
     dt = time.perf_counter() - t
     agg = sum(ns) * steps / dt
     finite = all(bool(np.isfinite(s.observables()[:6]).all()) for s in sims)
@@ -412,6 +422,8 @@ def run_batched(G, nrep=64, steps=240, alone=4, nthreads=8):
             "value": agg, "unit": UNIT, "replicas": nrep, "particles": int(sum(ns)), "steps": steps,
             "seconds": dt, "plain_value": plain, "plain_sample": "%d of the replicas alone, one after another" % alone,
             "vs_plain": agg / plain, "host_threads": nthreads, "dtype": "f32-bulk", "state_finite": finite,
+            "schedule": sched, "default_schedule_value": sum(ns) * steps / dt0,
+            "autotune": {"seconds": tune_s, "steps": tune_steps, "trial_steps": 48, "repeats": 2},
             "config": "Lx uniform 32..96, Ly = Lz = 32, 10/cell, 600-vertex mesh, knobs 100..600, "
                       "kon log-U 1e-4..1e-1, koff log-U 1e-3..1e-1, seeded"}
 
