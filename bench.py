@@ -348,7 +348,7 @@ def run_ours(args):
     if world == 1 and args.batch:
         line["batched"] = run_batched(G)
     if world == 1 and args.serve:
-        line["served"] = run_served(G)
+        line["served"] = run_served(G, schedule=line.get("batched", {}).get("schedule"))
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -428,11 +428,13 @@ def run_batched(G, nrep=64, steps=240, alone=4, nthreads=8):
                       "kon log-U 1e-4..1e-1, koff log-U 1e-3..1e-1, seeded"}
 
 
-def run_served(G, nreq=40, rate=8.0, steps_range=(240, 960), nthreads=8):
+def run_served(G, nreq=40, rate=8.0, steps_range=(240, 960), nthreads=8, schedule=None):
     """Poisson-arriving sweep requests (mean `rate`/s, `nreq` of them): kon,
     koff log-uniform, knobs 50..1000 (at most the mesh's vertices), shear
     walls/Lz in 0.002..0.02, Lx 32..128, Ly = Lz in 24..48 cells, the
-    600-vertex or the 2562-vertex mesh, FP32 bulk; admitted by footprint."""
+    600-vertex or the 2562-vertex mesh, FP32 bulk; admitted by footprint.
+    `schedule`: a launch schedule (the batched leg's tuned one) applied to
+    every admitted request."""
     import numpy as np
     from irbc_b200 import mesh
     meshes = [mesh.read_reference_files(*TROPH), mesh.discocyte()]
@@ -452,6 +454,8 @@ def run_served(G, nreq=40, rate=8.0, steps_range=(240, 960), nthreads=8):
             steps = min(steps, 720)
         reqs.append((p, V, E, T, nk, steps, float(rng.exponential(1.0 / rate))))
     srv = G.Server(nthreads=nthreads, round_steps=96)
+    if schedule:
+        srv.set_schedule(**schedule)
     t0 = srv.clock()
     for p, V, E, T, nk, steps, gap in reqs:
         time.sleep(gap)
@@ -470,6 +474,7 @@ def run_served(G, nreq=40, rate=8.0, steps_range=(240, 960), nthreads=8):
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "sims_per_hour": 3600.0 * len(got) / (t1 - t0), "value": work / (t1 - t0), "unit": UNIT,
             "arrival_rate_per_s": rate, "steps_per_request": list(steps_range), "dtype": "f32-bulk",
+            "schedule": schedule or "default",
             "config": "Poisson arrivals; kon log-U 1e-4..1e-1, koff log-U 1e-3..1e-1, knobs 50..1000, "
                       "walls/Lz 0.002..0.02, Lx 32..128, Ly = Lz 24..48, 600- or 2562-vertex mesh"}
 

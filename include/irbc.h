@@ -318,6 +318,11 @@ int32_t irbc_server_poll(irbc_server* s, irbc_result* out, int32_t max, double w
 /* out: pending, active, unread results, bytes in use, budget, particle-steps done */
 int irbc_server_status(irbc_server* s, int64_t out[6]);
 double irbc_server_clock(irbc_server* s);
+/* the launch schedule (irbc_schedule) for simulations admitted from now on
+ * and for the rounds' issue chunk; membrane = 2 applies only to meshes that
+ * fit the one-block form, the others keep the wide kernels.  Results do not
+ * depend on it. */
+int irbc_server_set_schedule(irbc_server* s, const irbc_schedule* sched);
 /* stops the loop; simulations still pending or running are dropped */
 void irbc_server_destroy(irbc_server* s);
 

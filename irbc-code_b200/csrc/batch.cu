@@ -317,6 +317,8 @@ struct irbc_server {
   int64_t budget = 0, used = 0;
   int64_t round = 240;
   int32_t max_active = 256;
+  irbc_schedule sched{2, 1, 0, 24};  // for simulations admitted from now on
+  bool scheduled = false;             // set explicitly: applied at admission
   StepPool pool;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   std::mutex mu;
@@ -336,8 +338,12 @@ namespace {
 // when there is nothing to do
 bool serve_round(irbc_server* s) {
   std::vector<Request> admit;
+  irbc_schedule sched;
+  bool scheduled;
   {
     std::lock_guard<std::mutex> lk(s->mu);
+    sched = s->sched;
+    scheduled = s->scheduled;
     while (!s->pending.empty() && (int32_t)(s->active.size() + admit.size()) < s->max_active &&
            s->used + s->pending.front().footprint <= s->budget) {
       s->used += s->pending.front().footprint;
@@ -371,6 +377,12 @@ bool serve_round(irbc_server* s) {
     int rc = irbc_create(&r.p, &h);
     if (!rc) rc = irbc_init(h, r.V.data(), (int32_t)(r.V.size() / 3), r.E.data(), (int32_t)(r.E.size() / 2),
                             r.T.data(), (int32_t)(r.T.size() / 3), r.nknobs);
+    // the one-block membrane form only where the mesh fits it
+    if (!rc && scheduled && apply_schedule(h, sched)) {
+      irbc_schedule wide = sched;
+      wide.membrane = 1;
+      rc = apply_schedule(h, wide);
+    }
     if (rc) {
       finish(r, h, rc, t_start);
       continue;
@@ -388,7 +400,7 @@ bool serve_round(irbc_server* s) {
     hs.push_back(a.h);
     steps.push_back(std::min(s->round, a.r.nsteps - a.done));
   }
-  const int rc = s->pool.step(hs, steps, 24);
+  const int rc = s->pool.step(hs, steps, sched.chunk);
   std::vector<Active> still;
   for (size_t i = 0; i < s->active.size(); ++i) {
     Active& a = s->active[i];
@@ -483,6 +495,14 @@ extern "C" int irbc_server_status(irbc_server* s, int64_t out[6]) {
   out[3] = s->used;
   out[4] = s->budget;
   out[5] = s->particle_steps;
+  return 0;
+}
+
+extern "C" int irbc_server_set_schedule(irbc_server* s, const irbc_schedule* sched) {
+  if (!s || !sched || !valid_schedule(*sched)) return IRBC_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->sched = *sched;
+  s->scheduled = true;
   return 0;
 }
 

@@ -193,6 +193,7 @@ def lib():
     L.irbc_server_status.argtypes = [B, C.POINTER(C.c_int64)]
     L.irbc_server_clock.restype = C.c_double
     L.irbc_server_clock.argtypes = [B]
+    L.irbc_server_set_schedule.argtypes = [B, C.POINTER(Schedule)]
     L.irbc_server_destroy.argtypes = [B]
     L.irbc_server_destroy.restype = None
     _lib = L
@@ -532,6 +533,13 @@ class Server:
         self.L.irbc_server_status(self.s, out)
         return dict(pending=out[0], active=out[1], results=out[2], used=out[3], budget=out[4],
                     particle_steps=out[5])
+
+    def set_schedule(self, streams=2, membrane=1, graphs=0, chunk=24):
+        """Launch schedule for simulations admitted from now on."""
+        s = Schedule(streams, membrane, graphs, chunk)
+        rc = self.L.irbc_server_set_schedule(self.s, C.byref(s))
+        if rc != 0:
+            raise IrbcError("irbc_server_set_schedule failed (%d)" % rc)
 
     def clock(self):
         return float(self.L.irbc_server_clock(self.s))

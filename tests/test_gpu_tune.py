@@ -51,3 +51,32 @@ def test_autotuned_batch_equals_members_alone():
     b.close()
     for s in sims:
         s.close()
+
+
+def test_server_schedule_keeps_results():
+    """A server given a launch schedule applies it to every request it
+    admits; the one-block membrane form only where the mesh fits it (the
+    600-vertex mesh), the wide kernels elsewhere (the 2562-vertex
+    discocyte).  Every kept result equals the same request run alone."""
+    import irbc_b200 as G
+    from irbc_b200 import mesh
+    troph, disc = H.troph(), mesh.discocyte()
+    reqs = [(_params(51, 0), troph, 96), (_params(52, 1, onrate=300.0, offrate=50.0), troph, 120),
+            (_params(53, 1), disc, 72)]
+    fp = sum(G.lib().irbc_footprint_bytes(G.C.byref(p), len(m[0]), len(m[1]), len(m[2])) for p, m, _ in reqs)
+    srv = G.Server(budget_bytes=int(1.5 * fp), nthreads=2, round_steps=24)
+    srv.set_schedule(streams=1, membrane=2, graphs=1, chunk=48)
+    ids = {}
+    for p, (V, E, T), steps in reqs:
+        ids[srv.submit(p, V, E, T, 300, steps, keep=True)] = (p, (V, E, T), steps)
+    got = []
+    while len(got) < len(reqs):
+        more = srv.poll(8, wait=60.0)
+        assert more, "server stalled"
+        got += more
+    for r in got:
+        assert r["status"] == 0
+        p, (V, E, T), steps = ids[r["id"]]
+        assert H.compare(r["sim"].get_state(), _alone(p, V, E, T, 300, steps), 0.0) == {}, r["id"]
+        r["sim"].close()
+    srv.close()
