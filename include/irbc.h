@@ -281,7 +281,9 @@ int irbc_tune_select(int32_t n, irbc_tune_measure measure, void* ctx, int32_t re
  * no field changes results, so they simply advance the simulations:
  * *steps_taken receives how far every member advanced.  The tuner sets the
  * members' stream, membrane and graph options itself, replacing settings
- * made on the handles before. */
+ * made on the handles before.  IRBC_ERR_STATE for a batch without members;
+ * after a step error the members are left under the candidate that failed,
+ * and *steps_taken counts only the completed trial stretches. */
 int irbc_batch_autotune(irbc_batch* b, int64_t trial_steps, int32_t repeats, double margin, irbc_schedule* best,
                         int64_t* steps_taken);
 /* The server takes whole simulations as requests: parameters, mesh, knob

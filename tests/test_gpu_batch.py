@@ -110,9 +110,10 @@ def test_one_stream_equals_two(precision):
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_one_block_membrane_equals_wide_kernels(precision):
-    """The one-block membrane step (the default for this 600-vertex mesh)
-    and the wide kernels give the same state, bit for bit, across
-    collisions, bond events and a list update."""
+    """The one-block membrane step (an option for meshes up to 1024
+    vertices, such as this 600-vertex one) and the wide kernels (the
+    default) give the same state, bit for bit, across collisions, bond
+    events and a list update."""
     import irbc_b200 as G
     V, E, T = H.troph()
     _, p = _small(13, precision=precision, onrate=300.0, offrate=50.0)
