@@ -57,6 +57,11 @@ VARIANTS = {
     "cfg1": dict(replay=True, defines=None),
     "cfg1_timing": dict(replay=False, defines=None),
     "small": dict(replay=True, defines={"Ns": "40000"}),
+    # the large workload's membrane (2562-vertex discocyte), angle, dtcd and
+    # wall speed in a 32^3 box with a thin solvent, for bit-exact tests
+    "disc_small": dict(replay=True, defines=dict(
+        Lx="32.0", Ly="32.0", Lz="32.0", Ns="40000", Nt="2562", dtcd="0.025", walls="0.32",
+        **_alpha(130.0))),
     "large_timing": dict(replay=False, defines=dict(
         Lx="128.0", Ly="64.0", Lz="64.0", Ns="5242880", Nt="2562", dtcd="0.025",
         walls="0.64", **_alpha(130.0))),

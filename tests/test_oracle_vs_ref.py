@@ -118,3 +118,40 @@ def test_cubic_solver_matches_reference():
         assert np.array_equal(xs_r[:nr if nr > 1 else 3], xs_o[:nr if nr > 1 else 3])
         assert R.call_solve(a, b, c) == L.orc_solve_cubic(a, b, c) or (
             np.isnan(R.call_solve(a, b, c)) and np.isnan(L.orc_solve_cubic(a, b, c)))
+
+
+@pytest.mark.skipif(not os.path.exists(O.ref_lib_path("disc_small")),
+                    reason="reference build oracle/_ref/disc_small not present")
+def test_oracle_bit_exact_on_the_discocyte(tmp_path):
+    """The large workload's membrane: the 2562-vertex discocyte written in the
+    reference's file format, 1000 knobs, its SRD angle, dtcd and wall speed
+    (a 32^3 box, thin solvent).  Mesh build, set-up and 89 steps (9
+    collisions, the list update at step 82, bonds forming and breaking at
+    raised rates) equal the reference bit for bit."""
+    from irbc_b200 import mesh
+    files = mesh.write_reference_files(str(tmp_path), *mesh.discocyte())
+    want = {0, 10, 40, 82, 83, 89}
+    R = O.Reference("disc_small")
+    snaps = {}
+
+    def cb(s):
+        if s in want:
+            snaps[s] = R.get_state(s)
+    assert R.run(*files, 1000, 89, seed=31, on_step=cb, onrate=300.0, offrate=50.0) == 0
+    assert R.p.Nt == 2562
+    V, E, T = O.load_mesh_files(*files)
+    orc = O.Oracle(R.p, 31)
+    orc.init(V, E, T, 1000)
+    M, M2 = R.get_mesh(), orc.get_mesh()
+    for k in M.a:
+        assert np.array_equal(M.a[k], M2.a[k]), k
+    bonds_seen = set()
+    for s in range(0, 90):
+        orc.step_part1()
+        if s in snaps:
+            st = orc.get_state()
+            assert _diff(st, snaps[s]) == {}, s
+            assert st.s["Sarea"] == snaps[s].s["Sarea"] and st.s["Volume"] == snaps[s].s["Volume"]
+            bonds_seen.add(int(st.a["bondi"].sum()))
+        orc.step_part2()
+    assert max(bonds_seen) > 0
