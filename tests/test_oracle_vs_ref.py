@@ -33,6 +33,45 @@ def _diff(a, b):
     return {k: v for k, v in d.items() if v != 0}
 
 
+def _crossing_state(st, M, ntri, seed):
+    """A copy of st whose first 2*ntri particles sit 0.004 off the
+    centroids of ntri sampled triangles, one on each side, moving at speed 5
+    towards the membrane: each crosses it within dtmd (0.002).  Each one's
+    indio names the side it starts on as the reference's side test reads
+    it (1 where (B-A) x (C-A) points at the particle), so that none is
+    skipped as already being on the wrong side."""
+    out = st.copy()
+    pos = np.stack([st.a["x"], st.a["y"], st.a["z"]], axis=1)
+    T = np.stack([M.a["t1"], M.a["t2"], M.a["t3"]], axis=1)
+    rng = np.random.default_rng(seed)
+    for k, j in enumerate(rng.choice(len(T), ntri, replace=False)):
+        A, B, C = pos[T[j]]
+        c = (A + B + C) / 3.0
+        n = np.cross(B - A, C - A)
+        n /= np.linalg.norm(n)
+        for side, i in ((1.0, 2 * k), (-1.0, 2 * k + 1)):
+            out.a["sx"][i], out.a["sy"][i], out.a["sz"][i] = c + side * 0.004 * n
+            out.a["svx"][i], out.a["svy"][i], out.a["svz"][i] = -side * 5.0 * n
+            out.a["sindio"][i] = 1 if side > 0 else 0
+    return out
+
+
+def _check_crossings(R, orc, st, M, ntri, step):
+    """reflectionFed on particles that must cross the membrane: the same
+    contact times and the same reflected states."""
+    cs = _crossing_state(st, M, ntri, 17)
+    R.set_state(cs)
+    orc.set_state(cs)
+    fr = np.array([R.call_reflection(i) for i in range(2 * ntri)])
+    fo = np.array([orc.reflection(i) for i in range(2 * ntri)])
+    assert np.array_equal(fr, fo)
+    # nearly all of them crossed (one may meet its triangle's edge or miss
+    # its cell's list; both sides must agree on those too)
+    assert np.count_nonzero(fr) >= 0.95 * 2 * ntri
+    assert _diff(R.get_state(step), orc.get_state()) == {}
+    assert _diff(R.get_state(step), cs) != {}  # and was reflected
+
+
 def test_init_prints_known_answers(capfd):
     """maincode.cpp:256-257,345-346,366-368,446 printouts (seed-independent)."""
     R, _ = _run_ref(0, 7, set())
@@ -103,6 +142,7 @@ def test_phase_functions_bit_exact():
     fo = np.array([orc.reflection(i) for i in range(st.ns)])
     assert np.array_equal(fr, fo)
     assert _diff(R.get_state(30), orc.get_state()) == {}
+    _check_crossings(R, orc, st, M, 200, 30)
 
 
 def test_cubic_solver_matches_reference():
@@ -155,3 +195,27 @@ def test_oracle_bit_exact_on_the_discocyte(tmp_path):
             bonds_seen.add(int(st.a["bondi"].sum()))
         orc.step_part2()
     assert max(bonds_seen) > 0
+    # each phase function, reflectionFed for every particle, and
+    # reflectionFed for particles placed to cross the membrane, called
+    # directly on the state of step 89
+    st = snaps[89]
+    for name, call_ref, call_orc in (
+            ("collide", lambda: R.call_collide(91), lambda: orc.collide(91)),
+            ("llist", R.call_llist, orc.llist_update),
+            ("totalva", R.call_totalva, orc.total_va),
+            ("pfdt", R.call_pfdt, orc.pfdt),
+            ("forces", R.call_forces, orc.forces)):
+        R.set_state(st)
+        orc.set_state(st)
+        call_ref()
+        call_orc()
+        a, b = R.get_state(89), orc.get_state()
+        assert _diff(a, b) == {}, name
+        assert a.s["Sarea"] == b.s["Sarea"], name
+    R.set_state(st)
+    orc.set_state(st)
+    fr = np.array([R.call_reflection(i) for i in range(st.ns)])
+    fo = np.array([orc.reflection(i) for i in range(st.ns)])
+    assert np.array_equal(fr, fo)
+    assert _diff(R.get_state(89), orc.get_state()) == {}
+    _check_crossings(R, orc, st, M, 200, 89)
