@@ -55,10 +55,21 @@ sys.path.insert(0, os.path.join(ROOT, "irbc-code_b200"))
 
 METRIC = "MPCD solvent particle-steps/s (large single simulation, 128x64x64, 5.24M particles)"
 UNIT = "particle-steps/s"
-WORKLOAD = dict(workload="large single simulation: box 128x64x64, 5242880 solvent, 2562-vertex discocyte "
+
+
+def workload_config():
+    from irbc_b200 import mesh, workloads
+    W = workloads.LARGE
+    V, E, _ = workloads.large_mesh()
+    return dict(workload="large single simulation: box 128x64x64, 5242880 solvent, 2562-vertex discocyte "
                          "R=4, 1000 knobs, alpha 130 deg, dtcd 0.025, dtmd 0.002, walls 0.64",
-                Lx=128.0, Ly=64.0, Lz=64.0, Ns=5242880, alpha_deg=130.0, dtcd=0.025, dtmd=0.002, walls=0.64,
-                nknobs=1000, kon=0.005, koff=0.015)
+                Lx=W["Lx"], Ly=W["Ly"], Lz=W["Lz"], Ns=W["Ns"], alpha_deg=W["alpha_deg"], dtcd=W["dtcd"],
+                dtmd=W["dtmd"], walls=W["walls"], nknobs=W["nknobs"], kon=W["kon"], koff=W["koff"],
+                elap=round(mesh.scaled_elap(V, E), 8), mesh="icosphere level 4 relaxed on the Evans-Fung surface")
+
+
+# whole collision cycles: a collision every 12 steps (dtcd / dtmd)
+CYCLE = 12
 
 
 def peaks():
@@ -157,12 +168,8 @@ def gpu_warm(device, seconds):
 
 
 def make_params(G, seed, precision):
-    import math
-    W = WORKLOAD
-    a = math.radians(W["alpha_deg"])
-    return G.default_params(Lx=W["Lx"], Ly=W["Ly"], Lz=W["Lz"], Ns=W["Ns"], cosalpha=math.cos(a),
-                            sinalpha=math.sin(a), dtcd=W["dtcd"], dtmd=W["dtmd"], walls=W["walls"],
-                            onrate=W["kon"], offrate=W["koff"], Nt=2562, seed=seed, precision=precision)
+    from irbc_b200 import workloads
+    return workloads.large_params(seed, precision)
 
 
 def dist_setup():
@@ -239,7 +246,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": d["value"], "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": warm, "ms_per_step": 1e3 * d["seconds"] / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, parallelism="host OpenMP, %d threads" % d["cores"]),
+        "config": dict(workload_config(), parallelism="host OpenMP, %d threads" % d["cores"]),
         "cpu_baseline": {"value": d["value"], "unit": UNIT, "cores": d["cores"], "kind": "reference",
                          "sample": "%d whole timesteps after %d warm-up of the reference's main loop "
                                    "(oracle/_ref/large_timing, -O3 -fopenmp, its own Mersenne Twister); "
@@ -253,13 +260,16 @@ def run_ours(args):
     world, rank, local = dist_setup()
     import numpy as np
     import irbc_b200 as G
-    from irbc_b200 import mesh
+    from irbc_b200 import workloads
     precision = G.FP32 if args.precision == "fp32" else G.FP64
+    # whole collision cycles, so that the timed steps hold the collision at
+    # its own frequency
+    steps = -(-args.steps // CYCLE) * CYCLE
     p = make_params(G, seed=replica_seed(rank), precision=precision)
     p.device = local
     sim = G.Simulation(p)
-    V, E, T = mesh.discocyte()
-    sim.init(V, E, T, WORKLOAD["nknobs"])
+    V, E, T = workloads.large_mesh()
+    sim.init(V, E, T, workloads.LARGE["nknobs"])
     sim.step(args.warmup)
     sim.sync()
     # the end-to-end leg below replays the same steps from this state
@@ -276,15 +286,15 @@ def run_ours(args):
         barrier(world)
         sim.timer_begin()
         h0 = time.perf_counter()
-        sim.step(args.steps)
+        sim.step(steps)
         host_enqueue_s = time.perf_counter() - h0
         t_local = sim.timer_end()
         sim.sync()
         barrier(world)
     launches = int(sim.L.irbc_launch_count(sim.h)) - launches0
     t_ms = reduce_max(t_local, world)
-    ns = WORKLOAD["Ns"]
-    value = aggregate(ns, args.steps, world, t_ms)
+    ns = workloads.LARGE["Ns"]
+    value = aggregate(ns, steps, world, t_ms)
     # the state must still be physical after the timed steps
     finite = bool(np.isfinite(sim.observables()[:6]).all())
     # per-phase and per-kernel times: a short profiled window right after
@@ -293,13 +303,19 @@ def run_ours(args):
     sim.step(48)
     kprof = sim.profile_end()
     # roofline of the dominant kernel, the bulk streaming kernel (one launch
-    # per step over every particle): algorithmic bytes per particle = state
-    # read + positions written (FP64: positions 3 x 8 and the 32-byte
-    # velocity record read, 3 x 8 written; FP32: two float4 read, one
-    # written), divided by its CUDA-event time per launch
-    bpp = 80 if precision == G.FP64 else 48
+    # per step over every particle): its algorithmic bytes per particle are
+    # the stream's state read and positions written -- FP64: positions 3 x 8
+    # and velocities 3 x 8 read, positions 3 x 8 written = 72 B; FP32: two
+    # float4 read, one written = 48 B (the 32-byte FP64 velocity record
+    # carries the reference index too, so the kernel moves 80 B, counted
+    # here as 72) -- divided by its CUDA-event time per launch
+    bpp = 72 if precision == G.FP64 else 48
     bulk_avg_ms = kprof["bulk_ms"] / max(1, kprof["bulk_launches"])
     achieved = ns * bpp / (bulk_avg_ms * 1e-3) / 1e9
+    # the whole step against the same bound: streaming every step plus the
+    # collision's read and write once per 10-12 steps (79.2 B FP64, 52.8 B
+    # FP32 per particle-step), at the measured particle-steps/s
+    step_bpp = 79.2 if precision == G.FP64 else 52.8
     peak, kind = peaks()
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "stream_traffic.json")
@@ -313,23 +329,28 @@ def run_ours(args):
     # page-locked memory, every step the RBCdata record out, the final state out
     e2e = None
     if args.e2e:
-        e2e = run_e2e(G, sim, start, args.steps, world)
+        e2e = run_e2e(G, sim, start, steps, workloads.LARGE["Ns"])
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "steps_requested": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if precision == G.FP64 else "f32", "data": "synthetic",
-        "config": dict(WORKLOAD, parallelism="replicas x%d" % world if world > 1 else "single GPU",
-                       l2="state larger than L2 (no flush needed)"),
+        "config": dict(workload_config(), parallelism="replicas x%d" % world if world > 1 else "single GPU",
+                       l2="state larger than L2 (no flush needed)",
+                       timed="whole collision cycles: the requested steps rounded up to a multiple of 12"),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "kernel": "k_stream_fast" if precision == G.FP64 else "k_stream_f",
                      "bytes_per_particle": bpp, "units_per_launch": ns, "peak_kind": kind,
-                     "kernel_ms_avg": bulk_avg_ms},
+                     "kernel_ms_avg": bulk_avg_ms,
+                     "step_bytes_per_particle_step": step_bpp,
+                     "step_achieved": value / world * step_bpp / 1e9,
+                     "step_frac": value / world * step_bpp / 1e9 / peak},
         "phase_ms_per_step": {"stream": kprof["stream_ms"] / 48, "collide": kprof["collide_ms"] / 48,
                               "membrane": kprof["membrane_ms"] / 48,
                               "window": "48 steps after the timed steps"},
         "gpu_launches": launches,
-        "host_enqueue_ms_per_step": 1e3 * host_enqueue_s / args.steps,
+        "host_enqueue_ms_per_step": 1e3 * host_enqueue_s / steps,
         "clocks": clocks.summary(),
         "state_finite": finite,
     }
@@ -360,99 +381,137 @@ TROPH = [os.path.join(ROOT, "tests", "golden", "troph600", n) for n in ("TrophV6
                                                                       "TrophT600.dat")]
 
 
-def replica_params(G, rng, precision, Lx, Ly, Lz, seed, kon, koff, walls_frac=0.01):
-    import math
-    a = math.radians(130.0)
-    return G.default_params(Lx=float(Lx), Ly=float(Ly), Lz=float(Lz), Ns=int(Lx * Ly * (Lz + 1) * 10),
-                            cosalpha=math.cos(a), sinalpha=math.sin(a), dtcd=0.025, dtmd=0.002,
-                            walls=walls_frac * Lz, onrate=kon, offrate=koff, seed=seed, precision=precision)
-
-
-def run_batched(G, nrep=64, steps=240, alone=4, nthreads=8):
+def run_batched(G, nrep=64, steps=240, nthreads=8):
     """64 replicas of uneven box (Lx in 32..96, Ly = Lz = 32 cells, 10 per
-    cell), the 600-vertex mesh, knobs in 100..1000, kon log-uniform in
-    1e-4..1e-1, koff in 1e-3..1e-1, FP32 bulk: stepped together vs the
-    first `alone` of them stepped one at a time (the plain path).  The
-    batch is timed under the default launch schedule and again after
-    irbc_batch_autotune has chosen one on the replicas themselves."""
+    cell), the 600-vertex mesh, knobs in 100..600 (the reference's knob
+    placement cannot place more knobs than the mesh has vertices), kon
+    log-uniform in 1e-4..1e-1, koff in 1e-3..1e-1, FP32 bulk.  Timed: every
+    replica alone on the plain path, one after another (the plain value);
+    the batch with one launch per phase over all replicas (the default
+    schedule); the batch through the pool of host threads (fused = 0); and
+    the batch under the schedule irbc_batch_autotune chose on the replicas
+    themselves.  Each timed stretch is `steps` steps (whole collision
+    cycles) after a warm-up, host wall clock with the device work waited
+    for."""
     import numpy as np
-    from irbc_b200 import mesh
+    from irbc_b200 import mesh, workloads
     V, E, T = mesh.read_reference_files(*TROPH)
     rng = np.random.default_rng(2024)
     sims = []
     for r in range(nrep):
         Lx = int(rng.integers(32, 97))
         kon, koff = 10 ** rng.uniform(-4, -1), 10 ** rng.uniform(-3, -1)
-        p = replica_params(G, rng, G.FP32, Lx, 32, 32, 5000 + r, kon, koff)
+        p = workloads.replica_params(Lx, 32, 32, 5000 + r, kon, koff, precision=G.FP32)
         s = G.Simulation(p)
         s.init(V, E, T, int(rng.integers(100, 601)))
         sims.append(s)
     ns = [s.params.Ns for s in sims]
-    # plain path: each replica alone, one after the other
+    total = sum(ns)
+    # plain path: every replica alone, one after the other
     t_alone = 0.0
-    for s in sims[:alone]:
+    for s in sims:
         s.step(48)
         s.sync()
         t = time.perf_counter()
         s.step(steps)
         s.sync()
         t_alone += time.perf_counter() - t
-    plain = sum(ns[:alone]) * steps / t_alone
+    plain = total * steps / t_alone
+
+    def timed(b, n):
+        t = time.perf_counter()
+        b.step(n)
+        return time.perf_counter() - t
+
     b = G.Batch(nthreads=nthreads)
     for s in sims:
         b.add(s)
-    b.step(48)  # past the first collision: every member's graphs are captured
-    t = time.perf_counter()
-    b.step(steps)
-    dt0 = time.perf_counter() - t
+    b.step(48)  # the cohort's tables built, every kernel loaded
+    l0 = sims[0].launch_count()
+    dt_fused = timed(b, steps)
+    launches = (sims[0].launch_count() - l0) / steps
+    b.set_schedule(fused=0)
+    b.step(48)
+    dt_pool = timed(b, steps)
+    b.set_schedule(fused=1)
     # the launch schedule tuned on the replicas themselves (its trial steps
     # advance them like any other), then the same stretch timed again
     t = time.perf_counter()
     sched, tune_steps = b.autotune(trial_steps=48, repeats=2)
     tune_s = time.perf_counter() - t
-    t = time.perf_counter()
-    b.step(steps)
-    dt = time.perf_counter() - t
-    agg = sum(ns) * steps / dt
+    dt = timed(b, steps)
+    agg = total * steps / dt
     finite = all(bool(np.isfinite(s.observables()[:6]).all()) for s in sims)
+    health = [s.health() for s in sims]
     b.close()
     for s in sims:
         s.close()
+    peak, kind = peaks()
     return {"metric": "aggregate solvent particle-steps/s, %d replicas stepped together" % nrep,
-            "value": agg, "unit": UNIT, "replicas": nrep, "particles": int(sum(ns)), "steps": steps,
-            "seconds": dt, "plain_value": plain, "plain_sample": "%d of the replicas alone, one after another" % alone,
-            "vs_plain": agg / plain, "host_threads": nthreads, "dtype": "f32-bulk", "state_finite": finite,
-            "schedule": sched, "default_schedule_value": sum(ns) * steps / dt0,
+            "value": agg, "unit": UNIT, "replicas": nrep, "particles": int(total), "steps": steps,
+            "seconds": dt, "ms_per_batch_step": 1e3 * dt / steps,
+            "plain_value": plain, "plain_sample": "all %d replicas alone, one after another" % nrep,
+            "vs_plain": agg / plain,
+            "fused_default_value": total * steps / dt_fused, "pool_value": total * steps / dt_pool,
+            "launches_per_batch_step": launches,
+            "roofline": {"bytes_per_particle_step": 52.8, "achieved_gbs": agg * 52.8 / 1e9, "peak": peak,
+                         "peak_kind": kind, "frac": agg * 52.8 / 1e9 / peak},
+            "host_threads": nthreads, "dtype": "f32-bulk", "state_finite": finite, "healthy": not any(health),
+            "schedule": sched,
             "autotune": {"seconds": tune_s, "steps": tune_steps, "trial_steps": 48, "repeats": 2},
             "config": "Lx uniform 32..96, Ly = Lz = 32, 10/cell, 600-vertex mesh, knobs 100..600, "
                       "kon log-U 1e-4..1e-1, koff log-U 1e-3..1e-1, seeded"}
 
 
-def run_served(G, nreq=40, rate=8.0, steps_range=(240, 960), nthreads=8, schedule=None):
-    """Poisson-arriving sweep requests (mean `rate`/s, `nreq` of them): kon,
-    koff log-uniform, knobs 50..1000 (at most the mesh's vertices), shear
-    walls/Lz in 0.002..0.02, Lx 32..128, Ly = Lz in 24..48 cells, the
-    600-vertex or the 2562-vertex mesh, FP32 bulk; admitted by footprint.
-    `schedule`: a launch schedule (the batched leg's tuned one) applied to
-    every admitted request."""
+def served_requests(G, nreq, rate, scale, seed=77):
+    """The serving workload's requests: Poisson arrivals (mean `rate`/s),
+    kon log-uniform in 1e-4..1e-1, koff in 1e-3..1e-1, knobs 50..1000 (at
+    most the mesh's vertices), shear walls/Lz in 0.002..0.02, Lx 32..128,
+    Ly = Lz in 24..48 cells, the 600-vertex trophozoite or the 2562-vertex
+    discocyte, FP32 bulk, and 10k..200k steps times `scale` (rounded to
+    whole 24-step stretches).  Returns (params, V, E, T, knobs, steps, gap)."""
     import numpy as np
-    from irbc_b200 import mesh
+    from irbc_b200 import mesh, workloads
     meshes = [mesh.read_reference_files(*TROPH), mesh.discocyte()]
-    rng = np.random.default_rng(77)
+    rng = np.random.default_rng(seed)
     reqs = []
     for k in range(nreq):
-        V, E, T = meshes[int(rng.integers(0, 2))]
+        which = int(rng.integers(0, 2))
+        V, E, T = meshes[which]
         Ly = int(rng.integers(24, 49))
-        p = replica_params(G, rng, G.FP32, int(rng.integers(32, 129)), Ly, Ly, 9000 + k,
-                           10 ** rng.uniform(-4, -1), 10 ** rng.uniform(-3, -1), rng.uniform(0.002, 0.02))
+        p = workloads.replica_params(int(rng.integers(32, 129)), Ly, Ly, 9000 + k, 10 ** rng.uniform(-4, -1),
+                                     10 ** rng.uniform(-3, -1), precision=G.FP32,
+                                     walls_frac=rng.uniform(0.002, 0.02), mesh_ve=(V, E) if which else None)
         nk = int(rng.integers(50, min(1000, len(V)) + 1))
-        steps = int(rng.integers(steps_range[0] // 24, steps_range[1] // 24 + 1)) * 24
-        if len(V) > 1000:
-            # the synthetic discocyte's membrane blows up after ~800-1400
-            # steps at dtmd 0.002 (in the reference's arithmetic too):
-            # requests on it stay inside its stable window
-            steps = min(steps, 720)
+        steps = max(24, int(round(rng.uniform(10000, 200000) * scale / 24.0)) * 24)
         reqs.append((p, V, E, T, nk, steps, float(rng.exponential(1.0 / rate))))
+    return reqs
+
+
+def run_alone_timed(G, p, V, E, T, nk, steps):
+    """one request on the plain path: create, set up, step, observables;
+    host seconds with the device work waited for"""
+    import numpy as np
+    t = time.perf_counter()
+    sim = G.Simulation(p)
+    sim.init(V, E, T, nk)
+    sim.step(steps)
+    obs = sim.observables()
+    sim.sync()
+    dt = time.perf_counter() - t
+    sim.close()
+    return dt, bool(np.isfinite(obs[:6]).all())
+
+
+def run_served(G, nreq=40, rate=2.0, scale=0.02, nthreads=8, schedule=None):
+    """Poisson-arriving sweep requests admitted by the request server by
+    device-memory footprint (served_requests), against the plain path: the
+    same requests each run alone, and those alone times pushed through a
+    one-at-a-time queue under the same arrival times.  `schedule`: a launch
+    schedule (the batched leg's tuned one) applied to every admitted
+    request."""
+    import numpy as np
+    reqs = served_requests(G, nreq, rate, scale)
     srv = G.Server(nthreads=nthreads, round_steps=96)
     if schedule:
         srv.set_schedule(**schedule)
@@ -462,24 +521,54 @@ def run_served(G, nreq=40, rate=8.0, steps_range=(240, 960), nthreads=8, schedul
         srv.submit(p, V, E, T, nk, steps)
     got = []
     while len(got) < nreq:
-        more = srv.poll(64, wait=60.0)
+        more = srv.poll(64, wait=120.0)
         if not more:
             break
         got += more
     t1 = srv.clock()
     srv.close()
-    lat = np.array([r["t_end"] - r["t_submit"] for r in got])
+    by_id = {r["id"]: r for r in got}
+    ids = sorted(by_id)
+    lat = np.array([by_id[i]["t_end"] - by_id[i]["t_submit"] for i in ids])
+    arrive = np.array([by_id[i]["t_submit"] for i in ids])
+    ok = int(sum(r["status"] == 0 for r in got))
     work = sum(r["ns"] * r["steps"] for r in got if r["status"] == 0)
-    return {"metric": "served sweep requests", "requests": nreq, "completed": int(sum(r["status"] == 0 for r in got)),
+    # the plain path: every request alone, one after another
+    alone, alone_ok = [], True
+    for p, V, E, T, nk, steps, _ in reqs:
+        dt, fin = run_alone_timed(G, p, V, E, T, nk, steps)
+        alone.append(dt)
+        alone_ok = alone_ok and fin
+    alone = np.array(alone)
+    # one at a time in arrival order under the same arrivals
+    done, plain_lat = 0.0, []
+    for a, d in zip(arrive, alone[:len(arrive)]):
+        done = max(done, a) + d
+        plain_lat.append(done - a)
+    plain_lat = np.array(plain_lat)
+    plain_span = done - arrive[0] if len(arrive) else float("nan")
+    span = t1 - t0
+    return {"metric": "served sweep requests", "requests": nreq, "completed": ok,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "sims_per_hour": 3600.0 * len(got) / (t1 - t0), "value": work / (t1 - t0), "unit": UNIT,
-            "arrival_rate_per_s": rate, "steps_per_request": list(steps_range), "dtype": "f32-bulk",
-            "schedule": schedule or "default",
-            "config": "Poisson arrivals; kon log-U 1e-4..1e-1, koff log-U 1e-3..1e-1, knobs 50..1000, "
-                      "walls/Lz 0.002..0.02, Lx 32..128, Ly = Lz 24..48, 600- or 2562-vertex mesh"}
+            "sims_per_hour": 3600.0 * len(got) / span, "value": work / span, "unit": UNIT,
+            "plain_alone_p50_s": float(np.percentile(alone, 50)), "plain_alone_p99_s": float(np.percentile(alone, 99)),
+            "plain_p50_s": float(np.percentile(plain_lat, 50)), "plain_p99_s": float(np.percentile(plain_lat, 99)),
+            "plain_sims_per_hour": 3600.0 * len(plain_lat) / plain_span,
+            "plain_busy_s": float(alone.sum()), "plain_finite": alone_ok,
+            "vs_plain": {"p50": float(np.percentile(lat, 50) / np.percentile(plain_lat, 50)),
+                         "p99": float(np.percentile(lat, 99) / np.percentile(plain_lat, 99)),
+                         "sims_per_hour": float((len(got) / span) / (len(plain_lat) / plain_span))},
+            "plain_note": "each request alone on the plain path (create, set-up, steps, observables), then those "
+                          "times pushed through a one-at-a-time queue under the same arrival times",
+            "arrival_rate_per_s": rate, "step_scale": scale,
+            "steps_per_request": [int(min(r[5] for r in reqs)), int(max(r[5] for r in reqs))],
+            "dtype": "f32-bulk", "schedule": schedule or "default",
+            "config": "Poisson arrivals at %g/s; kon log-U 1e-4..1e-1, koff log-U 1e-3..1e-1, knobs 50..1000, "
+                      "walls/Lz 0.002..0.02, Lx 32..128, Ly = Lz 24..48, 600- or 2562-vertex mesh, "
+                      "10k..200k steps x %g" % (rate, scale)}
 
 
-def run_e2e(G, sim, st, steps, world):
+def run_e2e(G, sim, st, steps, ns):
     """Same metric through the public API with host buffers: set_state of
     the full state `st` (the state the timed steps started from) from
     page-locked memory, the same `steps` steps each followed by the RBCdata
@@ -524,7 +613,6 @@ def run_e2e(G, sim, st, steps, world):
     dt = t3 - t0
     # the list entries copied, not the buffer's spare room
     d2h = d2h_rec * steps + sum(out.a[k].nbytes for k in out.a if k != "lidx") + 4 * int(out.a["llen"].sum())
-    ns = WORKLOAD["Ns"]
     return {"value": ns * steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d / steps),
             "d2h_bytes_per_step": int(d2h / steps),
             "seconds": {"set_state": t1 - t0, "steps": t2 - t1, "get_state": t3 - t2}}

@@ -28,6 +28,7 @@ extern "C" {
 #define IRBC_ERR_STATE -3    /* call out of order (no mesh, no solvent)       */
 #define IRBC_ERR_CAPACITY -4 /* a list outgrew its capacity                   */
 #define IRBC_ERR_IO -5       /* file could not be written                     */
+#define IRBC_ERR_HEALTH -6   /* the state went bad: non-finite or out of box   */
 
 #define IRBC_FP64 0          /* all solvent arithmetic in double               */
 #define IRBC_FP32 1          /* solvent state and arithmetic in float          */
@@ -149,7 +150,9 @@ int irbc_set_streams(irbc_handle* h, int32_t n);
  * (the default) as wide kernels over many SMs; mode 2 as one block per
  * launch, two kernels per step instead of eight, for meshes up to 1024
  * vertices (IRBC_ERR_CAPACITY for a larger mesh; a mesh set later keeps
- * the wide kernels).  The results are the same either way. */
+ * the wide kernels); mode 3 as one launch of a thread-block cluster (8
+ * blocks of 512 threads on one GPC, its phases separated by cluster
+ * barriers), any mesh.  The results are the same in every mode. */
 int irbc_set_membrane_kernels(irbc_handle* h, int32_t mode);
 int irbc_step_part1(irbc_handle* h);
 int irbc_step_part2(irbc_handle* h);
@@ -183,8 +186,10 @@ int irbc_bin_particles(const irbc_params* p, const double* x, const double* y, c
  * static device array (4 MiB plus 12 KiB) that every GPU loading the library
  * keeps until the process exits, so boxes are limited to 1,048,576 cells
  * (Lx*Ly*(Lz+1)); larger boxes return IRBC_ERR_CAPACITY.  The first call on
- * a device looks up the array's device address; make that first call before
- * any stream capture.  All calls share the one array, so calls that overlap
+ * a device looks up the array's device address and keeps it for the life of
+ * the process; make that first call before any stream capture, and do not
+ * use this entry point on a device after cudaDeviceReset (which can move
+ * the array).  All calls share the one array, so calls that overlap
  * on the GPU (other host threads, other streams) race; this one runs on the
  * legacy default stream and returns after it has finished. */
 int irbc_bin_particles_noalloc(const irbc_params* p, const double* x, const double* y, const double* z,
@@ -204,14 +209,29 @@ int irbc_write_stl(irbc_handle* h, const char* path);
  * asynchronously. */
 int64_t irbc_record_bytes(const irbc_handle* h);
 int irbc_record_async(irbc_handle* h, void* host, int64_t bytes);
-/* observables not in the reference: out[0..] = mean solvent kT, centre of
- * mass x,y,z (unwrapped), Sarea, Volume, bond count */
+/* observables not in the reference: out[0] = solvent kT from peculiar
+ * velocities (each particle's velocity minus the mean velocity of its
+ * z-layer of height a, so the Couette flow's kinetic energy is not counted
+ * as heat), out[1..3] = membrane centre of mass x,y,z (unwrapped), out[4] =
+ * Sarea, out[5] = Volume, out[6] = bond count, out[7] = mean solvent vx,
+ * out[8] = sum m|v|^2 / (3 Ns) with the flow included; nout <= 9 values */
 int irbc_observables(irbc_handle* h, double* out, int32_t nout);
 /* Couette profile: mean vx of the solvent per z-layer of height a, nbins = Lz/a */
 int irbc_velocity_profile(irbc_handle* h, double* out, int32_t nbins);
 
-/* ---- timing and host buffers (not in the reference) ------------------------------ */
+/* ---- health, timing and host buffers (not in the reference) ----------------------
+ * The kernels that write the state check it as they go: a solvent particle
+ * whose position or velocity is not finite or whose height left [-a, Lz + a]
+ * sets bit 1, a membrane vertex whose force or velocity is not finite sets
+ * bit 2 of the simulation's health word.  (The reference has no such check:
+ * a blown-up run of it prints NaN into RBCdata.dat.)  irbc_sync waits for
+ * the queued work and returns IRBC_ERR_HEALTH when the word is set;
+ * irbc_step returns it, without stepping, once the word copied at the end
+ * of an earlier irbc_step shows a problem.  irbc_set_state clears it. */
 int irbc_sync(irbc_handle* h);
+/* waits like irbc_sync and writes the health word (0: healthy) to *flags;
+ * returns 0 unless the wait itself fails */
+int irbc_health(irbc_handle* h, int32_t* flags);
 /* kernel launches issued by this handle since creation */
 int64_t irbc_launch_count(const irbc_handle* h);
 /* CUDA-event timing on the handle's stream between begin and end.
@@ -250,9 +270,16 @@ int irbc_batch_step(irbc_batch* b, int64_t n);
  *             2 one block; default 1)
  *   graphs    irbc_set_graphs for every member (0 or 1; default 0)
  *   chunk     steps a pool thread issues to one member before it turns to
- *             its next member (a multiple of 24 in 24..2400; default 24) */
+ *             its next member (a multiple of 24 in 24..2400; default 24)
+ *   fused     1 (the default): FP32 members in the same phase (created or
+ *             admitted together, stepped together) advance as one cohort,
+ *             each phase of the step ONE kernel launch over all of them,
+ *             its blocks split among the members; streams, membrane and
+ *             graphs then apply only to the other members (FP64, or out of
+ *             phase), which the pool of host threads steps.  0: every
+ *             member through the pool. */
 typedef struct irbc_schedule {
-  int32_t streams, membrane, graphs, chunk;
+  int32_t streams, membrane, graphs, chunk, fused;
 } irbc_schedule;
 /* Applies s to every member now and to every member added later.  On an
  * error (IRBC_ERR_CAPACITY: a member's mesh is too large for membrane = 2)
@@ -273,7 +300,7 @@ typedef int (*irbc_tune_measure)(int32_t candidate, void* ctx, double* seconds);
 int irbc_tune_select(int32_t n, irbc_tune_measure measure, void* ctx, int32_t repeats, double margin,
                      double* medians, int32_t* best);
 /* Tunes the batch's schedule on its own members, one field at a time in
- * the order membrane, streams, graphs, chunk (24, 96, 240): the current
+ * the order fused, membrane, streams, graphs, chunk (24, 96, 240): the current
  * value against the others, each candidate scored by irbc_tune_select as
  * the host time of trial_steps batch steps with their device work waited
  * for.  Ends with the winner applied (to members added later too) and
@@ -295,8 +322,13 @@ int irbc_batch_autotune(irbc_batch* b, int64_t trial_steps, int32_t repeats, dou
  * arrive meanwhile join at the next round.  A finished simulation yields an
  * irbc_result: its times on the server clock (seconds since creation), its
  * observables (irbc_observables) and, when submitted with keep = 1, its
- * handle, which the caller then owns and destroys; otherwise the server
- * frees it.  Each simulation computes exactly what it would alone. */
+ * handle; otherwise the server frees it.  A kept handle's device memory
+ * stays charged to the budget until the caller hands it back with
+ * irbc_server_release (which destroys it); after irbc_server_destroy the
+ * caller destroys kept handles with irbc_destroy.  Each simulation computes
+ * exactly what it would alone, and each has its own status: one that fails
+ * (a CUDA error, or IRBC_ERR_HEALTH) ends with that status while the others
+ * go on. */
 typedef struct irbc_server irbc_server;
 typedef struct irbc_result {
   int64_t id;
@@ -317,7 +349,8 @@ int irbc_server_submit(irbc_server* s, const irbc_params* p, const double* V, in
 /* up to max finished results, waiting up to wait_s seconds for the first;
  * returns how many were written */
 int32_t irbc_server_poll(irbc_server* s, irbc_result* out, int32_t max, double wait_s);
-/* out: pending, active, unread results, bytes in use, budget, particle-steps done */
+/* out: pending, active, unread results, bytes in use (kept handles not yet
+ * released included), budget, particle-steps done */
 int irbc_server_status(irbc_server* s, int64_t out[6]);
 double irbc_server_clock(irbc_server* s);
 /* the launch schedule (irbc_schedule) for simulations admitted from now on
@@ -325,7 +358,12 @@ double irbc_server_clock(irbc_server* s);
  * fit the one-block form, the others keep the wide kernels.  Results do not
  * depend on it. */
 int irbc_server_set_schedule(irbc_server* s, const irbc_schedule* sched);
-/* stops the loop; simulations still pending or running are dropped */
+/* destroys a kept handle (a polled result of a keep = 1 request) and frees
+ * its share of the budget; IRBC_ERR_ARG for a handle the server did not hand
+ * out */
+int irbc_server_release(irbc_server* s, irbc_handle* h);
+/* stops the loop; simulations still pending or running are dropped, and so
+ * are the handles of results never polled */
 void irbc_server_destroy(irbc_server* s);
 
 /* page-locked host memory for fast state exchange */

@@ -3,6 +3,7 @@
 // 94-446), state exchange in the reference's layout, the step sequence of
 // the loop body (maincode.cpp:461-764) and the output writers.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -11,8 +12,10 @@
 #include <string>
 #include <vector>
 
+#include "cohort.h"
 #include "fast.h"
 #include "fp32.h"
+#include "multi.h"
 #include "irbc.h"
 #include "sim.h"
 
@@ -32,7 +35,7 @@ struct irbc_handle {
   cudaStream_t st = nullptr;   // solvent kernels; every public call orders on it
   cudaStream_t st2 = nullptr;  // membrane kernels, run beside the solvent ones (== st with one stream)
   cudaStream_t st2_own = nullptr;  // the side stream this handle created
-  int mem_mode = 1;                // membrane step: 1 wide kernels, 2 one block
+  int mem_mode = 1;                // membrane step: 1 wide kernels, 2 one block, 3 one cluster
   FastBufs fb;
   bool fp32 = false;           // solvent held in sf (float4) between exchanges
   SolventF sf;
@@ -60,6 +63,11 @@ struct irbc_handle {
   double report[9] = {0};
   std::vector<double> xlig, ylig;
   double* obs = nullptr;  // device scratch for observables
+  // run-time health word (DevParams::health) and its page-locked host
+  // mirror, copied after every irbc_step call (ev_health marks the copy)
+  int* health = nullptr;
+  int* health_host = nullptr;
+  cudaEvent_t ev_health = nullptr;
   int64_t launches0 = 0;
   // CUDA-event profiling window
   bool prof = false;
@@ -376,10 +384,26 @@ int upload_mesh(irbc_handle* h, const HostMesh& M) {
   h->dp.sth0 = sin(M.theta0 * h->P.Pi / 180.0);
   h->have_mesh = true;
   h->fb.one_block = h->mem_mode == 2 && one_block_fits(h->dp);
+  h->fb.cluster = h->mem_mode == 3;
   return 0;
 }
 
 int64_t launches_in(const irbc_handle* h) { return g_launches.load() - h->launches0; }
+
+// the status for a health word: 0, or IRBC_ERR_HEALTH with the message
+int health_status(irbc_handle* h, int flags) {
+  if (!flags) return 0;
+  std::string m = "health check:";
+  if (flags & HEALTH_SOLVENT) m += " a solvent particle became non-finite or left the box;";
+  if (flags & HEALTH_MEMBRANE) m += " a membrane vertex became non-finite;";
+  return fail(h, IRBC_ERR_HEALTH, m);
+}
+
+// a fresh state: clears the health word and its host mirror
+cudaError_t clear_health(irbc_handle* h) {
+  *h->health_host = 0;
+  return cudaMemsetAsync(h->health, 0, sizeof(int), h->st);
+}
 
 // epoch base for the launches that follow on the main stream (the side
 // stream joins after it through the usual events)
@@ -525,7 +549,8 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
       return IRBC_ERR_CUDA;
     }
     h->st2_own = h->st2;
-    for (cudaEvent_t* e : {&h->ev_snap, &h->ev_mem, &h->ev_coll, &h->ev_str[0], &h->ev_str[1], &h->ev_vbin})
+    for (cudaEvent_t* e : {&h->ev_snap, &h->ev_mem, &h->ev_coll, &h->ev_str[0], &h->ev_str[1], &h->ev_vbin,
+                           &h->ev_health})
       cudaEventCreateWithFlags(e, cudaEventDisableTiming);
   }
   fill_devparams(h);
@@ -558,7 +583,10 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   A(dalloc(&h->m.sc, 1));
   A(dalloc(&h->ebase, 1));
   h->dp.ebase = h->ebase;
-  A(dalloc(&h->obs, 64 + 4096));
+  A(dalloc(&h->obs, kObsDoubles));
+  A(dalloc(&h->health, 1));
+  h->dp.health = h->health;
+  A(cudaHostAlloc((void**)&h->health_host, sizeof(int), cudaHostAllocDefault));
   A(dalloc(&h->fb.queue, s.n));
   A(dalloc(&h->fb.qn, 4));
   if (p->precision == IRBC_FP32) {
@@ -573,6 +601,8 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   cudaMemsetAsync(h->m.ligi, 0, sizeof(int) * h->dp.nlig, h->st);
   cudaMemsetAsync(h->m.sc, 0, sizeof(MemScalars), h->st);
   cudaMemsetAsync(h->ebase, 0, sizeof(uint64_t), h->st);
+  cudaMemsetAsync(h->health, 0, sizeof(int), h->st);
+  *h->health_host = 0;
   cudaMemsetAsync(s.pid, 0, sizeof(int) * std::max<int64_t>(1, s.n), h->st);
   cudaMemcpyAsync(h->m.xlig, h->xlig.data(), sizeof(double) * h->dp.nlig, cudaMemcpyHostToDevice, h->st);
   cudaMemcpyAsync(h->m.ylig, h->ylig.data(), sizeof(double) * h->dp.nlig, cudaMemcpyHostToDevice, h->st);
@@ -594,8 +624,10 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   if (h->rec) cudaFree(h->rec);
   for (float4** q : {&h->sf.pos, &h->sf.vel, &h->sf.pos2, &h->sf.vel2}) dfree(*q);
   dfree(h->sf.pid); dfree(h->sf.pid2);
-  for (cudaEvent_t e : {h->ev_snap, h->ev_mem, h->ev_coll, h->ev_str[0], h->ev_str[1], h->ev_vbin})
+  for (cudaEvent_t e : {h->ev_snap, h->ev_mem, h->ev_coll, h->ev_str[0], h->ev_str[1], h->ev_vbin, h->ev_health})
     if (e) cudaEventDestroy(e);
+  dfree(h->health);
+  if (h->health_host) cudaFreeHost(h->health_host);
   if (h->st2_own) cudaStreamDestroy(h->st2_own);
   Solvent& s = h->s;
   Cells& c = h->c;
@@ -620,11 +652,26 @@ extern "C" const char* irbc_last_error(const irbc_handle* h) { return h ? h->err
 extern "C" int64_t irbc_ncell(const irbc_handle* h) { return h ? h->dp.ncell : -1; }
 extern "C" int32_t irbc_nlig(const irbc_handle* h) { return h ? h->dp.nlig : -1; }
 extern "C" int64_t irbc_launch_count(const irbc_handle* h) { return h ? launches_in(h) : -1; }
+// the health word after everything queued so far; IRBC_ERR_HEALTH when set
+static int check_health(irbc_handle* h) {
+  CK(cudaMemcpyAsync(h->health_host, h->health, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return health_status(h, *h->health_host);
+}
+
 extern "C" int irbc_sync(irbc_handle* h) {
   if (!h) return IRBC_ERR_ARG;
   cudaSetDevice(h->P.device);
   CK(cudaStreamSynchronize(h->st));
-  return 0;
+  return check_health(h);
+}
+
+extern "C" int irbc_health(irbc_handle* h, int32_t* flags) {
+  if (!h) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
+  const int rc = check_health(h);
+  if (flags) *flags = *h->health_host;
+  return rc == IRBC_ERR_HEALTH ? 0 : rc;
 }
 
 // ---- llist -----------------------------------------------------------------
@@ -907,16 +954,16 @@ extern "C" int irbc_set_state(irbc_handle* h, const irbc_view* v) {
   Membrane& m = h->m;
   const int64_t n = s.n;
   if (v->sx) {
-    std::vector<int> id(n);
-    for (int64_t i = 0; i < n; ++i) id[i] = (int)i;
-    // velocities and indices go through the free second position set and
-    // key into the velocity records
+    // velocities go through the free second position set into the velocity
+    // records, with the reference index (the array position) made on the
+    // device
     if (up(h, s.x, v->sx, n) || up(h, s.y, v->sy, n) || up(h, s.z, v->sz, n) || up(h, s.x2, v->svx, n) ||
         up(h, s.y2, v->svy, n) || up(h, s.z2, v->svz, n) || up(h, s.pid, v->spid, n) ||
-        up(h, s.indio, v->sindio, n) || up(h, s.key, id))
+        up(h, s.indio, v->sindio, n))
       return IRBC_ERR_CUDA;
+    launch_iota(s.key, n, h->st);
     launch_pack_vel(s, s.x2, s.y2, s.z2, s.key, h->st);
-    g_launches += 1;
+    g_launches += 2;
     if (h->fp32) f32_from_f64(h->s, h->sf, h->st);
     CK(cudaStreamSynchronize(h->st));
   }
@@ -939,22 +986,27 @@ extern "C" int irbc_set_state(irbc_handle* h, const irbc_view* v) {
   if (v->ligi && up(h, m.ligi, v->ligi, h->dp.nlig)) return IRBC_ERR_CUDA;
   if (v->llen) {
     Cells& c = h->c;
-    std::vector<int> start(c.n + 1, 0);
     int64_t tot = 0;
-    for (int64_t i = 0; i < c.n; ++i) { start[i] = (int)tot; tot += v->llen[i]; }
-    start[c.n] = (int)tot;
+    for (int64_t i = 0; i < c.n; ++i) tot += v->llen[i];
+    if (tot >= (1LL << 31)) return fail(h, IRBC_ERR_ARG, "list entries exceed the int range");
     if (tot > c.lcap) {
+      CK(cudaStreamSynchronize(h->st));
       invalidate_graphs(h);
       dfree(c.lidx);
       c.lcap = tot + 1024;
       CK(dalloc(&c.lidx, c.lcap));
     }
-    if (up(h, c.lstart, start) || up(h, c.lidx, v->lidx, tot)) return IRBC_ERR_CUDA;
+    // list starts: the lengths scanned on the device
+    if (up(h, c.lcnt, v->llen, c.n) || up(h, c.lidx, v->lidx, tot)) return IRBC_ERR_CUDA;
+    launch_scan3(c.lcnt, nullptr, nullptr, c.lstart, nullptr, nullptr, c.totals + 8, c.n, c.scan_part, h->st);
+    CK(cudaMemcpyAsync(c.lstart + c.n, c.totals + 8, sizeof(int), cudaMemcpyDeviceToDevice, h->st));
+    g_launches += 3;
     int rc = refresh_listed(h);
     if (rc) return rc;
   }
   h->dp.wallspeed = v->wallspeed;
   h->step = v->step; h->colsteps = v->colsteps; h->upd = v->upd; h->filecc = v->filecc; h->filec = v->filec;
+  CK(clear_health(h));
   CK(cudaStreamSynchronize(h->st));
   return 0;
 }
@@ -1316,6 +1368,9 @@ extern "C" int irbc_step(irbc_handle* h, int64_t n) {
   if (!h || n < 0) return IRBC_ERR_ARG;
   if (!h->have_mesh) return fail(h, IRBC_ERR_STATE, "no mesh");
   cudaSetDevice(h->P.device);
+  // the health word as of the end of an earlier call, without waiting: a
+  // simulation found unhealthy is not stepped further
+  if (cudaEventQuery(h->ev_health) == cudaSuccess && *h->health_host) return health_status(h, *h->health_host);
   cudaStream_t ms = h->st, ss = h->st2;
   // epochs: base h->step; the side stream starts after everything already
   // queued on the main one
@@ -1347,6 +1402,8 @@ extern "C" int irbc_step(irbc_handle* h, int64_t n) {
     k += 1;
   }
   CK(cudaStreamWaitEvent(ms, h->ev_mem, 0));
+  CK(cudaMemcpyAsync(h->health_host, h->health, sizeof(int), cudaMemcpyDeviceToHost, ms));
+  CK(cudaEventRecord(h->ev_health, ms));
   CK(cudaGetLastError());
   return 0;
 }
@@ -1365,16 +1422,17 @@ extern "C" int irbc_set_streams(irbc_handle* h, int32_t n) {
 }
 
 extern "C" int irbc_set_membrane_kernels(irbc_handle* h, int32_t mode) {
-  if (!h || mode < 1 || mode > 2) return IRBC_ERR_ARG;
+  if (!h || mode < 1 || mode > 3) return IRBC_ERR_ARG;
   cudaSetDevice(h->P.device);
   CK(cudaStreamSynchronize(h->st));
   CK(cudaStreamSynchronize(h->st2_own));
   h->mem_mode = mode;
   if (h->have_mesh) {
-    const bool ob = mode == 2;
+    const bool ob = mode == 2, cl = mode == 3;
     if (ob && !one_block_fits(h->dp)) return fail(h, IRBC_ERR_CAPACITY, "mesh too large for the one-block membrane step");
-    if (ob != h->fb.one_block) invalidate_graphs(h);
+    if (ob != h->fb.one_block || cl != h->fb.cluster) invalidate_graphs(h);
     h->fb.one_block = ob;
+    h->fb.cluster = cl;
   }
   return 0;
 }
@@ -1385,6 +1443,277 @@ extern "C" int irbc_set_graphs(irbc_handle* h, int32_t on) {
   if (!h->graphs_on) invalidate_graphs(h);
   return 0;
 }
+
+// ---- cohorts: one launch per phase over many simulations (cohort.h) -----------
+namespace irbc {
+
+struct Cohort {
+  int device = 0;
+  cudaStream_t ms = nullptr, ss = nullptr;  // solvent phases / membrane phases, as a handle's two streams
+  cudaEvent_t ev_snap = nullptr, ev_mem = nullptr, ev_coll = nullptr, ev_str[2] = {nullptr, nullptr};
+  cudaEvent_t ev_join = nullptr;
+  MultiPlan plan;                       // device tables of `members`
+  std::vector<irbc_handle*> members;    // the plan's members, in order
+  std::vector<Member> host;             // their descriptors as uploaded
+  size_t cap = 0;                       // members the device tables have room for
+  size_t tab_cap = 0;                   // block-table entries they have room for
+  int64_t ncoll = 0;                    // collisions of this cohort: a physical re-sort every kResortEvery
+  bool ok = false;
+};
+
+Cohort* cohort_create(int device) {
+  Cohort* c = new Cohort();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) return c;
+  int lo = 0, hi = 0;
+  cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  bool ok = cudaStreamCreateWithFlags(&c->ms, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithPriority(&c->ss, cudaStreamNonBlocking, hi) == cudaSuccess;
+  for (cudaEvent_t* e : {&c->ev_snap, &c->ev_mem, &c->ev_coll, &c->ev_str[0], &c->ev_str[1], &c->ev_join})
+    ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+  c->ok = ok;
+  return c;
+}
+
+void cohort_destroy(Cohort* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->ms) cudaStreamSynchronize(c->ms);
+  if (c->ss) cudaStreamSynchronize(c->ss);
+  for (cudaEvent_t e : {c->ev_snap, c->ev_mem, c->ev_coll, c->ev_str[0], c->ev_str[1], c->ev_join})
+    if (e) cudaEventDestroy(e);
+  if (c->ms) cudaStreamDestroy(c->ms);
+  if (c->ss) cudaStreamDestroy(c->ss);
+  if (c->plan.mem) cudaFree(c->plan.mem);
+  if (c->plan.blk) cudaFree(c->plan.blk);
+  delete c;
+}
+
+int64_t cohort_key(const irbc_handle* h) {
+  if (!h || !h->fp32 || !h->have_mesh || h->capturing) return -1;
+  int64_t k = h->P.device;
+  k = k * 4096 + h->csteps;
+  k = k * 4096 + (h->colsteps + 1);
+  k = k * 2 + (h->step & 1);
+  k = k * 2 + (h->snap_ready ? 1 : 0);
+  return k;
+}
+
+static Member member_of(irbc_handle* h) {
+  Member M;
+  M.p = h->dp;
+  M.s = h->s;
+  M.f = h->sf;
+  M.c = h->c;
+  M.m = h->m;
+  M.fb = h->fb;
+  // the staging capacity follows the longest list (as stream_any does for
+  // plain launches)
+  M.fb.hcap = heavy_cap(h->c.lmax);
+  return M;
+}
+
+// (Re)builds and uploads the device tables of the current members; both
+// streams are idle when it returns, so no kernel reads the old tables
+static int cohort_upload(Cohort* c) {
+  if (cudaStreamSynchronize(c->ms) != cudaSuccess || cudaStreamSynchronize(c->ss) != cudaSuccess)
+    return IRBC_ERR_CUDA;
+  const size_t n = c->members.size();
+  MultiPlan& P = c->plan;
+  P.n = (int)n;
+  c->host.resize(n);
+  std::vector<std::array<int, MP_NPHASE>> nbk(n);
+  int64_t tot[MP_NPHASE] = {};
+  P.cells_smem = P.vbin_smem = P.sum_smem = 0;
+  for (size_t r = 0; r < n; ++r) {
+    c->host[r] = member_of(c->members[r]);
+    int sm[3];
+    multi_blocks(c->host[r], nbk[r].data());
+    multi_smem(c->host[r], sm);
+    for (int k = 0; k < MP_NPHASE; ++k) tot[k] += nbk[r][k];
+    P.cells_smem = std::max(P.cells_smem, sm[0]);
+    P.vbin_smem = std::max(P.vbin_smem, sm[1]);
+    P.sum_smem = std::max(P.sum_smem, sm[2]);
+  }
+  // the block tables: phase by phase, member by member
+  int64_t all = 0;
+  for (int k = 0; k < MP_NPHASE; ++k) {
+    if (tot[k] >= (1LL << 31)) return IRBC_ERR_CAPACITY;
+    P.off[k] = all;
+    P.blocks[k] = (int)tot[k];
+    all += tot[k];
+  }
+  std::vector<int2> tab((size_t)all);
+  for (int k = 0; k < MP_NPHASE; ++k) {
+    int64_t q = P.off[k];
+    for (size_t r = 0; r < n; ++r)
+      for (int b = 0; b < nbk[r][k]; ++b) tab[(size_t)q++] = make_int2((int)r, b);
+  }
+  if (n > c->cap || (size_t)all > c->tab_cap) {
+    if (P.mem) cudaFree(P.mem);
+    if (P.blk) cudaFree(P.blk);
+    P.mem = nullptr;
+    P.blk = nullptr;
+    c->cap = n + n / 2 + 8;
+    c->tab_cap = (size_t)all + (size_t)all / 2 + 1024;
+    if (cudaMalloc((void**)&P.mem, c->cap * sizeof(Member)) != cudaSuccess ||
+        cudaMalloc((void**)&P.blk, c->tab_cap * sizeof(int2)) != cudaSuccess)
+      return IRBC_ERR_CUDA;
+  }
+  // staging memory: plain (pageable) copies, finished when the calls return
+  if (cudaMemcpy(P.mem, c->host.data(), n * sizeof(Member), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(P.blk, tab.data(), tab.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess)
+    return IRBC_ERR_CUDA;
+  return 0;
+}
+
+// whether the uploaded descriptor of member r still describes its handle:
+// the fields that calls between steps can move (list updates and state
+// loads grow the lists and buckets, a new mesh moves the membrane arrays)
+// and the wall speed
+static bool member_current(const Cohort* c, size_t r) {
+  const Member now = member_of(c->members[r]);
+  const Member& was = c->host[r];
+  return now.p.wallspeed == was.p.wallspeed && now.fb.hcap == was.fb.hcap && now.fb.bcap == was.fb.bcap &&
+         now.c.lidx == was.c.lidx && now.c.lstart == was.c.lstart && now.fb.bcnt == was.fb.bcnt &&
+         now.fb.bucket == was.fb.bucket && now.fb.border == was.fb.border && now.m.x == was.m.x &&
+         now.m.sc == was.m.sc && now.fb.slot == was.fb.slot && now.fb.pre[0] == was.fb.pre[0] &&
+         now.f.pos == was.f.pos && now.p.nv == was.p.nv && now.p.Sarea0 == was.p.Sarea0;
+}
+
+int cohort_step(Cohort* c, const std::vector<irbc_handle*>& all, int64_t n, std::vector<int>& status) {
+  status.assign(all.size(), 0);
+  if (!c || !c->ok || n < 0) return IRBC_ERR_ARG;
+  if (all.empty() || n == 0) return 0;
+  cudaSetDevice(c->device);
+  // members already found unhealthy are not stepped (as irbc_step)
+  std::vector<irbc_handle*> hs;
+  for (size_t i = 0; i < all.size(); ++i) {
+    irbc_handle* h = all[i];
+    if (cudaEventQuery(h->ev_health) == cudaSuccess && *h->health_host) status[i] = health_status(h, *h->health_host);
+    else hs.push_back(h);
+  }
+  if (hs.empty()) return 0;
+  const int64_t key = cohort_key(hs[0]);
+  for (irbc_handle* h : hs)
+    if (key < 0 || cohort_key(h) != key || h->P.device != c->device) return IRBC_ERR_ARG;
+  cudaStream_t ms = c->ms, ss = c->ss;
+  int64_t launched = 0;
+  // the cohort's work follows each member's earlier work; the epochs of
+  // this call are each member's step count plus the step's offset
+  for (irbc_handle* h : hs) {
+    if (cudaEventRecord(c->ev_join, h->st) != cudaSuccess || cudaStreamWaitEvent(ms, c->ev_join, 0) != cudaSuccess)
+      return IRBC_ERR_CUDA;
+    h->ebase_val = h->step;
+    launch_set_u64(h->ebase, (uint64_t)h->step, ms);
+    if (cudaMemsetAsync(h->fb.qn, 0, 2 * sizeof(int), ms) != cudaSuccess) return IRBC_ERR_CUDA;
+    launched += 1;
+  }
+  if (cudaEventRecord(c->ev_coll, ms) != cudaSuccess || cudaStreamWaitEvent(ss, c->ev_coll, 0) != cudaSuccess)
+    return IRBC_ERR_CUDA;
+  // the device tables: rebuilt when the members changed or a member's
+  // buffers, capacities or wall speed moved
+  bool stale = hs != c->members;
+  for (size_t r = 0; !stale && r < hs.size(); ++r) stale = !member_current(c, r);
+  if (stale) {
+    c->members = hs;
+    int rc = cohort_upload(c);
+    if (rc) return rc;
+  }
+  irbc_handle* h0 = hs[0];
+  const int csteps = h0->csteps;
+  for (int64_t k = 0; k < n; ++k) {
+    const int buf = (int)(h0->step & 1);
+    bool moved = false;
+    for (irbc_handle* h : hs) {
+      const irbc_params& p = h->P;
+      const double ws = (h->step < p.warm_steps) ? p.warm_speed : p.walls;
+      if (ws != h->dp.wallspeed) { h->dp.wallspeed = ws; moved = true; }
+      h->colsteps += 1; h->bbi += 1; h->upd += 1;
+      if (h->step > 0) h->filecc += 1;
+    }
+    if (moved) {
+      int rc = cohort_upload(c);
+      if (rc) return rc;
+    }
+    const bool collide = h0->colsteps == csteps;
+    if (collide) {
+      c->ncoll += 1;
+      const bool resort = c->ncoll % kResortEvery == 0;
+      for (irbc_handle* h : hs) {
+        h->s.ncoll += 1;
+        if (resort) h->s.resorted = h->s.ncoll;
+        h->colsteps = 0;
+        h->snap_ready = false;
+      }
+      launched += multi_collide_front(c->plan, (uint64_t)k, ms);
+      launched += multi_collide_count(c->plan, (uint64_t)k, ms);
+      launched += multi_collide_scan(c->plan, ms);
+      launched += multi_collide_back(c->plan, (uint64_t)k, resort, ms);
+      if (cudaEventRecord(c->ev_coll, ms) != cudaSuccess || cudaStreamWaitEvent(ss, c->ev_coll, 0) != cudaSuccess)
+        return IRBC_ERR_CUDA;
+    }
+    if (!h0->snap_ready) {
+      if (cudaStreamWaitEvent(ss, c->ev_str[buf], 0) != cudaSuccess) return IRBC_ERR_CUDA;
+      launched += multi_kick(c->plan, buf, ss);
+    }
+    // list updates (rare, per member, with host waits): positions of this
+    // step are final once the side stream reaches here
+    bool listed = false;
+    for (irbc_handle* h : hs) {
+      if (h->upd != h->uplist) continue;
+      if (!listed) {
+        if (cudaEventRecord(c->ev_snap, ss) != cudaSuccess || cudaStreamWaitEvent(ms, c->ev_snap, 0) != cudaSuccess)
+          return IRBC_ERR_CUDA;
+        listed = true;
+      }
+      if (cudaEventRecord(c->ev_join, ms) != cudaSuccess || cudaStreamWaitEvent(h->st, c->ev_join, 0) != cudaSuccess)
+        return IRBC_ERR_CUDA;
+      int rc = do_llist(h);
+      if (rc) return rc;
+      h->upd = 0;
+      if (cudaEventRecord(c->ev_join, h->st) != cudaSuccess || cudaStreamWaitEvent(ms, c->ev_join, 0) != cudaSuccess)
+        return IRBC_ERR_CUDA;
+    }
+    if (listed) {
+      int rc = cohort_upload(c);  // lists, buckets and staging may have moved or grown
+      if (rc) return rc;
+    }
+    const bool next_collides = h0->colsteps + 1 == csteps;
+    const bool next_kick = k != n - 1 && !next_collides;
+    // as step_one: the bulk streaming starts at once, the near-membrane
+    // kernel waits for the snapshot, the membrane step runs beside them and
+    // writes the next snapshot only after the streaming that read it
+    if (cudaEventRecord(c->ev_snap, ss) != cudaSuccess) return IRBC_ERR_CUDA;
+    launched += multi_stream(c->plan, buf, ms, c->ev_snap);
+    if (cudaEventRecord(c->ev_str[buf], ms) != cudaSuccess) return IRBC_ERR_CUDA;
+    launched += multi_membrane(c->plan, (uint64_t)k, ss);
+    if (next_kick) {
+      if (cudaStreamWaitEvent(ss, c->ev_str[buf ^ 1], 0) != cudaSuccess) return IRBC_ERR_CUDA;
+      launched += multi_kick(c->plan, buf ^ 1, ss);
+    }
+    if (cudaEventRecord(c->ev_mem, ss) != cudaSuccess) return IRBC_ERR_CUDA;
+    for (irbc_handle* h : hs) {
+      h->snap_ready = next_kick;
+      if (h->filecc == h->P.out_every) { h->filec += 1; h->filecc = 0; }
+      h->step += 1;
+    }
+  }
+  // each member's own stream follows the cohort's work; its health word
+  // is copied for the next irbc_step (as at the end of irbc_step)
+  if (cudaStreamWaitEvent(ms, c->ev_mem, 0) != cudaSuccess || cudaEventRecord(c->ev_join, ms) != cudaSuccess)
+    return IRBC_ERR_CUDA;
+  for (irbc_handle* h : hs) {
+    if (cudaStreamWaitEvent(h->st, c->ev_join, 0) != cudaSuccess ||
+        cudaMemcpyAsync(h->health_host, h->health, sizeof(int), cudaMemcpyDeviceToHost, h->st) != cudaSuccess ||
+        cudaEventRecord(h->ev_health, h->st) != cudaSuccess)
+      return IRBC_ERR_CUDA;
+  }
+  g_launches += launched;
+  return cudaGetLastError() == cudaSuccess ? 0 : IRBC_ERR_CUDA;
+}
+
+}  // namespace irbc
 
 // ---- output ----------------------------------------------------------------------
 namespace {
@@ -1485,7 +1814,7 @@ extern "C" int irbc_write_stl(irbc_handle* h, const char* path) {
 extern "C" int irbc_observables(irbc_handle* h, double* out, int32_t nout) {
   if (!h || !out || nout <= 0) return IRBC_ERR_ARG;
   if (h->fp32) f32_to_f64(h->sf, h->s, h->st);
-  launch_observables(h->dp, h->s, h->m, h->obs, nullptr, 0, h->st);
+  launch_observables(h->dp, h->s, h->m, h->obs, 0, h->st);
   g_launches += 2;
   double buf[16] = {0};
   CK(cudaMemcpyAsync(buf, h->obs, sizeof(double) * 16, cudaMemcpyDeviceToHost, h->st));
@@ -1495,10 +1824,10 @@ extern "C" int irbc_observables(irbc_handle* h, double* out, int32_t nout) {
 }
 
 extern "C" int irbc_velocity_profile(irbc_handle* h, double* out, int32_t nbins) {
-  if (!h || !out || nbins <= 0 || nbins > 2048) return IRBC_ERR_ARG;
+  if (!h || !out || nbins <= 0 || nbins > kObsMaxBins) return IRBC_ERR_ARG;
   if (h->fp32) f32_to_f64(h->sf, h->s, h->st);
-  launch_observables(h->dp, h->s, h->m, h->obs, h->obs + 64, nbins, h->st);
-  g_launches += 3;
+  launch_observables(h->dp, h->s, h->m, h->obs, nbins, h->st);
+  g_launches += 2;
   std::vector<double> buf(2 * nbins);
   CK(cudaMemcpyAsync(buf.data(), h->obs + 64, sizeof(double) * 2 * nbins, cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));

@@ -11,6 +11,7 @@
 // is stepped exactly as it would be alone.
 #include <algorithm>
 #include <chrono>
+#include <map>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -18,6 +19,7 @@
 #include <thread>
 #include <vector>
 #include <cuda_runtime.h>
+#include "cohort.h"
 #include "irbc.h"
 
 namespace {
@@ -37,20 +39,27 @@ class StepPool {
     for (auto& th : threads_) th.join();
   }
   // advances members[i] by steps[i] (interleaved in chunks of `chunk`) and
-  // waits for their device work; returns the first error, 0 if none
-  int step(const std::vector<irbc_handle*>& members, const std::vector<int64_t>& steps, int64_t chunk) {
+  // waits for their device work.  status[i] receives member i's own result:
+  // 0, or the error of its irbc_step or irbc_sync (a member that fails stops
+  // stepping there; the others go on).  Returns the first error, 0 if none.
+  int step(const std::vector<irbc_handle*>& members, const std::vector<int64_t>& steps, int64_t chunk,
+           std::vector<int>* status = nullptr) {
     std::unique_lock<std::mutex> lk(mu_);
     members_ = &members;
     steps_ = &steps;
+    status_.assign(members.size(), 0);
     chunk_ = std::max<int64_t>(1, chunk);
-    first_error_ = 0;
     pending_ = n_;
     ++job_;
     cv_.notify_all();
     done_.wait(lk, [this] { return pending_ == 0; });
     members_ = nullptr;
     steps_ = nullptr;
-    return first_error_;
+    int first = 0;
+    for (int e : status_)
+      if (e && !first) first = e;
+    if (status) *status = status_;
+    return first;
   }
 
  private:
@@ -59,6 +68,7 @@ class StepPool {
     for (;;) {
       std::vector<irbc_handle*> mine;
       std::vector<int64_t> todo;
+      std::vector<size_t> where;
       int64_t chunk;
       {
         std::unique_lock<std::mutex> lk(mu_);
@@ -69,26 +79,27 @@ class StepPool {
         for (size_t i = t; i < members_->size(); i += n_) {
           mine.push_back((*members_)[i]);
           todo.push_back((*steps_)[i]);
+          where.push_back(i);
         }
       }
-      int err = 0;
-      for (int64_t k = 0; !err; k += chunk) {
+      std::vector<int> err(mine.size(), 0);
+      for (int64_t k = 0;; k += chunk) {
         bool any = false;
-        for (size_t i = 0; i < mine.size() && !err; ++i) {
+        for (size_t i = 0; i < mine.size(); ++i) {
           const int64_t m = std::min(chunk, todo[i] - k);
-          if (m <= 0) continue;
+          if (m <= 0 || err[i]) continue;
           any = true;
-          err = irbc_step(mine[i], m);
+          err[i] = irbc_step(mine[i], m);
         }
         if (!any) break;
       }
-      for (irbc_handle* h : mine) {
-        const int e = irbc_sync(h);
-        if (!err) err = e;
+      for (size_t i = 0; i < mine.size(); ++i) {
+        const int e = irbc_sync(mine[i]);
+        if (!err[i]) err[i] = e;
       }
       {
         std::lock_guard<std::mutex> lk(mu_);
-        if (err && !first_error_) first_error_ = err;
+        for (size_t i = 0; i < mine.size(); ++i) status_[where[i]] = err[i];
         if (--pending_ == 0) done_.notify_all();
       }
     }
@@ -101,13 +112,62 @@ class StepPool {
   const std::vector<irbc_handle*>* members_ = nullptr;
   const std::vector<int64_t>* steps_ = nullptr;
   int64_t chunk_ = 24;
+  std::vector<int> status_;
   uint64_t job_ = 0;
-  int pending_ = 0, first_error_ = 0;
+  int pending_ = 0;
   bool stop_ = false;
 };
 
 double now_s(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Advances members[i] by steps[i] and waits for their device work;
+// status[i] receives member i's own result.  Under a fused schedule, the
+// members that can share a cohort (FP32, same phase, same step count: equal
+// irbc::cohort_key) go through one launch per phase, a cohort per group;
+// the others through the pool of host threads, whose work overlaps the
+// cohorts' on the GPU.  Returns the first error, 0 if none.
+int step_members(StepPool& pool, std::vector<irbc::Cohort*>& cohorts, const std::vector<irbc_handle*>& members,
+                 const std::vector<int64_t>& steps, const irbc_schedule& sched, std::vector<int>& status) {
+  status.assign(members.size(), 0);
+  if (!sched.fused) return pool.step(members, steps, sched.chunk, &status);
+  std::map<std::pair<int64_t, int64_t>, std::vector<size_t>> groups;
+  std::vector<size_t> rest;
+  for (size_t i = 0; i < members.size(); ++i) {
+    const int64_t k = irbc::cohort_key(members[i]);
+    if (k < 0 || steps[i] <= 0) rest.push_back(i);
+    else groups[{k, steps[i]}].push_back(i);
+  }
+  size_t g = 0;
+  for (auto& kv : groups) {
+    if (cohorts.size() <= g) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cohorts.push_back(irbc::cohort_create(dev));
+    }
+    std::vector<irbc_handle*> hs;
+    for (size_t i : kv.second) hs.push_back(members[i]);
+    std::vector<int> st;
+    const int rc = irbc::cohort_step(cohorts[g], hs, kv.first.second, st);
+    for (size_t j = 0; j < kv.second.size(); ++j) status[kv.second[j]] = rc ? rc : st[j];
+    ++g;
+  }
+  if (!rest.empty()) {
+    std::vector<irbc_handle*> hs;
+    std::vector<int64_t> ns;
+    for (size_t i : rest) { hs.push_back(members[i]); ns.push_back(steps[i]); }
+    std::vector<int> st;
+    pool.step(hs, ns, sched.chunk, &st);
+    for (size_t j = 0; j < rest.size(); ++j) status[rest[j]] = st[j];
+  }
+  // the cohorts' device work (and each member's health word)
+  for (auto& kv : groups)
+    for (size_t i : kv.second)
+      if (!status[i]) status[i] = irbc_sync(members[i]);
+  for (int e : status)
+    if (e) return e;
+  return 0;
 }
 
 }  // namespace
@@ -116,15 +176,20 @@ double now_s(std::chrono::steady_clock::time_point t0) {
 struct irbc_batch {
   std::vector<irbc_handle*> members;
   StepPool pool;
-  irbc_schedule sched{2, 1, 0, 24};  // the handles' defaults and the pool's chunk
-  bool scheduled = false;             // set explicitly: members added later get it too
+  std::vector<irbc::Cohort*> cohorts;    // fused schedules: one per group of members
+  irbc_schedule sched{2, 1, 0, 24, 1};  // the handles' defaults, the pool's chunk, fused
+  bool scheduled = false;               // set explicitly: members added later get it too
   explicit irbc_batch(int nthreads) : pool(nthreads) {}
+  ~irbc_batch() {
+    for (irbc::Cohort* c : cohorts) irbc::cohort_destroy(c);
+  }
 };
 
 namespace {
 bool valid_schedule(const irbc_schedule& s) {
   return (s.streams == 1 || s.streams == 2) && (s.membrane == 1 || s.membrane == 2) &&
-         (s.graphs == 0 || s.graphs == 1) && s.chunk >= 24 && s.chunk <= 2400 && s.chunk % 24 == 0;
+         (s.graphs == 0 || s.graphs == 1) && s.chunk >= 24 && s.chunk <= 2400 && s.chunk % 24 == 0 &&
+         (s.fused == 0 || s.fused == 1);
 }
 
 int apply_schedule(irbc_handle* h, const irbc_schedule& s) {
@@ -167,7 +232,8 @@ extern "C" int32_t irbc_batch_size(const irbc_batch* b) { return b ? (int32_t)b-
 extern "C" int irbc_batch_step(irbc_batch* b, int64_t n) {
   if (!b || n < 0) return IRBC_ERR_ARG;
   std::vector<int64_t> steps(b->members.size(), n);
-  return b->pool.step(b->members, steps, b->sched.chunk);
+  std::vector<int> status;
+  return step_members(b->pool, b->cohorts, b->members, steps, b->sched, status);
 }
 
 // ---- launch schedules and the autotuner --------------------------------------
@@ -243,8 +309,9 @@ int measure_schedule(int32_t i, void* ctx, double* seconds) {
   const int rc = irbc_batch_set_schedule(b, &s);
   if (rc) return rc;
   std::vector<int64_t> steps(b->members.size(), run->trial);
+  std::vector<int> status;
   const auto t0 = std::chrono::steady_clock::now();
-  const int e = b->pool.step(b->members, steps, s.chunk);
+  const int e = step_members(b->pool, b->cohorts, b->members, steps, s, status);
   *seconds = now_s(t0);
   if (!e) run->taken += run->trial;
   return e;
@@ -262,10 +329,13 @@ extern "C" int irbc_batch_autotune(irbc_batch* b, int64_t trial_steps, int32_t r
   irbc_schedule cur = b->sched;
   static const int32_t kChunks[] = {24, 96, 240};
   int rc = 0;
-  for (int field = 0; field < 4 && !rc; ++field) {
+  for (int field = -1; field < 4 && !rc; ++field) {
     run.cands.assign(1, cur);
     irbc_schedule alt = cur;
-    if (field == 0) {
+    if (field == -1) {
+      alt.fused = 1 - cur.fused;
+      run.cands.push_back(alt);
+    } else if (field == 0) {
       alt.membrane = 3 - cur.membrane;
       run.cands.push_back(alt);
     } else if (field == 1) {
@@ -317,15 +387,20 @@ struct irbc_server {
   int64_t budget = 0, used = 0;
   int64_t round = 240;
   int32_t max_active = 256;
-  irbc_schedule sched{2, 1, 0, 24};  // for simulations admitted from now on
-  bool scheduled = false;             // set explicitly: applied at admission
+  irbc_schedule sched{2, 1, 0, 24, 1};  // for simulations admitted from now on
+  bool scheduled = false;                // set explicitly: applied at admission
   StepPool pool;
+  std::vector<irbc::Cohort*> cohorts;    // fused schedules: one per group of simulations
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   std::mutex mu;
   std::condition_variable cv;
   std::deque<Request> pending;
   std::vector<Active> active;
   std::deque<irbc_result> results;
+  // finished simulations handed out with keep = 1: their memory stays
+  // charged to the budget until irbc_server_release
+  std::vector<std::pair<irbc_handle*, int64_t>> kept;
+  int64_t n_active = 0;  // active.size(), readable under mu while the loop runs
   int64_t next_id = 1;
   int64_t particle_steps = 0;
   bool stop = false;
@@ -361,13 +436,15 @@ bool serve_round(irbc_server* s) {
     res.t_start = t_start;
     res.t_end = now_s(s->t0);
     if (h && status == 0) irbc_observables(h, res.obs, 8);
-    if (h && r.keep && status == 0) {
+    const bool hand_out = h && r.keep && status == 0;
+    if (hand_out) {
       res.handle = h;
     } else if (h) {
       irbc_destroy(h);
     }
     std::lock_guard<std::mutex> lk(s->mu);
-    s->used -= r.footprint;
+    if (hand_out) s->kept.push_back({h, r.footprint});
+    else s->used -= r.footprint;
     s->results.push_back(res);
     s->cv.notify_all();
   };
@@ -391,7 +468,9 @@ bool serve_round(irbc_server* s) {
     a.r = std::move(r);
     a.h = h;
     a.t_start = t_start;
+    std::lock_guard<std::mutex> lk(s->mu);
     s->active.push_back(std::move(a));
+    s->n_active = (int64_t)s->active.size();
   }
   if (s->active.empty()) return !admit.empty();
   std::vector<irbc_handle*> hs;
@@ -400,8 +479,12 @@ bool serve_round(irbc_server* s) {
     hs.push_back(a.h);
     steps.push_back(std::min(s->round, a.r.nsteps - a.done));
   }
-  const int rc = s->pool.step(hs, steps, sched.chunk);
+  // each simulation's own status: one that fails (a CUDA error, or the
+  // health check of irbc_sync) is retired with it, the others go on
+  std::vector<int> status;
+  step_members(s->pool, s->cohorts, hs, steps, sched, status);
   std::vector<Active> still;
+  std::vector<size_t> done;
   for (size_t i = 0; i < s->active.size(); ++i) {
     Active& a = s->active[i];
     a.done += steps[i];
@@ -409,11 +492,23 @@ bool serve_round(irbc_server* s) {
       std::lock_guard<std::mutex> lk(s->mu);
       s->particle_steps += steps[i] * a.r.p.Ns;
     }
-    if (rc || a.done >= a.r.nsteps) finish(a.r, a.h, rc, a.t_start);
-    else still.push_back(std::move(a));
+    if (status[i] || a.done >= a.r.nsteps) done.push_back(i);
   }
+  for (size_t i : done) finish(s->active[i].r, s->active[i].h, status[i], s->active[i].t_start);
+  for (size_t i = 0, d = 0; i < s->active.size(); ++i) {
+    if (d < done.size() && done[d] == i) { ++d; continue; }
+    still.push_back(std::move(s->active[i]));
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
   s->active = std::move(still);
+  s->n_active = (int64_t)s->active.size();
   return true;
+}
+
+// whether the loop has work: simulations to step, or a pending request
+// that fits the budget now (under s->mu)
+bool has_work(const irbc_server* s) {
+  return !s->active.empty() || (!s->pending.empty() && s->used + s->pending.front().footprint <= s->budget);
 }
 
 void serve_loop(irbc_server* s) {
@@ -421,13 +516,17 @@ void serve_loop(irbc_server* s) {
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv.wait(lk, [s] { return s->stop || !s->pending.empty() || !s->active.empty(); });
+      s->cv.wait(lk, [s] { return s->stop || has_work(s); });
       if (s->stop) break;
     }
     serve_round(s);
   }
   for (Active& a : s->active) irbc_destroy(a.h);
+  for (irbc::Cohort* c : s->cohorts) irbc::cohort_destroy(c);
+  s->cohorts.clear();
+  std::lock_guard<std::mutex> lk(s->mu);
   s->active.clear();
+  s->n_active = 0;
 }
 }  // namespace
 
@@ -490,7 +589,7 @@ extern "C" int irbc_server_status(irbc_server* s, int64_t out[6]) {
   if (!s || !out) return IRBC_ERR_ARG;
   std::lock_guard<std::mutex> lk(s->mu);
   out[0] = (int64_t)s->pending.size();
-  out[1] = (int64_t)s->active.size();
+  out[1] = s->n_active;
   out[2] = (int64_t)s->results.size();
   out[3] = s->used;
   out[4] = s->budget;
@@ -508,6 +607,24 @@ extern "C" int irbc_server_set_schedule(irbc_server* s, const irbc_schedule* sch
 
 extern "C" double irbc_server_clock(irbc_server* s) { return s ? now_s(s->t0) : 0.0; }
 
+extern "C" int irbc_server_release(irbc_server* s, irbc_handle* h) {
+  if (!s || !h) return IRBC_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = std::find_if(s->kept.begin(), s->kept.end(),
+                           [h](const std::pair<irbc_handle*, int64_t>& k) { return k.first == h; });
+    if (it == s->kept.end()) return IRBC_ERR_ARG;
+    // a result not yet polled still names the handle: it may not go
+    for (const irbc_result& r : s->results)
+      if (r.handle == h) return IRBC_ERR_STATE;
+    s->used -= it->second;
+    s->kept.erase(it);
+  }
+  irbc_destroy(h);
+  s->cv.notify_all();  // the memory may admit a pending request
+  return 0;
+}
+
 extern "C" void irbc_server_destroy(irbc_server* s) {
   if (!s) return;
   {
@@ -516,5 +633,8 @@ extern "C" void irbc_server_destroy(irbc_server* s) {
   }
   s->cv.notify_all();
   s->loop.join();
+  // handles of results never polled were never handed out
+  for (irbc_result& r : s->results)
+    if (r.handle) irbc_destroy(r.handle);
   delete s;
 }

@@ -62,7 +62,10 @@ __global__ void k_na_segsort(const int* start, int64_t ncell, int* order) {
 namespace {
 // Device address of g_bin_scratch per device ordinal.  The host symbol is a
 // stand-in and must not be handed to a kernel, so the address is looked up
-// once per device with cudaGetSymbolAddress while that device is current.
+// once per device with cudaGetSymbolAddress while that device is current,
+// and kept for the life of the process.  A cudaDeviceReset unloads the
+// module and can move the array, leaving the kept address stale: this entry
+// point must not be used on a device after it has been reset.
 std::mutex g_scratch_mu;
 int* g_scratch_dev[256] = {nullptr};
 
@@ -108,7 +111,8 @@ extern "C" int irbc_bin_particles_noalloc(const irbc_params* p, const double* x,
   if (cudaMemsetAsync(cnt, 0, sizeof(int) * d.ncell, st) != cudaSuccess) return IRBC_ERR_CUDA;
   if (n) k_na_count<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d, x, y, z, n, rx, ry, rz, cell, cnt);
   launch_scan3(cnt, nullptr, nullptr, start, nullptr, nullptr, totals, d.ncell, part, st);
-  cudaMemcpyAsync(start + d.ncell, totals, sizeof(int), cudaMemcpyDeviceToDevice, st);
+  if (cudaMemcpyAsync(start + d.ncell, totals, sizeof(int), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return IRBC_ERR_CUDA;
   if (cudaMemsetAsync(cnt, 0, sizeof(int) * d.ncell, st) != cudaSuccess) return IRBC_ERR_CUDA;
   if (n) k_na_fill<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(cell, start, n, cnt, order);
   k_na_segsort<<<(unsigned)((d.ncell + 255) / 256), 256, 0, st>>>(start, d.ncell, order);

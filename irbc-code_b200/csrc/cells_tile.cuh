@@ -284,14 +284,15 @@ __device__ void cell_from_global(const DevParams& p, Solvent& s, SolventF& f, co
   }
 }
 
+// block `bid` of the collision tiles
 template <bool F32>
-__global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Solvent s, SolventF f, Cells cl,
-                                                               Membrane m, uint64_t eoff) {
+__device__ __forceinline__ void cells_tile_block(const DevParams& p, Solvent& s, SolventF& f, const Cells& cl,
+                                                 const Membrane& m, uint64_t eoff, int64_t bid) {
   const uint64_t epoch = epoch_of(p, eoff);
   __shared__ CellTile tiles[kTileWarps];
   const int lane = threadIdx.x & 31;
   CellTile& t = tiles[threadIdx.x >> 5];
-  const int64_t c0 = ((int64_t)blockIdx.x * kTileWarps + (threadIdx.x >> 5)) * kTileCells;
+  const int64_t c0 = (bid * kTileWarps + (threadIdx.x >> 5)) * kTileCells;
   if (c0 >= p.ncell) return;  // whole warp
   const int ncl = (int)min((int64_t)kTileCells, p.ncell - c0);
   const int* __restrict__ perm = s.perm;
@@ -371,6 +372,11 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Sol
       store_rotated<F32>(p, s, f, qv[u], idv[u], v, t.P[t.cell[j]]);
     }
   }
+}
+template <bool F32>
+__global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Solvent s, SolventF f, Cells cl,
+                                                               Membrane m, uint64_t eoff) {
+  cells_tile_block<F32>(p, s, f, cl, m, eoff, blockIdx.x);
 }
 
 inline unsigned cells_tile_blocks(int64_t ncell) {

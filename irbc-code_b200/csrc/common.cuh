@@ -22,7 +22,25 @@ struct DevParams {
   // the host writes the base once per step call, so that a captured
   // sequence of steps replays with the right epochs
   const uint64_t* ebase;
+  // run-time health word of the simulation (HEALTH_* bits), or null
+  int* health;
 };
+
+// Health bits, raised by the kernels that write the state and read back by
+// the host (irbc_sync, irbc_health): a solvent particle whose position or
+// velocity is not finite, or whose height left [-a, Lz + a]; a membrane
+// vertex whose force or velocity is not finite.  The checks ride on values
+// the kernels hold in registers anyway and write only when something is
+// wrong.
+enum : int { HEALTH_SOLVENT = 1, HEALTH_MEMBRANE = 2 };
+__device__ __forceinline__ void raise_health(const DevParams& p, bool bad, int bit) {
+  if (bad && p.health) atomicOr(p.health, bit);
+}
+template <typename R>
+__device__ __forceinline__ bool solvent_bad(const DevParams& p, R X, R Y, R Z, R VX, R VY, R VZ) {
+  const R s = X + Y + VX + VY + VZ;
+  return !isfinite(s) || !(Z >= R(-p.a) && Z <= R(p.Lz + p.a));
+}
 
 __device__ __forceinline__ uint64_t epoch_of(const DevParams& p, uint64_t off) { return *p.ebase + off; }
 

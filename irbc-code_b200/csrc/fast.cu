@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <cooperative_groups.h>
 #include "fast.h"
 #include "fp32.h"
 
@@ -245,6 +246,7 @@ __global__ void __launch_bounds__(256) k_stream_fast(DevParams p, Solvent s, con
     return;
   }
   finish_stream(p, 0.0, X, Y, Z, VX, VY, VZ);
+  raise_health(p, solvent_bad(p, X, Y, Z, VX, VY, VZ), HEALTH_SOLVENT);
   s.x[i] = X; s.y[i] = Y; s.z[i] = Z;
   if (VX != VX0 || VY != VY0 || VZ != VZ0 || VX0 != VX0) { s.v[i].vx = VX; s.v[i].vy = VY; s.v[i].vz = VZ; }
 }
@@ -343,6 +345,7 @@ __device__ __forceinline__ void heavy_particle(const DevParams& p, Solvent& s, S
   heavy_walk(p, sn, tri, ids, len, lane, indio, st[0], st[1], st[2], st[3], st[4], st[5], fulldt);
   if (lane == 0) {
     finish_stream(p, fulldt, st[0], st[1], st[2], st[3], st[4], st[5]);
+    raise_health(p, solvent_bad(p, st[0], st[1], st[2], st[3], st[4], st[5]), HEALTH_SOLVENT);
     HeavyIO<F32>::store(s, f, i, st, st0);
   }
 }
@@ -357,21 +360,22 @@ __device__ __forceinline__ void heavy_particle(const DevParams& p, Solvent& s, S
 // particle, from global memory.  nact is read on the device and the grid
 // is sized by the bucket capacity, so a captured launch stays valid across
 // list updates.
+// block `bid` of `nblk`
 template <bool F32>
-__global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, SolventF f,
-                                                      const int* __restrict__ lstart, const int* __restrict__ lidx,
-                                                      const int* __restrict__ acell, int* bcnt,
-                                                      const int* __restrict__ bucket, Snap sn,
-                                                      const TriPre* __restrict__ pre, const int* queue,
-                                                      const int* qn, const int* __restrict__ nactp,
-                                                      const int* __restrict__ border) {
+__device__ __forceinline__ void stream_cells_block(const DevParams& p, Solvent& s, SolventF& f,
+                                                   const int* __restrict__ lstart, const int* __restrict__ lidx,
+                                                   const int* __restrict__ acell, int* bcnt,
+                                                   const int* __restrict__ bucket, const Snap& sn,
+                                                   const TriPre* __restrict__ pre, const int* queue, const int* qn,
+                                                   const int* __restrict__ nactp, const int* __restrict__ border,
+                                                   int bid, int nblk) {
   extern __shared__ double sh[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int nact = *nactp;
-  if ((int)blockIdx.x >= nact) {
+  if (bid >= nact) {
     const int nq = *qn;
-    const int64_t gw = (int64_t)(blockIdx.x - nact) * nw + w;
-    const int64_t tw = (int64_t)(gridDim.x - nact) * nw;
+    const int64_t gw = (int64_t)(bid - nact) * nw + w;
+    const int64_t tw = (int64_t)(nblk - nact) * nw;
     for (int64_t q = gw; q < nq; q += tw) {
       const int64_t i = queue[q];
       double X, Y, Z;
@@ -387,7 +391,7 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
     }
     return;
   }
-  const int a = border[blockIdx.x];
+  const int a = border[bid];
   __shared__ int s_n;
   if (threadIdx.x == 0) {
     s_n = min(bcnt[a], kBucket);
@@ -411,6 +415,17 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
     heavy_particle<F32>(p, s, f, sn, i, lane, len, [&](int e) -> const TriPre& { return st[e]; },
                         [&](int e) { return sj[e]; });
   }
+}
+template <bool F32>
+__global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, SolventF f,
+                                                      const int* __restrict__ lstart, const int* __restrict__ lidx,
+                                                      const int* __restrict__ acell, int* bcnt,
+                                                      const int* __restrict__ bucket, Snap sn,
+                                                      const TriPre* __restrict__ pre, const int* queue,
+                                                      const int* qn, const int* __restrict__ nactp,
+                                                      const int* __restrict__ border) {
+  stream_cells_block<F32>(p, s, f, lstart, lidx, acell, bcnt, bucket, sn, pre, queue, qn, nactp, border,
+                          (int)blockIdx.x, (int)gridDim.x);
 }
 
 // ========================================================= membrane step ====
@@ -714,10 +729,10 @@ __device__ __forceinline__ void bond_prep_item(const DevParams& p, Membrane& m, 
 // and bending terms and the bond preparation, which do not depend on
 // Sarea / Volume, so they overlap the sums.  The triangle terms follow in
 // k_force_tri.
-__global__ void __launch_bounds__(256) k_sum_edges(DevParams p, Membrane m, double* __restrict__ slot, int do_sum,
-                                                    int* __restrict__ vd, int* __restrict__ vw,
-                                                    double* __restrict__ vX) {
-  if (blockIdx.x == 0) {
+__device__ __forceinline__ void sum_edges_block(const DevParams& p, Membrane& m, double* __restrict__ slot,
+                                                int do_sum, int* __restrict__ vd, int* __restrict__ vw,
+                                                double* __restrict__ vX, int bid) {
+  if (bid == 0) {
     if (!do_sum) return;
     extern __shared__ double sh[];
     const bool staged = p.nt <= kSumSmemT;
@@ -731,10 +746,15 @@ __global__ void __launch_bounds__(256) k_sum_edges(DevParams p, Membrane m, doub
     else if (threadIdx.x == 32) m.sc->Volume = ordered_sum(v, p.nt);
     return;
   }
-  const int k = (blockIdx.x - 1) * blockDim.x + threadIdx.x;  // 0 .. 2E + V
+  const int k = (bid - 1) * blockDim.x + threadIdx.x;  // 0 .. 2E + V
   if (k < p.ne) force_item(p, m, slot, k);
   else if (k < 2 * p.ne) force_item(p, m, slot, p.nt + k);  // dihedral k - E
   else bond_prep_item(p, m, vd, vw, vX, k - 2 * p.ne);
+}
+__global__ void __launch_bounds__(256) k_sum_edges(DevParams p, Membrane m, double* __restrict__ slot, int do_sum,
+                                                    int* __restrict__ vd, int* __restrict__ vw,
+                                                    double* __restrict__ vX) {
+  sum_edges_block(p, m, slot, do_sum, vd, vw, vX, (int)blockIdx.x);
 }
 __global__ void k_force_tri(DevParams p, Membrane m, double* __restrict__ slot) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -794,18 +814,25 @@ __device__ __forceinline__ void gather_vertex(const DevParams& p, Membrane& m, c
   if (cc < 0.5) f[2] -= 300.0 * exp(-50.0 * cc);
   m.fx[i] = f[0]; m.fy[i] = f[1]; m.fz[i] = f[2];
   // second half-kick (maincode.cpp:727-733)
-  m.vx[i] += (f[0] * p.dtmd / (2.0 * p.pmass));
-  m.vy[i] += (f[1] * p.dtmd / (2.0 * p.pmass));
-  m.vz[i] += (f[2] * p.dtmd / (2.0 * p.pmass));
+  const double vx = m.vx[i] + (f[0] * p.dtmd / (2.0 * p.pmass));
+  const double vy = m.vy[i] + (f[1] * p.dtmd / (2.0 * p.pmass));
+  const double vz = m.vz[i] + (f[2] * p.dtmd / (2.0 * p.pmass));
+  m.vx[i] = vx; m.vy[i] = vy; m.vz[i] = vz;
+  const double chk = f[0] + f[1] + f[2] + vx + vy + vz;
+  raise_health(p, !isfinite(chk), HEALTH_MEMBRANE);
+}
+__device__ __forceinline__ void gather_block(const DevParams& p, Membrane& m, const double* __restrict__ slot,
+                                             const int* __restrict__ gstart, const int* __restrict__ gidx, int bid) {
+  __shared__ double sh[kGW][kGSlots * 3 + 3];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = bid * kGW + w;
+  if (i >= p.nv) return;
+  gather_vertex(p, m, slot, gstart, gidx, i, lane, sh[w]);
 }
 __global__ void __launch_bounds__(32 * kGW) k_force_gather_w(DevParams p, Membrane m, const double* __restrict__ slot,
                                                            const int* __restrict__ gstart,
                                                            const int* __restrict__ gidx) {
-  __shared__ double sh[kGW][kGSlots * 3 + 3];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int i = blockIdx.x * kGW + w;
-  if (i >= p.nv) return;
-  gather_vertex(p, m, slot, gstart, gidx, i, lane, sh[w]);
+  gather_block(p, m, slot, gstart, gidx, (int)blockIdx.x);
 
 }
 
@@ -976,11 +1003,15 @@ constexpr int kBlockT = 512;      // threads of the one-block membrane kernels
 constexpr int kBlockMaxV = 1024;  // meshes up to this many vertices use them
 __global__ void __launch_bounds__(kBlockT) k_membrane_block(DevParams p, Membrane m, FastBufs f, uint64_t eoff);
 __global__ void __launch_bounds__(kBlockT) k_kick_prep_block(DevParams p, Membrane m, Snap sn, TriPre* pre);
+constexpr int kClusterCTAs = 8, kClusterT = 512;  // the cluster membrane kernel's blocks and threads
+__global__ void __launch_bounds__(kClusterT)
+    k_membrane_cluster(DevParams p, Membrane m, FastBufs f, uint64_t eoff, int next_kick, int next_buf);
 
 bool is_membrane_kernel(const void* fn) {
   const void* k[] = {(const void*)k_m_drift, (const void*)k_m_av, (const void*)k_m_sum,
                      (const void*)k_sum_edges, (const void*)k_force_tri, (const void*)k_force_gather_w,
                      (const void*)k_tail_b, (const void*)k_kick_snap, (const void*)k_membrane_block,
+                     (const void*)k_membrane_cluster,
                      (const void*)k_kick_prep_block,
                      (const void*)k_tri_prep, (const void*)k_snap};
   for (const void* q : k)
@@ -1118,6 +1149,69 @@ __global__ void __launch_bounds__(kBlockT) k_membrane_block(DevParams p, Membran
   tail_b_block(p, m, f.vd, f.vw, f.vX, epoch_of(p, eoff), *reinterpret_cast<TailSmem*>(shb));
 }
 
+// ================================================ membrane step, one cluster ===
+// The whole membrane step of a mesh of any size in ONE launch: a cluster of
+// kClusterCTAs blocks of kClusterT threads, co-scheduled on one GPC, whose
+// phases are separated by cluster barriers (barrier.cluster arrive.release /
+// wait.acquire: every global write of one phase is visible to all blocks of
+// the cluster in the next) instead of kernel boundaries.  Each phase calls
+// the same per-item functions in the same order as the wide kernels, so
+// results are bit for bit the same; the chain of eight dependent launches
+// becomes one.  next_kick: the next step's half-kick, snapshot next_buf and
+// its triangle records follow in the same launch.
+__global__ void __launch_bounds__(kClusterT)
+    k_membrane_cluster(DevParams p, Membrane m, FastBufs f, uint64_t eoff, int next_kick, int next_buf) {
+  extern __shared__ double shc[];
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  const int T = blockDim.x, t = threadIdx.x;
+  const int cta = (int)cl.block_rank();
+  const int g = cta * T + t, G = kClusterCTAs * T;
+  for (int i = g; i < p.nv; i += G) m_drift_item(p, m, i);
+  cl.sync();
+  for (int i = g; i < p.nt; i += G) m_av_item(p, m, i);
+  cl.sync();
+  // block 0's warps 0 and 1: Sarea and Volume left to right, staged in its
+  // shared memory when they fit; every other thread of the cluster: the
+  // edge and bending terms and the bond preparation
+  const bool staged = p.nt <= kSumSmemT;
+  if (cta == 0 && staged) {
+    for (int i = t; i < p.nt; i += T) { shc[i] = m.area[i]; shc[p.nt + i] = m.vol[i]; }
+    __syncthreads();
+  }
+  if (cta == 0 && t == 0) {
+    m.sc->Sarea = ordered_sum(staged ? shc : m.area, p.nt);
+  } else if (cta == 0 && t == 32) {
+    m.sc->Volume = ordered_sum(staged ? shc + p.nt : m.vol, p.nt);
+  } else if (g >= 64) {
+    const int n = 2 * p.ne + p.nv;
+    for (int k = g - 64; k < n; k += G - 64) {
+      if (k < p.ne) force_item(p, m, f.slot, k);
+      else if (k < 2 * p.ne) force_item(p, m, f.slot, p.nt + k);  // dihedral k - E
+      else bond_prep_item(p, m, f.vd, f.vw, f.vX, k - 2 * p.ne);
+    }
+  }
+  cl.sync();
+  for (int k = g; k < p.nt; k += G) force_item(p, m, f.slot, p.ne + k);
+  cl.sync();
+  {
+    const int lane = t & 31;
+    double* shw = shc + (t >> 5) * (kGSlots * 3 + 3);
+    for (int i = g >> 5; i < p.nv; i += G >> 5) gather_vertex(p, m, f.slot, f.gstart, f.gidx, i, lane, shw);
+  }
+  cl.sync();
+  if (cta == 0) tail_b_block(p, m, f.vd, f.vw, f.vX, epoch_of(p, eoff), *reinterpret_cast<TailSmem*>(shc));
+  if (!next_kick) return;
+  cl.sync();
+  for (int i = g; i < p.nv; i += G) kick_snap_item(p, m, f.snap[next_buf], i);
+  cl.sync();
+  for (int j = g; j < p.nt; j += G) tri_prep_one(p, m, j, m.vx, m.vy, m.vz, f.pre[next_buf]);
+}
+
+static size_t cluster_smem(const DevParams& p) {
+  size_t b = std::max((size_t)(kClusterT / 32) * (kGSlots * 3 + 3) * sizeof(double), sizeof(TailSmem));
+  return p.nt <= kSumSmemT ? std::max(b, 2 * (size_t)p.nt * sizeof(double)) : b;
+}
+
 static size_t block_smem(const DevParams& p) {
   size_t b = std::max((size_t)(kBlockT / 32) * (kGSlots * 3 + 3) * sizeof(double), sizeof(TailSmem));
   return std::max(b, 2 * (size_t)p.nt * sizeof(double));
@@ -1127,6 +1221,27 @@ bool one_block_fits(const DevParams& p) { return p.nv <= kBlockMaxV && 2 * (size
 
 int fast_membrane_step(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
                        cudaStream_t st, cudaEvent_t readers) {
+  if (f.cluster) {
+    // the snapshot the kick writes was read by the previous streaming
+    if (next_kick && readers) cudaStreamWaitEvent(st, readers, 0);
+    if (first_on_device(7))
+      cudaFuncSetAttribute(k_membrane_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    // one cluster of kClusterCTAs blocks
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kClusterCTAs);
+    cfg.blockDim = dim3(kClusterT);
+    cfg.dynamicSmemBytes = cluster_smem(p);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kClusterCTAs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_membrane_cluster, p, m, f, epoch, next_kick, next_buf);
+    return 1;
+  }
   if (!f.one_block)
     return fast_drift_va(p, m, st, false) + fast_forces_tail(p, m, f, epoch, next_kick, next_buf, st, true, readers);
   const size_t smem = block_smem(p);
@@ -1163,3 +1278,6 @@ int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoc
 
 // FP32-bulk solvent kernels share the device helpers above
 #include "fp32.cuh"
+
+// one launch per phase over a cohort of FP32 simulations
+#include "multi.cuh"

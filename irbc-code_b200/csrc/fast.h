@@ -32,6 +32,7 @@ struct FastBufs {
   int64_t bcap = 0;       // listed cells the buckets have room for
   int* border = nullptr;  // the listed cell (rank) of each k_stream_cells block: longest lists first
   bool one_block = false; // the membrane step as one block per launch (small meshes)
+  bool cluster = false;   // the membrane step as one launch of a thread-block cluster (any mesh)
   int hcap = kHeavyList;  // list entries k_stream_cells stages (its shared memory); longer lists go
                           // to the overflow queue
   double* slot = nullptr; // force terms: 3 doubles per slot, 4E + 9T + 4E slots
@@ -66,8 +67,9 @@ bool is_membrane_kernel(const void* fn);
 int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
                      cudaStream_t st, bool sum_pending, cudaEvent_t readers = nullptr);
 // the whole membrane step of irbc_step (drift .. bond_dynamics, then the
-// next half-kick and snapshot as fast_forces_tail): in one block per launch
-// when f.one_block, else fast_drift_va + fast_forces_tail
+// next half-kick and snapshot as fast_forces_tail): in one launch of a
+// thread-block cluster when f.cluster, in one block per launch when
+// f.one_block, else fast_drift_va + fast_forces_tail
 int fast_membrane_step(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
                        cudaStream_t st, cudaEvent_t readers = nullptr);
 // whether a mesh suits the one-block membrane step

@@ -47,14 +47,16 @@ __device__ __forceinline__ int shifted_cell_f(const DevParams& p, float4 q, cons
   return cell_of(p, fx, fy, fz);
 }
 
-__global__ void __launch_bounds__(256) k_count_f(DevParams p, SolventF f, int* cnt, int* slot, uint64_t eoff) {
+// block `bid` of the count: kCountPer particles per thread
+__device__ __forceinline__ void count_f_block(const DevParams& p, const SolventF& f, int* cnt, int* slot,
+                                              uint64_t eoff, int64_t bid) {
   const uint64_t epoch = epoch_of(p, eoff);
   // the grid shift, drawn once per block
   __shared__ double sr[3];
   if (threadIdx.x == 0) grid_shift(p, epoch, sr);
   __syncthreads();
   const double r[3] = {sr[0], sr[1], sr[2]};
-  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x * kCountPer + threadIdx.x;
+  const int64_t i0 = bid * blockDim.x * kCountPer + threadIdx.x;
   int c[kCountPer];
 #pragma unroll
   for (int u = 0; u < kCountPer; ++u) {
@@ -72,30 +74,39 @@ __global__ void __launch_bounds__(256) k_count_f(DevParams p, SolventF f, int* c
     }
   }
 }
+__global__ void __launch_bounds__(256) k_count_f(DevParams p, SolventF f, int* cnt, int* slot, uint64_t eoff) {
+  count_f_block(p, f, cnt, slot, eoff, blockIdx.x);
+}
 
-__global__ void k_perm_f(const int* __restrict__ key, const int* __restrict__ slot, const int* __restrict__ start,
-                         int64_t n, int* __restrict__ perm) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void perm_f_item(const int* __restrict__ key, const int* __restrict__ slot,
+                                            const int* __restrict__ start, int64_t n, int* __restrict__ perm,
+                                            int64_t i) {
   if (i >= n) return;
   perm[(int64_t)start[key[i]] + slot[i]] = (int)i;
 }
+__global__ void k_perm_f(const int* __restrict__ key, const int* __restrict__ slot, const int* __restrict__ start,
+                         int64_t n, int* __restrict__ perm) {
+  perm_f_item(key, slot, start, n, perm, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // physical re-sort by collision cell every kResortEvery collisions
-__global__ void k_gather_f(SolventF f, const int* __restrict__ perm) {
-  int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void gather_f_item(const SolventF& f, const int* __restrict__ perm, int64_t j) {
   if (j >= f.n) return;
   const int i = perm[j];
   f.pos2[j] = f.pos[i];
   f.vel2[j] = f.vel[i];
   f.pid2[j] = f.pid[i];
 }
-__global__ void k_copy_back_f(SolventF f) {
-  int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void copy_back_f_item(const SolventF& f, int64_t j) {
   if (j >= f.n) return;
   f.pos[j] = f.pos2[j];
   f.vel[j] = f.vel2[j];
   f.pid[j] = f.pid2[j];
 }
+__global__ void k_gather_f(SolventF f, const int* __restrict__ perm) {
+  gather_f_item(f, perm, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_copy_back_f(SolventF f) { copy_back_f_item(f, (int64_t)blockIdx.x * blockDim.x + threadIdx.x); }
 
 void launch_collide_count_f(const DevParams& p, SolventF& f, Solvent& s, Cells& c, uint64_t epoch,
                             cudaStream_t st) {
@@ -125,10 +136,9 @@ void launch_resort_f(SolventF& f, Solvent& s, cudaStream_t st) {
 // ---- streaming ------------------------------------------------------------------
 // free flight, walls and wrap in float (maincode.cpp:516-560); particles in
 // cells with triangles are handed to k_stream_cells<true> (double precision)
-__global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const int* __restrict__ lstart,
-                                                  const int* __restrict__ lrank, int* bcnt, int* bucket,
-                                                  int* queue, int* qn, int hcap) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void stream_f_item(const DevParams& p, const SolventF& f, const int* __restrict__ lstart,
+                                              const int* __restrict__ lrank, int* bcnt, int* bucket, int* queue,
+                                              int* qn, int hcap, int64_t i) {
   if (i >= f.n) return;
   const float Lx = (float)p.Lx, Ly = (float)p.Ly, Lz = (float)p.Lz, dt = (float)p.dtmd;
   float4 q = f.pos[i], v = f.vel[i];
@@ -156,7 +166,13 @@ __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const
   }
   X = bbound(X, Lx);
   Y = bbound(Y, Ly);
+  raise_health(p, solvent_bad(p, X, Y, Z, v.x, v.y, v.z), HEALTH_SOLVENT);
   f.pos[i] = make_float4(X, Y, Z, q.w);
+}
+__global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const int* __restrict__ lstart,
+                                                  const int* __restrict__ lrank, int* bcnt, int* bucket,
+                                                  int* queue, int* qn, int hcap) {
+  stream_f_item(p, f, lstart, lrank, bcnt, bucket, queue, qn, hcap, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 void fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb, int buf, cudaStream_t st,

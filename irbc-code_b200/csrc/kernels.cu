@@ -7,6 +7,7 @@
 // exp, log) elsewhere.
 #include <cstdio>
 #include "sim.h"
+#include "multi.h"
 #include "cells_tile.cuh"
 
 namespace irbc {
@@ -57,6 +58,13 @@ __global__ void k_unpack_vel(Solvent s, double* vx, double* vy, double* vz, int*
   const SolVel r = s.v[i];
   if (vx) { vx[i] = r.vx; vy[i] = r.vy; vz[i] = r.vz; }
   if (id) id[i] = r.id;
+}
+__global__ void k_iota(int* d, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) d[i] = (int)i;
+}
+void launch_iota(int* d, int64_t n, cudaStream_t st) {
+  if (n > 0) k_iota<<<nblk(n, 256), 256, 0, st>>>(d, n);
 }
 void launch_pack_vel(Solvent& s, const double* vx, const double* vy, const double* vz, const int* id,
                      cudaStream_t st) {
@@ -174,8 +182,9 @@ int64_t scan_part_blocks(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
 
 __device__ __forceinline__ int ld0(const int* a, int64_t i) { return a ? a[i] : 0; }
 
-__global__ void k_scan_part(const int* a, const int* b, const int* c, int64_t n, int* part) {
-  int64_t base = (int64_t)blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+__device__ __forceinline__ void scan_part_block(const int* a, const int* b, const int* c, int64_t n, int* part,
+                                                int64_t bid) {
+  int64_t base = bid * kScanTile + threadIdx.x * kScanItems;
   int s[3] = {0, 0, 0};
   for (int q = 0; q < kScanItems; ++q) {
     int64_t i = base + q;
@@ -193,12 +202,15 @@ __global__ void k_scan_part(const int* a, const int* b, const int* c, int64_t n,
   if (threadIdx.x < 3) {
     int t = 0;
     for (int q = 0; q < kScanT / 32; ++q) t += ws[threadIdx.x][q];
-    part[blockIdx.x * 3 + threadIdx.x] = t;
+    part[bid * 3 + threadIdx.x] = t;
   }
+}
+__global__ void k_scan_part(const int* a, const int* b, const int* c, int64_t n, int* part) {
+  scan_part_block(a, b, c, n, part, blockIdx.x);
 }
 
 // one block: exclusive scan of the block sums in place, totals out
-__global__ void k_scan_top(int* part, int64_t nb, int* totals) {
+__device__ __forceinline__ void scan_top_block(int* part, int64_t nb, int* totals) {
   __shared__ int carry[3];
   if (threadIdx.x < 3) carry[threadIdx.x] = 0;
   __syncthreads();
@@ -234,10 +246,11 @@ __global__ void k_scan_top(int* part, int64_t nb, int* totals) {
   }
   if (threadIdx.x < 3 && totals) totals[threadIdx.x] = carry[threadIdx.x];
 }
+__global__ void k_scan_top(int* part, int64_t nb, int* totals) { scan_top_block(part, nb, totals); }
 
-__global__ void k_scan_final(const int* a, const int* b, const int* c, int* oa, int* ob, int* oc,
-                             int64_t n, const int* part) {
-  int64_t base = (int64_t)blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+__device__ __forceinline__ void scan_final_block(const int* a, const int* b, const int* c, int* oa, int* ob, int* oc,
+                                                 int64_t n, const int* part, int64_t bid) {
+  int64_t base = bid * kScanTile + threadIdx.x * kScanItems;
   int loc[3][kScanItems];
   int s[3] = {0, 0, 0};
   for (int q = 0; q < kScanItems; ++q) {
@@ -265,7 +278,7 @@ __global__ void k_scan_final(const int* a, const int* b, const int* c, int* oa, 
     for (int q = 0; q < kScanT / 32; ++q) { int t = ws[threadIdx.x][q]; ws[threadIdx.x][q] = acc; acc += t; }
   }
   __syncthreads();
-  for (int k = 0; k < 3; ++k) ex[k] += ws[k][w] + part[blockIdx.x * 3 + k];
+  for (int k = 0; k < 3; ++k) ex[k] += ws[k][w] + part[bid * 3 + k];
   for (int q = 0; q < kScanItems; ++q) {
     int64_t i = base + q;
     if (i < n) {
@@ -274,6 +287,10 @@ __global__ void k_scan_final(const int* a, const int* b, const int* c, int* oa, 
       if (oc) oc[i] = ex[2] + loc[2][q];
     }
   }
+}
+__global__ void k_scan_final(const int* a, const int* b, const int* c, int* oa, int* ob, int* oc,
+                             int64_t n, const int* part) {
+  scan_final_block(a, b, c, oa, ob, oc, n, part, blockIdx.x);
 }
 
 void launch_scan3(const int* a, const int* b, const int* c, int* oa, int* ob, int* oc, int* totals,
@@ -300,7 +317,7 @@ __device__ __forceinline__ int shifted_cell(const DevParams& p, double x, double
 
 // vertices and parasite into the shifted grid (:149-162); vertex keys sorted
 // by (cell, vertex) with a bitonic sort in shared memory
-__global__ void k_vbin(DevParams p, Membrane m, int* ncm, uint64_t eoff) {
+__device__ __forceinline__ void vbin_block(const DevParams& p, const Membrane& m, int* ncm, uint64_t eoff) {
   const uint64_t epoch = epoch_of(p, eoff);
   extern __shared__ uint64_t sk[];
   double r[3];
@@ -337,6 +354,7 @@ __global__ void k_vbin(DevParams p, Membrane m, int* ncm, uint64_t eoff) {
   }
   for (int i = threadIdx.x; i < p.nv; i += blockDim.x) m.vkey[i] = sk[i];
 }
+__global__ void k_vbin(DevParams p, Membrane m, int* ncm, uint64_t eoff) { vbin_block(p, m, ncm, eoff); }
 
 // cell of each particle in the shifted grid; warp-aggregated slot counters
 __global__ void __launch_bounds__(256) k_count(DevParams p, Solvent s, int* cnt, uint64_t eoff) {
@@ -371,9 +389,8 @@ __global__ void __launch_bounds__(256) k_count(DevParams p, Solvent s, int* cnt,
 // ghost flags for the scan: wall cells (zmax >= Lz or zmin <= 0) with fewer
 // than navg solvent particles (:185-204), and membrane cells with fewer
 // than navg particles of any kind (:236-244)
-__global__ void k_ghost_flags(DevParams p, const int* cnt, const int* ncm, const MemScalars* sc,
-                              int* wflag, int* mflag) {
-  int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ghost_flags_item(const DevParams& p, const int* cnt, const int* ncm,
+                                                 const MemScalars* sc, int* wflag, int* mflag, int64_t c) {
   if (c >= p.ncell) return;
   int k = (int)(c % p.nz);
   double zmin = -1.0 + (double)k * p.a, zmax = -1.0 + (double)k * p.a + p.a;
@@ -383,6 +400,10 @@ __global__ void k_ghost_flags(DevParams p, const int* cnt, const int* ncm, const
   int mem = (ncm[c] > 0) && (nt < p.navg);
   wflag[c] = wall;
   mflag[c] = mem;
+}
+__global__ void k_ghost_flags(DevParams p, const int* cnt, const int* ncm, const MemScalars* sc,
+                              int* wflag, int* mflag) {
+  ghost_flags_item(p, cnt, ncm, sc, wflag, mflag, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // counting sort of particle indices: perm[start[cell] + slot] = i
@@ -1172,11 +1193,17 @@ void launch_kick2(const DevParams& p, Membrane& m, cudaStream_t st) {
 
 // ========================================================== observables ===
 // Quantities the reference does not compute (its only outputs are the files):
-// out[0] = sum m|v|^2 / (3 N) of the solvent, out[1..3] = membrane centre of
-// mass (unwrapped), out[4] = Sarea, out[5] = Volume, out[6] = bonds,
-// out[7] = mean solvent vx.  prof[2k], prof[2k+1] = sum vx and count in the
-// z-layer [k a, (k+1) a).
-__global__ void k_obs_solvent(DevParams p, Solvent s, double* out, double* prof, int nbins) {
+// out[0] = solvent temperature sum m|v - u|^2 / (3 N), u the mean velocity
+// of the particle's z-layer of height a (the Couette flow's own kinetic
+// energy is not heat), out[1..3] = membrane centre of mass (unwrapped),
+// out[4] = Sarea, out[5] = Volume, out[6] = bonds, out[7] = mean solvent
+// vx, out[8] = sum m|v|^2 / (3 N) (flow included).  prof[2k], prof[2k+1] =
+// sum vx and count in the z-layer [k a, (k+1) a).
+__device__ __forceinline__ int obs_layer(double z, double a, int n) {
+  int b = (int)floor(z / a);
+  return b < 0 ? 0 : (b >= n ? n - 1 : b);
+}
+__global__ void k_obs_solvent(DevParams p, Solvent s, double* out, double* lay, int nlay, double* prof, int nbins) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0, vxs = 0;
   if (i < s.n) {
@@ -1184,9 +1211,14 @@ __global__ void k_obs_solvent(DevParams p, Solvent s, double* out, double* prof,
     double vx = r.vx, vy = r.vy, vz = r.vz;
     e = p.mass * (vx * vx + vy * vy + vz * vz);
     vxs = vx;
+    const double z = s.z[i];
+    double* L = lay + 4 * obs_layer(z, p.a, nlay);
+    atomicAdd(L, vx);
+    atomicAdd(L + 1, vy);
+    atomicAdd(L + 2, vz);
+    atomicAdd(L + 3, 1.0);
     if (prof) {
-      int b = (int)floor(s.z[i] / p.a);
-      b = b < 0 ? 0 : (b >= nbins ? nbins - 1 : b);
+      const int b = obs_layer(z, p.a, nbins);
       atomicAdd(&prof[2 * b], vx);
       atomicAdd(&prof[2 * b + 1], 1.0);
     }
@@ -1197,7 +1229,7 @@ __global__ void k_obs_solvent(DevParams p, Solvent s, double* out, double* prof,
   }
   if ((threadIdx.x & 31) == 0) { atomicAdd(&out[8], e); atomicAdd(&out[9], vxs); }
 }
-__global__ void k_obs_membrane(DevParams p, Membrane m, double* out, int64_t ns) {
+__global__ void k_obs_membrane(DevParams p, Membrane m, double* out, const double* lay, int nlay, int64_t ns) {
   if (threadIdx.x != 0) return;
   double cx = 0, cy = 0, cz = 0;
   int bonds = 0;
@@ -1205,17 +1237,80 @@ __global__ void k_obs_membrane(DevParams p, Membrane m, double* out, int64_t ns)
     cx += m.x[i] + m.ix[i] * p.Lx; cy += m.y[i] + m.iy[i] * p.Ly; cz += m.z[i];
     bonds += m.bondi[i] == 1;
   }
-  out[0] = ns ? out[8] / (3.0 * (double)ns) : 0.0;
+  // sum m|v - u|^2 = sum m|v|^2 - sum over layers of m |S|^2 / n (S the
+  // layer's velocity sum, n its count)
+  double flow = 0;
+  for (int b = 0; b < nlay; ++b) {
+    const double* L = lay + 4 * b;
+    if (L[3] > 0) flow += p.mass * (L[0] * L[0] + L[1] * L[1] + L[2] * L[2]) / L[3];
+  }
+  out[0] = ns ? (out[8] - flow) / (3.0 * (double)ns) : 0.0;
   out[1] = cx / p.nv; out[2] = cy / p.nv; out[3] = cz / p.nv;
   out[4] = m.sc->Sarea; out[5] = m.sc->Volume; out[6] = bonds;
   out[7] = ns ? out[9] / (double)ns : 0.0;
+  out[8] = ns ? out[8] / (3.0 * (double)ns) : 0.0;
 }
-void launch_observables(const DevParams& p, const Solvent& s, const Membrane& m, double* out,
-                        double* prof, int nbins, cudaStream_t st) {
-  cudaMemsetAsync(out, 0, sizeof(double) * 16, st);
+void launch_observables(const DevParams& p, const Solvent& s, const Membrane& m, double* obs, int nbins,
+                        cudaStream_t st) {
+  int nlay = (int)(p.Lz / p.a);
+  nlay = nlay < 1 ? 1 : (nlay > kObsMaxBins ? kObsMaxBins : nlay);
+  double* lay = obs + kObsLayers;
+  double* prof = nbins > 0 ? obs + 64 : nullptr;
+  cudaMemsetAsync(obs, 0, sizeof(double) * 16, st);
+  cudaMemsetAsync(lay, 0, sizeof(double) * 4 * nlay, st);
   if (prof) cudaMemsetAsync(prof, 0, sizeof(double) * 2 * nbins, st);
-  if (s.n) k_obs_solvent<<<nblk(s.n, 256), 256, 0, st>>>(p, s, out, prof, nbins);
-  k_obs_membrane<<<1, 32, 0, st>>>(p, m, out, s.n);
+  if (s.n) k_obs_solvent<<<nblk(s.n, 256), 256, 0, st>>>(p, s, obs, lay, nlay, prof, nbins);
+  k_obs_membrane<<<1, 32, 0, st>>>(p, m, obs, lay, nlay, s.n);
+}
+
+// ============================== one launch per phase over a cohort (multi.h) ==
+// the counters of a collision cleared: cnt (solvent per cell) and ncm
+// (membrane vertices per cell), 256 cells per block
+__global__ void __launch_bounds__(256) km_zero(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  const int64_t c = (int64_t)b * blockDim.x + threadIdx.x;
+  if (c < M.c.n) { M.c.cnt[c] = 0; M.c.ncm[c] = 0; }
+}
+__global__ void __launch_bounds__(1024) km_vbin(Member* __restrict__ mem, const int2* __restrict__ tab,
+                                                uint64_t eoff) {
+  KM_MEMBER;
+  vbin_block(M.p, M.m, M.c.ncm, eoff);
+}
+__global__ void __launch_bounds__(256) km_ghost(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  ghost_flags_item(M.p, M.c.cnt, M.c.ncm, M.m.sc, M.c.wrank, M.c.mrank, (int64_t)b * blockDim.x + threadIdx.x);
+}
+// the scans of (cnt, wrank, mrank) into (start, wrank, mrank), as launch_scan3
+__global__ void __launch_bounds__(kScanT) km_scan_part(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  scan_part_block(M.c.cnt, M.c.wrank, M.c.mrank, M.c.n, M.c.scan_part, b);
+}
+// one block per member; also start[C] = the particle total
+__global__ void __launch_bounds__(1024) km_scan_top(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  scan_top_block(M.c.scan_part, (M.c.n + kScanTile - 1) / kScanTile, M.c.totals);
+  __syncthreads();
+  if (threadIdx.x == 0) M.c.start[M.c.n] = M.c.totals[0];
+}
+__global__ void __launch_bounds__(kScanT) km_scan_final(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  scan_final_block(M.c.cnt, M.c.wrank, M.c.mrank, M.c.start, M.c.wrank, M.c.mrank, M.c.n, M.c.scan_part, b);
+}
+
+int multi_collide_front(const MultiPlan& P, uint64_t eoff, cudaStream_t st) {
+  if (first_on_device(4))
+    cudaFuncSetAttribute(km_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
+  km_zero<<<P.blocks[MP_ZERO], 256, 0, st>>>(P.mem, P.table(MP_ZERO));
+  km_vbin<<<P.blocks[MP_VBIN], 1024, P.vbin_smem, st>>>(P.mem, P.table(MP_VBIN), eoff);
+  return 2;
+}
+
+int multi_collide_scan(const MultiPlan& P, cudaStream_t st) {
+  km_ghost<<<P.blocks[MP_GHOST], 256, 0, st>>>(P.mem, P.table(MP_GHOST));
+  km_scan_part<<<P.blocks[MP_SCAN], kScanT, 0, st>>>(P.mem, P.table(MP_SCAN));
+  km_scan_top<<<P.blocks[MP_SCAN_TOP], 1024, 0, st>>>(P.mem, P.table(MP_SCAN_TOP));
+  km_scan_final<<<P.blocks[MP_SCAN], kScanT, 0, st>>>(P.mem, P.table(MP_SCAN));
+  return 4;
 }
 
 }  // namespace irbc

@@ -1,0 +1,171 @@
+// multi.cuh -- (part of fast.cu) one launch per phase over a cohort of FP32
+// simulations (multi.h): the fused kernels of the streaming, the membrane
+// chain and the collision's particle phases.  Each block reads its member
+// and its block index within that member from the phase's block table
+// (KM_MEMBER) and runs the single-simulation kernel's device code.
+#include "multi.h"
+
+namespace irbc {
+
+// ---- streaming -------------------------------------------------------------
+__global__ void __launch_bounds__(256) km_stream_f(Member* __restrict__ mem, const int2* __restrict__ tab,
+                                                   int par) {
+  KM_MEMBER;
+  const DevParams& p = M.p;
+  const int64_t i0 = (int64_t)b * blockDim.x * kMultiStreamPer + threadIdx.x;
+#pragma unroll
+  for (int u = 0; u < kMultiStreamPer; ++u)
+    stream_f_item(p, M.f, M.c.lstart, M.c.lrank, M.fb.bcnt, M.fb.bucket, M.fb.queue, M.fb.qn + par, M.fb.hcap,
+                  i0 + (int64_t)u * blockDim.x);
+}
+
+__global__ void __launch_bounds__(256) km_stream_cells(Member* __restrict__ mem, const int2* __restrict__ tab,
+                                                       int par) {
+  KM_MEMBER;
+  // the overflow counter of the next step starts at zero
+  if (b == 0 && threadIdx.x == 0) M.fb.qn[par ^ 1] = 0;
+  stream_cells_block<true>(M.p, M.s, M.f, M.c.lstart, M.c.lidx, M.c.acell, M.fb.bcnt, M.fb.bucket, M.fb.snap[par],
+                           M.fb.pre[par], M.fb.queue, M.fb.qn + par, M.c.totals + 4, M.fb.border, b,
+                           (int)M.fb.bcap + kOverflowBlocks);
+}
+
+int multi_stream(const MultiPlan& P, int par, cudaStream_t st, cudaEvent_t snap) {
+  if (first_on_device(5))
+    cudaFuncSetAttribute(km_stream_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kHeavyList * (int)(sizeof(TriPre) + sizeof(int)));
+  km_stream_f<<<P.blocks[MP_STREAM], 256, 0, st>>>(P.mem, P.table(MP_STREAM), par);
+  if (snap) cudaStreamWaitEvent(st, snap, 0);
+  km_stream_cells<<<P.blocks[MP_CELLS], 256, P.cells_smem, st>>>(P.mem, P.table(MP_CELLS), par);
+  return 2;
+}
+
+// ---- membrane chain (the wide kernels' phases) --------------------------------
+__global__ void __launch_bounds__(128) km_drift(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  m_drift_item(M.p, M.m, b * blockDim.x + threadIdx.x);
+}
+__global__ void __launch_bounds__(128) km_av(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  m_av_item(M.p, M.m, b * blockDim.x + threadIdx.x);
+}
+__global__ void __launch_bounds__(256) km_sum_edges(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  sum_edges_block(M.p, M.m, M.fb.slot, 1, M.fb.vd, M.fb.vw, M.fb.vX, b);
+}
+__global__ void __launch_bounds__(128) km_force_tri(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  const int k = b * blockDim.x + threadIdx.x;
+  if (k < M.p.nt) force_item(M.p, M.m, M.fb.slot, M.p.ne + k);
+}
+__global__ void __launch_bounds__(32 * kGW) km_gather(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  gather_block(M.p, M.m, M.fb.slot, M.fb.gstart, M.fb.gidx, b);
+}
+__global__ void __launch_bounds__(kTailT) km_tail(Member* __restrict__ mem, const int2* __restrict__ tab,
+                                                  uint64_t eoff) {
+  KM_MEMBER;
+  __shared__ TailSmem S;
+  tail_b_block(M.p, M.m, M.fb.vd, M.fb.vw, M.fb.vX, epoch_of(M.p, eoff), S);
+}
+
+int multi_membrane(const MultiPlan& P, uint64_t eoff, cudaStream_t st) {
+  if (first_on_device(6))
+    cudaFuncSetAttribute(km_sum_edges, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kSumSmemT * sizeof(double));
+  km_drift<<<P.blocks[MP_DRIFT], 128, 0, st>>>(P.mem, P.table(MP_DRIFT));
+  km_av<<<P.blocks[MP_AV], 128, 0, st>>>(P.mem, P.table(MP_AV));
+  km_sum_edges<<<P.blocks[MP_SUM_EDGES], 256, P.sum_smem, st>>>(P.mem, P.table(MP_SUM_EDGES));
+  km_force_tri<<<P.blocks[MP_FORCE_TRI], 128, 0, st>>>(P.mem, P.table(MP_FORCE_TRI));
+  km_gather<<<P.blocks[MP_GATHER], 32 * kGW, 0, st>>>(P.mem, P.table(MP_GATHER));
+  km_tail<<<P.blocks[MP_TAIL], kTailT, 0, st>>>(P.mem, P.table(MP_TAIL), eoff);
+  return 6;
+}
+
+// next half-kick, snapshot `buf` and its triangle records
+__global__ void __launch_bounds__(128) km_kick(Member* __restrict__ mem, const int2* __restrict__ tab, int buf) {
+  KM_MEMBER;
+  kick_snap_item(M.p, M.m, M.fb.snap[buf], b * blockDim.x + threadIdx.x);
+}
+__global__ void __launch_bounds__(128) km_tri_prep(Member* __restrict__ mem, const int2* __restrict__ tab,
+                                                   int buf) {
+  KM_MEMBER;
+  const int j = b * blockDim.x + threadIdx.x;
+  if (j < M.p.nt) tri_prep_one(M.p, M.m, j, M.m.vx, M.m.vy, M.m.vz, M.fb.pre[buf]);
+}
+
+int multi_kick(const MultiPlan& P, int buf, cudaStream_t st) {
+  km_kick<<<P.blocks[MP_KICK], 128, 0, st>>>(P.mem, P.table(MP_KICK), buf);
+  km_tri_prep<<<P.blocks[MP_TRI_PREP], 128, 0, st>>>(P.mem, P.table(MP_TRI_PREP), buf);
+  return 2;
+}
+
+// ---- collision: particle phases ---------------------------------------------------
+__global__ void __launch_bounds__(256) km_count(Member* __restrict__ mem, const int2* __restrict__ tab,
+                                                uint64_t eoff) {
+  KM_MEMBER;
+  count_f_block(M.p, M.f, M.c.cnt, M.s.slot, eoff, b);
+}
+__global__ void __launch_bounds__(256) km_perm(Member* __restrict__ mem, const int2* __restrict__ tab) {
+  KM_MEMBER;
+  perm_f_item(M.f.pid, M.s.slot, M.c.start, M.f.n, M.s.perm, (int64_t)b * blockDim.x + threadIdx.x);
+}
+__global__ void __launch_bounds__(32 * kTileWarps) km_tile(Member* __restrict__ mem, const int2* __restrict__ tab,
+                                                           uint64_t eoff) {
+  KM_MEMBER;
+  cells_tile_block<true>(M.p, M.s, M.f, M.c, M.m, eoff, b);
+}
+__global__ void __launch_bounds__(256) km_move(Member* __restrict__ mem, const int2* __restrict__ tab, int back) {
+  KM_MEMBER;
+  const int64_t j = (int64_t)b * blockDim.x + threadIdx.x;
+  if (back) copy_back_f_item(M.f, j);
+  else gather_f_item(M.f, M.s.perm, j);
+}
+
+int multi_collide_count(const MultiPlan& P, uint64_t eoff, cudaStream_t st) {
+  km_count<<<P.blocks[MP_COUNT], 256, 0, st>>>(P.mem, P.table(MP_COUNT), eoff);
+  return 1;
+}
+
+int multi_collide_back(const MultiPlan& P, uint64_t eoff, bool resort, cudaStream_t st) {
+  km_perm<<<P.blocks[MP_PERM], 256, 0, st>>>(P.mem, P.table(MP_PERM));
+  km_tile<<<P.blocks[MP_TILE], 32 * kTileWarps, 0, st>>>(P.mem, P.table(MP_TILE), eoff);
+  if (!resort) return 2;
+  km_move<<<P.blocks[MP_MOVE], 256, 0, st>>>(P.mem, P.table(MP_MOVE), 0);
+  km_move<<<P.blocks[MP_MOVE], 256, 0, st>>>(P.mem, P.table(MP_MOVE), 1);
+  return 4;
+}
+
+// ---- the tables' sizes (host) -------------------------------------------------------
+void multi_blocks(const Member& M, int out[MP_NPHASE]) {
+  const DevParams& p = M.p;
+  const int64_t ns = M.f.n, nc = M.c.n;
+  out[MP_STREAM] = (int)nbf(ns, 256 * kMultiStreamPer);
+  out[MP_CELLS] = (int)M.fb.bcap + kOverflowBlocks;
+  out[MP_DRIFT] = (int)nb(p.nv, 128);
+  out[MP_AV] = (int)nb(p.nt, 128);
+  out[MP_SUM_EDGES] = 1 + (int)nb(2 * p.ne + p.nv, 256);
+  out[MP_FORCE_TRI] = (int)nb(p.nt, 128);
+  out[MP_GATHER] = (int)nb(p.nv, kGW);
+  out[MP_TAIL] = 1;
+  out[MP_KICK] = (int)nb(p.nv, 128);
+  out[MP_TRI_PREP] = (int)nb(p.nt, 128);
+  out[MP_ZERO] = (int)nb(nc, 256);
+  out[MP_VBIN] = 1;
+  out[MP_COUNT] = (int)nbf(ns, 256 * kCountPer);
+  out[MP_GHOST] = (int)nb(nc, 256);
+  out[MP_SCAN] = (int)scan_part_blocks(nc);
+  out[MP_SCAN_TOP] = 1;
+  out[MP_PERM] = (int)nbf(ns, 256);
+  out[MP_TILE] = (int)cells_tile_blocks(nc);
+  out[MP_MOVE] = (int)nbf(ns, 256);
+}
+
+void multi_smem(const Member& M, int out[3]) {
+  const DevParams& p = M.p;
+  out[0] = M.fb.hcap * (int)(sizeof(TriPre) + sizeof(int));
+  int n2 = 1;
+  while (n2 < p.nv) n2 <<= 1;
+  out[1] = (int)sizeof(uint64_t) * n2;
+  out[2] = p.nt <= kSumSmemT ? 2 * p.nt * (int)sizeof(double) : 0;
+}
+
+}  // namespace irbc

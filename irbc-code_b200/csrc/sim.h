@@ -82,6 +82,13 @@ struct Membrane {
   MemScalars* sc = nullptr;
 };
 
+// observables scratch (doubles): [0, 16) results and sums; from 64 the
+// velocity profile of irbc_velocity_profile (2 per bin); from kObsLayers the
+// per-layer sums of vx, vy, vz and the count behind the temperature
+constexpr int kObsMaxBins = 2048;
+constexpr int kObsLayers = 64 + 2 * kObsMaxBins;
+constexpr int kObsDoubles = kObsLayers + 4 * kObsMaxBins;
+
 constexpr int kMaxPairs = 64;        // bond candidates per vertex (<= 25 with dthr = 0.5)
 
 // ---- launchers (kernels.cu) ---------------------------------------------------
@@ -90,6 +97,8 @@ void launch_init_solvent(const DevParams& p, Solvent& s, cudaStream_t st);
 void launch_set_u64(uint64_t* d, uint64_t v, cudaStream_t st);
 // velocity records from / to plain arrays (state exchange); a null vx keeps
 // the velocities, a null id keeps the indices
+// d[i] = i for i < n
+void launch_iota(int* d, int64_t n, cudaStream_t st);
 void launch_pack_vel(Solvent& s, const double* vx, const double* vy, const double* vz, const int* id,
                      cudaStream_t st);
 void launch_unpack_vel(const Solvent& s, double* vx, double* vy, double* vz, int* id, cudaStream_t st);
@@ -125,8 +134,10 @@ void launch_bonds(const DevParams& p, Membrane& m, uint64_t epoch, cudaStream_t 
 void launch_kick2(const DevParams& p, Membrane& m, cudaStream_t st);
 void launch_scan3(const int* a, const int* b, const int* c, int* oa, int* ob, int* oc, int* totals,
                   int64_t n, int* part, cudaStream_t st);
-void launch_observables(const DevParams& p, const Solvent& s, const Membrane& m, double* out,
-                        double* prof, int nbins, cudaStream_t st);
+// obs: the kObsDoubles scratch; nbins > 0 also fills the velocity profile
+// (obs + 64, nbins <= kObsMaxBins)
+void launch_observables(const DevParams& p, const Solvent& s, const Membrane& m, double* obs, int nbins,
+                        cudaStream_t st);
 
 int64_t scan_part_blocks(int64_t n);
 

@@ -67,7 +67,8 @@ class View(C.Structure):
 
 class Schedule(C.Structure):
     """irbc_schedule: how a batch launches its members' steps."""
-    _fields_ = [("streams", C.c_int32), ("membrane", C.c_int32), ("graphs", C.c_int32), ("chunk", C.c_int32)]
+    _fields_ = [("streams", C.c_int32), ("membrane", C.c_int32), ("graphs", C.c_int32), ("chunk", C.c_int32),
+                ("fused", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -75,7 +76,9 @@ class Schedule(C.Structure):
 
 # int (*)(int32_t candidate, void* ctx, double* seconds)
 TUNE_MEASURE = C.CFUNCTYPE(C.c_int, C.c_int32, C.c_void_p, C.POINTER(C.c_double))
-ERR_ARG, ERR_CAPACITY = -1, -4
+ERR_ARG, ERR_CAPACITY, ERR_HEALTH = -1, -4, -6
+# bits of the health word (irbc_health)
+HEALTH_SOLVENT, HEALTH_MEMBRANE = 1, 2
 
 
 def tune_select(n, measure, repeats=3, margin=0.02):
@@ -154,6 +157,7 @@ def lib():
     L.irbc_write_rbcdata.argtypes = [H, C.c_char_p, C.c_int32]
     L.irbc_write_stl.argtypes = [H, C.c_char_p]
     L.irbc_observables.argtypes = [H, D, C.c_int32]
+    L.irbc_health.argtypes = [H, I]
     L.irbc_velocity_profile.argtypes = [H, D, C.c_int32]
     L.irbc_launch_count.restype = C.c_int64
     L.irbc_launch_count.argtypes = [H]
@@ -194,6 +198,7 @@ def lib():
     L.irbc_server_clock.restype = C.c_double
     L.irbc_server_clock.argtypes = [B]
     L.irbc_server_set_schedule.argtypes = [B, C.POINTER(Schedule)]
+    L.irbc_server_release.argtypes = [B, H]
     L.irbc_server_destroy.argtypes = [B]
     L.irbc_server_destroy.restype = None
     _lib = L
@@ -256,6 +261,9 @@ class State:
         for k in self.SCAL:
             self.s[k] = getattr(v, k)
 
+    def copy(self):
+        return State.from_other(self)
+
     @classmethod
     def from_other(cls, other):
         """Copies any object with .a/.s dicts and ns/nv/nlig/ncell (e.g. an oracle state)."""
@@ -281,10 +289,13 @@ class Simulation:
         self.nv = 0
 
     @classmethod
-    def adopt(cls, handle, params, nv):
-        """wraps a handle the library created (a server result with keep = 1)"""
+    def adopt(cls, handle, params, nv, server=None):
+        """wraps a handle the library created (a server result with keep = 1);
+        close() hands it back to `server` (irbc_server_release) while that
+        server is open"""
         sim = cls.__new__(cls)
         sim.L = lib()
+        sim._server = server
         sim.params = params
         sim.h = C.c_void_p(handle)
         sim.ncell = int(sim.L.irbc_ncell(sim.h))
@@ -294,7 +305,12 @@ class Simulation:
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:
-            self.L.irbc_destroy(self.h)
+            srv = getattr(self, "_server", None)
+            if srv is not None and srv.s.value:
+                if self.L.irbc_server_release(srv.s, self.h) != 0:
+                    self.L.irbc_destroy(self.h)
+            else:
+                self.L.irbc_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):
@@ -348,7 +364,7 @@ class Simulation:
         for k, arr in a.items():
             setattr(m, k, _p(arr, I if arr.dtype == np.int32 else D))
         self._ck(self.L.irbc_get_mesh(self.h, C.byref(m)), "irbc_get_mesh")
-        return a, {"Sarea0": m.Sarea0, "Volume0": m.Volume0, "theta0": m.theta0}
+        return a, {"Sarea0": m.Sarea0, "Volume0": m.Volume0, "theta0": m.theta0, "center": np.array(m.center[:])}
 
     def set_state(self, st):
         v = st.view()
@@ -367,6 +383,13 @@ class Simulation:
 
     def sync(self):
         self._ck(self.L.irbc_sync(self.h), "irbc_sync")
+
+    def health(self):
+        """the health word after the queued work (0: healthy; HEALTH_SOLVENT,
+        HEALTH_MEMBRANE bits)"""
+        f = C.c_int32(0)
+        self._ck(self.L.irbc_health(self.h, C.byref(f)), "irbc_health")
+        return f.value
 
     def call(self, name, *args):
         self._ck(getattr(self.L, "irbc_" + name)(self.h, *args), "irbc_" + name)
@@ -524,7 +547,7 @@ class Server:
                      t_end=r.t_end, obs=np.array(r.obs[:]), sim=None)
             if r.handle:
                 params, nv = self.params[r.id]
-                d["sim"] = Simulation.adopt(r.handle, params, nv)
+                d["sim"] = Simulation.adopt(r.handle, params, nv, server=self)
             out.append(d)
         return out
 
@@ -534,9 +557,9 @@ class Server:
         return dict(pending=out[0], active=out[1], results=out[2], used=out[3], budget=out[4],
                     particle_steps=out[5])
 
-    def set_schedule(self, streams=2, membrane=1, graphs=0, chunk=24):
+    def set_schedule(self, streams=2, membrane=1, graphs=0, chunk=24, fused=1):
         """Launch schedule for simulations admitted from now on."""
-        s = Schedule(streams, membrane, graphs, chunk)
+        s = Schedule(streams, membrane, graphs, chunk, fused)
         rc = self.L.irbc_server_set_schedule(self.s, C.byref(s))
         if rc != 0:
             raise IrbcError("irbc_server_set_schedule failed (%d)" % rc)

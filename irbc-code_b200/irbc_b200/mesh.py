@@ -71,14 +71,112 @@ def orient_outward(V, F):
     return F
 
 
-def discocyte(subdiv=4, R=4.0):
-    """(V, E, T): 2562 vertices / 7680 edges / 5120 triangles for subdiv=4.
-    Triangles are oriented on the sphere (where the test is exact) before
-    the mapping, which preserves orientation."""
+def _pole_rotation(v):
+    """rotation matrix taking the unit vector v to +z (Rodrigues)"""
+    z = np.array([0.0, 0.0, 1.0])
+    v = v / np.linalg.norm(v)
+    ax = np.cross(v, z)
+    s, c = np.linalg.norm(ax), float(v @ z)
+    if s < 1e-15:
+        return np.eye(3) if c > 0 else np.diag([1.0, -1.0, -1.0])
+    ax /= s
+    K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+    return np.eye(3) + s * K + (1 - c) * (K @ K)
+
+
+def _profile(theta, R):
+    """Evans-Fung profile as a closed curve in the (r, z) half-plane,
+    parameterised by the polar angle theta of the sphere point mapped there
+    (evans_fung): r = R sin(theta), z = +-h(r)"""
+    rho = np.sin(theta)
+    r2 = rho * rho
+    h = 0.5 * R * np.sqrt(np.clip(1.0 - r2, 0.0, 1.0)) * (EF_C0 + EF_C1 * r2 + EF_C2 * r2 * r2)
+    return R * rho, np.where(theta <= 0.5 * np.pi, h, -h)
+
+
+def _project(P, theta, R, newton=4, eps=1e-6):
+    """Nearest points of the discocyte surface to the points P: each keeps
+    its azimuth, and the profile parameter theta (started from its previous
+    value) takes a few damped Newton steps on the squared (r, z) distance.
+    Returns the surface points and their parameters."""
+    rp, zp, phi = np.hypot(P[:, 0], P[:, 1]), P[:, 2], np.arctan2(P[:, 1], P[:, 0])
+    for _ in range(newton):
+        d = []
+        for t in (theta - eps, theta, theta + eps):
+            r, z = _profile(t, R)
+            d.append((r - rp) ** 2 + (z - zp) ** 2)
+        g = (d[2] - d[0]) / (2 * eps)
+        hs = (d[2] - 2 * d[1] + d[0]) / (eps * eps)
+        step = np.where(hs > 0, -g / np.maximum(hs, 1e-30), -np.sign(g) * 1e-3)
+        theta = np.clip(theta + np.clip(step, -0.05, 0.05), 0.0, np.pi)
+    r, z = _profile(theta, R)
+    return np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=1), theta
+
+
+_cache = {}
+
+
+def discocyte(subdiv=4, R=4.0, relax_iters=1000, step=0.2):
+    """(V, E, T): 2562 vertices / 7680 edges / 5120 triangles for subdiv=4
+    (fresh copies of a per-process cache; see _discocyte)."""
+    key = (subdiv, R, relax_iters, step)
+    if key not in _cache:
+        _cache[key] = _discocyte(*key)
+    return tuple(a.copy() for a in _cache[key])
+
+
+def _discocyte(subdiv, R, relax_iters, step):
+    """The discocyte mesh.
+
+    The icosphere is turned so that one of its twelve 5-valent vertices sits
+    on the axis (the others then lie at +-26.6 deg latitude, away from the
+    rim), mapped onto the Evans-Fung surface (evans_fung), and relaxed on
+    that surface towards equal edge lengths: gradient steps on
+    sum (l - mean l)^2, each followed by projection back onto the surface
+    (_project).  The plain mapping crushes the rim (edges 0.15-0.35 at
+    R = 4, with 5-valent vertices on the rim); the relaxed mesh's edges
+    span 0.20-0.32 about a mean of 0.253.  Triangles are oriented on the
+    sphere (where the test is exact) before the mapping; neither the
+    mapping nor the relaxation turns a triangle over."""
     Vs, F = icosphere(subdiv)
+    Vs = Vs @ _pole_rotation(Vs[5]).T
     F = orient_outward(Vs, F)
+    theta = np.arccos(np.clip(Vs[:, 2], -1.0, 1.0))
     V = evans_fung(Vs, R)
-    return V, edges_of(F), F
+    E = edges_of(F)
+    n = len(V)
+    for _ in range(relax_iters):
+        d = V[E[:, 0]] - V[E[:, 1]]
+        ln = np.sqrt((d * d).sum(axis=1))
+        g = ((ln - ln.mean()) / ln)[:, None] * d
+        G = np.stack([np.bincount(E[:, 0], g[:, k], n) - np.bincount(E[:, 1], g[:, k], n) for k in range(3)],
+                     axis=1)
+        V, theta = _project(V - step * G, theta, R)
+    return V, E, F
+
+
+# The WLC spring of the reference's membrane model (Src/memfuncs.cpp:233-258)
+# has a fixed persistence constant elap = 0.0005 (maincode.cpp:347), chosen
+# for its shipped 600-vertex mesh, whose mean edge is 0.983753.  Its spring
+# force does not shrink with the edge, so on a finer mesh the tension per
+# unit length grows as 1 / (mean edge), and below an edge of about 0.35 the
+# POW coefficient kappap (maincode.cpp:349-360) turns negative: the edge
+# loses its repulsive core.  Coarse-graining the WLC-POW model (Fedosov,
+# Caswell and Karniadakis, Biophys. J. 98 (2010) 2215) keeps the membrane's
+# shear modulus by scaling the persistence length with the mesh, i.e.
+# elap x mean edge held at the shipped mesh's value.
+REF_ELAP, REF_MEAN_EDGE = 0.0005, 0.983753
+
+
+def mean_edge(V, E):
+    """mean edge length as main() prints it (maincode.cpp:239-257)"""
+    V, E = np.asarray(V, float), np.asarray(E)
+    return float(np.sqrt(((V[E[:, 0]] - V[E[:, 1]]) ** 2).sum(axis=1)).sum() / len(E))
+
+
+def scaled_elap(V, E):
+    """elap for a mesh: the reference's elap x (its mean edge / this mesh's)"""
+    return REF_ELAP * REF_MEAN_EDGE / mean_edge(V, E)
 
 
 def write_reference_files(folder, V, E, T, stem="Disc"):

@@ -10,8 +10,9 @@
 // the other define.h parameters are irbc_params_default(); the vertex count
 // is the vertex file's line count.  Not in the reference: IRBC_STEPS (total
 // steps, default the reference's 4,000,000), IRBC_OUT_EVERY (default 5000),
-// IRBC_SEED, IRBC_PRECISION (fp64 / fp32) and IRBC_DEVICE in the
-// environment.
+// IRBC_SEED, IRBC_NS (solvent particles, default define.h's Ns: the
+// reference's value is fixed at compile time), IRBC_PRECISION (fp64 /
+// fp32) and IRBC_DEVICE in the environment.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -68,6 +69,7 @@ int main(int argc, char** argv) {
   p.Nt = nv;
   p.seed = (uint64_t)env_i64("IRBC_SEED", (int64_t)p.seed);
   p.out_every = env_i64("IRBC_OUT_EVERY", p.out_every);
+  p.Ns = env_i64("IRBC_NS", p.Ns);
   p.device = (int32_t)env_i64("IRBC_DEVICE", 0);
   const char* prec = std::getenv("IRBC_PRECISION");
   if (prec && std::strcmp(prec, "fp32") == 0) p.precision = IRBC_FP32;

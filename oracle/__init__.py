@@ -13,7 +13,6 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_DIR = os.environ.get("IRBC_REFERENCE_DIR", "/root/reference")
 DATA_DIR = os.path.join(os.path.dirname(HERE), "tests", "golden", "troph600")
 
 D = C.POINTER(C.c_double)
@@ -154,13 +153,13 @@ def load_mesh_files(vfile, efile, tfile):
 
 
 def troph_files():
-    """The shipped 600-vertex trophozoite mesh (a copy is kept as a test
-    fixture in tests/golden/troph600 for machines without the reference)."""
+    """The shipped 600-vertex trophozoite mesh: the byte-identical copy kept
+    as a test fixture in tests/golden/troph600 (test_oracle_vs_ref.py checks
+    it against the reference's own files where the reference tree is)."""
     names = ("TrophV600.dat", "TrophE600.dat", "TrophT600.dat")
-    for d in (REFERENCE_DIR, DATA_DIR):
-        if all(os.path.exists(os.path.join(d, n)) for n in names):
-            return tuple(os.path.join(d, n) for n in names)
-    raise FileNotFoundError("trophozoite mesh files not found")
+    if all(os.path.exists(os.path.join(DATA_DIR, n)) for n in names):
+        return tuple(os.path.join(DATA_DIR, n) for n in names)
+    raise FileNotFoundError("trophozoite mesh files not found in " + DATA_DIR)
 
 
 # ------------------------------------------------------------------- oracle
@@ -340,16 +339,17 @@ class Reference:
         self.p = p
 
     def run(self, vfile, efile, tfile, nknobs, stop_step, seed, onrate=0.005, offrate=0.015,
-            on_step=None, fast_init=0, workdir=None):
+            on_step=None, fast_init=0, workdir=None, stl=0):
         """Runs main() until the TotalVA snapshot of step `stop_step`.
-        on_step(step) is called at each step's TotalVA point."""
+        on_step(step) is called at each step's TotalVA point; stl is main()'s
+        stl_flag argument (1: an rbc<k>.stl beside each RBCdata record)."""
         def cb(s):
             if on_step is not None:
                 on_step(int(s))
         self._cb = REF_CB(cb)
         wd = workdir or tempfile.mkdtemp(prefix="irbc_ref_")
         args = ["MAIN", repr(onrate), repr(offrate), os.path.abspath(vfile), os.path.abspath(efile),
-                os.path.abspath(tfile), str(nknobs), os.path.join(wd, "RBCdata.dat"), "0"]
+                os.path.abspath(tfile), str(nknobs), os.path.join(wd, "RBCdata.dat"), str(int(stl))]
         argv = (C.c_char_p * len(args))(*[a.encode() for a in args])
         self.p.onrate, self.p.offrate = onrate, offrate
         with _in_dir(wd):

@@ -45,6 +45,39 @@ def gpu_like(op, orc, seed, precision=0, state=None):
     return sim
 
 
+def oracle_params(p):
+    """oracle Params with the fields of the irbc_params p"""
+    op = O.default_params()
+    for name, _ in O.Params._fields_:
+        if name != "pad_":
+            setattr(op, name, getattr(p, name))
+    return op
+
+
+def oracle_like(sim, p):
+    """an oracle with the GPU simulation's parameters, mesh and state"""
+    op = oracle_params(p)
+    orc = O.Oracle(op, p.seed)
+    a, sc = sim.get_mesh_arrays()
+    M = O.MeshArrays(sim.nv, len(a["e1"]), len(a["t1"]))
+    for k in M.a:
+        M.a[k][:] = a[k]
+    M.s.update(sc)
+    orc.set_mesh(M)
+    orc.set_state(oracle_state(sim.get_state()))
+    return op, orc
+
+
+def oracle_state(st):
+    """an oracle State holding the arrays and scalars of a GPU state"""
+    ost = O.State(st.ns, st.nv, st.nlig, st.ncell, max(1, st.a["lidx"].size))
+    for k, v in st.a.items():
+        ost.a[k] = np.ascontiguousarray(v).copy()
+    for k, v in st.s.items():
+        ost.s[k] = np.array(v).copy() if isinstance(v, np.ndarray) else v
+    return ost
+
+
 def rel_err(a, b):
     """normwise relative error max|a-b| / max|b|"""
     a, b = np.asarray(a), np.asarray(b)

@@ -65,25 +65,33 @@ def test_server_results_same_alone_and_in_mix():
     fp = max(G.lib().irbc_footprint_bytes(G.C.byref(p), len(V), len(E), len(T)) for p, _, _ in reqs)
     srv = G.Server(budget_bytes=int(2.5 * fp), nthreads=2, round_steps=24)
     ids = {}
+    spans = []
+
+    def check(results):
+        # each kept result stays charged to the budget until it is handed
+        # back: compare it with the request run alone, then release it
+        for r in results:
+            assert r["status"] == 0
+            p, nk, steps = ids[r["id"]]
+            assert r["steps"] == steps
+            assert r["t_submit"] <= r["t_start"] <= r["t_end"]
+            spans.append((r["t_start"], r["t_end"]))
+            ref = _run_alone(p, V, E, T, nk, steps)
+            assert H.compare(r["sim"].get_state(), ref, 0.0) == {}, r["id"]
+            r["sim"].close()
+        return len(results)
+
     for p, nk, steps in reqs[:3]:
         ids[srv.submit(p, V, E, T, nk, steps, keep=True)] = (p, nk, steps)
-    got = srv.poll(8, wait=30.0)
+    got = check(srv.poll(8, wait=30.0))
     for p, nk, steps in reqs[3:]:
         ids[srv.submit(p, V, E, T, nk, steps, keep=True)] = (p, nk, steps)
-    while len(got) < len(reqs):
+    while got < len(reqs):
         more = srv.poll(8, wait=60.0)
         assert more, "server stalled"
-        got += more
-    spans = []
-    for r in got:
-        assert r["status"] == 0
-        p, nk, steps = ids[r["id"]]
-        assert r["steps"] == steps
-        assert r["t_submit"] <= r["t_start"] <= r["t_end"]
-        spans.append((r["t_start"], r["t_end"]))
-        ref = _run_alone(p, V, E, T, nk, steps)
-        assert H.compare(r["sim"].get_state(), ref, 0.0) == {}, r["id"]
-        r["sim"].close()
+        got += check(more)
+    st = srv.status()
+    assert st["used"] == 0 and st["active"] == 0, st
     # never more than two admitted at the same time
     for t, _ in spans:
         assert sum(1 for a, b in spans if a <= t < b) <= 2
@@ -126,3 +134,34 @@ def test_one_block_membrane_equals_wide_kernels(precision):
         out.append(s.get_state())
         s.close()
     assert H.compare(out[0], out[1], 0.0) == {}
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("which", ["troph", "disc"])
+def test_cluster_membrane_equals_wide_kernels(precision, which):
+    """The membrane step as one launch of a thread-block cluster (any mesh:
+    the 600-vertex trophozoite and the 2562-vertex discocyte) and the wide
+    kernels give the same state, bit for bit, across collisions, bond
+    events, list updates and captured graphs."""
+    import irbc_b200 as G
+    from irbc_b200 import mesh
+    if which == "troph":
+        V, E, T = H.troph()
+        _, p = _small(14, precision=precision, onrate=300.0, offrate=50.0)
+        nk = 300
+    else:
+        V, E, T = mesh.discocyte()
+        _, p = _small(15, precision=precision, onrate=300.0, offrate=50.0)
+        p.Nt, p.elap, nk = len(V), mesh.scaled_elap(V, E), 900
+    out = []
+    for mode, graphs in ((1, 0), (3, 0), (3, 1)):
+        s = G.Simulation(p)
+        s.init(V, E, T, nk)
+        s.set_membrane_kernels(mode)
+        s.set_graphs(graphs)
+        s.step(97)
+        s.step(80)
+        out.append(s.get_state())
+        s.close()
+    assert H.compare(out[1], out[0], 0.0) == {}
+    assert H.compare(out[2], out[0], 0.0) == {}

@@ -38,10 +38,10 @@ def test_autotuned_batch_equals_members_alone():
         sims.append(s)
         b.add(s)
     sched, taken = b.autotune(trial_steps=24, repeats=1)
-    # membrane, streams and graphs try two values each, chunk three; each
-    # candidate runs once untimed and once timed, all feasible for this
-    # 600-vertex mesh
-    assert taken == (2 + 2 + 2 + 3) * 2 * 24
+    # fused, membrane, streams and graphs try two values each, chunk three;
+    # each candidate runs once untimed and once timed, all feasible for
+    # this 600-vertex mesh
+    assert taken == (2 + 2 + 2 + 2 + 3) * 2 * 24
     assert sched == b.schedule()
     assert sched["streams"] in (1, 2) and sched["membrane"] in (1, 2) and sched["graphs"] in (0, 1)
     assert sched["chunk"] in (24, 96, 240)

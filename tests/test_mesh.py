@@ -40,13 +40,35 @@ def test_discocyte_topology_and_orientation():
     assert (len(V), len(E), len(T)) == (2562, 7680, 5120)
     assert (E[:, 0] < E[:, 1]).all()
     _closed_manifold(E, T, len(V))
-    # outward triangles enclose a positive volume (divergence theorem)
+    # every triangle outward, so they enclose a positive volume
+    assert (_outward(V, T) > 0).all()
     A, B, C = V[T[:, 0]], V[T[:, 1]], V[T[:, 2]]
     vol = np.einsum("ij,ij->i", A, np.cross(B, C)).sum() / 6.0
     assert vol > 0
-    # Evans-Fung shape of radius 4: diameter 8, thickness well below it
-    assert abs(V[:, 0].max() - 4.0) < 1e-9 and abs(V[:, 1].min() + 4.0) < 1e-9
+    # on the Evans-Fung surface of radius 4: |z| = h(r) at every vertex
+    r = np.hypot(V[:, 0], V[:, 1])
+    rho2 = np.clip((r / 4.0) ** 2, 0, 1)
+    h = 2.0 * np.sqrt(1 - rho2) * (mesh.EF_C0 + mesh.EF_C1 * rho2 + mesh.EF_C2 * rho2 ** 2)
+    assert np.max(np.abs(np.abs(V[:, 2]) - h)) < 1e-12
+    assert 3.99 < r.max() <= 4.0 + 1e-12
     assert 0.5 < V[:, 2].max() - V[:, 2].min() < 4.0
+
+
+def test_discocyte_edges_are_near_uniform():
+    """The relaxed mesh: edges within about +-25% of their mean (the plain
+    mapping of the icosphere spans 0.15-0.35), and none of the twelve
+    5-valent vertices on the rim."""
+    from irbc_b200 import mesh
+    V, E, T = mesh.discocyte()
+    ln = np.linalg.norm(V[E[:, 0]] - V[E[:, 1]], axis=1)
+    assert ln.min() > 0.75 * ln.mean() and ln.max() < 1.3 * ln.mean()
+    assert ln.std() < 0.1 * ln.mean()
+    valence = np.bincount(E.ravel())
+    assert (valence == 5).sum() == 12
+    assert np.hypot(V[valence == 5, 0], V[valence == 5, 1]).max() < 0.9 * 4.0
+    # the persistence constant scaled to the mesh keeps the shipped mesh's
+    # elap x mean edge
+    assert abs(mesh.scaled_elap(V, E) * mesh.mean_edge(V, E) - 0.0005 * 0.983753) < 1e-15
 
 
 def test_reference_file_round_trip(tmp_path):

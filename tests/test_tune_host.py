@@ -109,14 +109,14 @@ def test_argument_checks():
 
 def test_batch_schedule_defaults_and_checks():
     b = G.Batch(nthreads=2)
-    assert b.schedule() == dict(streams=2, membrane=1, graphs=0, chunk=24)
-    b.set_schedule(streams=1, graphs=1, chunk=96)
-    assert b.schedule() == dict(streams=1, membrane=1, graphs=1, chunk=96)
+    assert b.schedule() == dict(streams=2, membrane=1, graphs=0, chunk=24, fused=1)
+    b.set_schedule(streams=1, graphs=1, chunk=96, fused=0)
+    assert b.schedule() == dict(streams=1, membrane=1, graphs=1, chunk=96, fused=0)
     for bad in (dict(streams=3), dict(membrane=0), dict(graphs=2), dict(chunk=30), dict(chunk=0),
-                dict(chunk=2424)):
+                dict(chunk=2424), dict(fused=2)):
         with pytest.raises(G.IrbcError):
             b.set_schedule(**bad)
-        assert b.schedule() == dict(streams=1, membrane=1, graphs=1, chunk=96)
+        assert b.schedule() == dict(streams=1, membrane=1, graphs=1, chunk=96, fused=0)
     L = G.lib()
     s, taken = G.Schedule(), C.c_int64(0)
     # nothing to tune on: no members
