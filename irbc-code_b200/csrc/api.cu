@@ -117,6 +117,7 @@ void fill_devparams_from(const irbc_params& P, DevParams& d) {
   d.ny = (int)(P.Ly / P.a);
   d.nz = (int)(P.Lz / P.a) + 1;
   d.ncell = (int64_t)d.nx * d.ny * d.nz;
+  d.tree_sums = P.precision == IRBC_FP32 ? 1 : 0;
 }
 
 void fill_devparams(irbc_handle* h) { fill_devparams_from(h->P, h->dp); }

@@ -24,6 +24,9 @@ struct DevParams {
   const uint64_t* ebase;
   // run-time health word of the simulation (HEALTH_* bits), or null
   int* health;
+  // Sarea and Volume as a fixed warp tree instead of the reference's
+  // left-to-right sum (the FP32-bulk solvent, which claims no bit parity)
+  int tree_sums;
 };
 
 // Health bits, raised by the kernels that write the state and read back by

@@ -335,12 +335,11 @@ struct HeavyIO {
 };
 
 template <bool F32, class TriAt, class IdAt>
-__device__ __forceinline__ void heavy_particle(const DevParams& p, Solvent& s, SolventF& f, const Snap& sn,
-                                               int64_t i, int lane, int len, TriAt tri, IdAt ids) {
+__device__ __forceinline__ void heavy_particle_from(const DevParams& p, Solvent& s, SolventF& f, const Snap& sn,
+                                                    int64_t i, int lane, int len, TriAt tri, IdAt ids,
+                                                    const double st_in[6], int indio) {
   double st[6], st0[6];
-  int indio;
-  HeavyIO<F32>::load(s, f, i, st, indio);
-  for (int k = 0; k < 6; ++k) st0[k] = st[k];
+  for (int k = 0; k < 6; ++k) st0[k] = st[k] = st_in[k];
   double fulldt = 0.0;
   heavy_walk(p, sn, tri, ids, len, lane, indio, st[0], st[1], st[2], st[3], st[4], st[5], fulldt);
   if (lane == 0) {
@@ -348,6 +347,14 @@ __device__ __forceinline__ void heavy_particle(const DevParams& p, Solvent& s, S
     raise_health(p, solvent_bad(p, st[0], st[1], st[2], st[3], st[4], st[5]), HEALTH_SOLVENT);
     HeavyIO<F32>::store(s, f, i, st, st0);
   }
+}
+template <bool F32, class TriAt, class IdAt>
+__device__ __forceinline__ void heavy_particle(const DevParams& p, Solvent& s, SolventF& f, const Snap& sn,
+                                               int64_t i, int lane, int len, TriAt tri, IdAt ids) {
+  double st[6];
+  int indio;
+  HeavyIO<F32>::load(s, f, i, st, indio);
+  heavy_particle_from<F32>(p, s, f, sn, i, lane, len, tri, ids, st, indio);
 }
 
 // Particles in cells with triangles (reflectionFed, Src/solfuncs.cpp:400-598,
@@ -410,10 +417,25 @@ __device__ __forceinline__ void stream_cells_block(const DevParams& p, Solvent& 
     st[e] = pre[jj];
   }
   __syncthreads();
-  for (int q = w; q < n; q += nw) {
-    const int64_t i = bucket[(int64_t)a * kBucket + q];
-    heavy_particle<F32>(p, s, f, sn, i, lane, len, [&](int e) -> const TriPre& { return st[e]; },
-                        [&](int e) { return sj[e]; });
+  // this warp's particles are q = w, w + nw, ... (n <= kBucket = 32): lane
+  // j loads the j-th one's state, so all their loads are in flight at once;
+  // then the warp walks them one after another, each state broadcast from
+  // its lane
+  const int mine = n > w ? (n - w + nw - 1) / nw : 0;
+  int64_t pi = -1;
+  double pst[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  int pind = 0;
+  if (lane < mine) {
+    pi = bucket[(int64_t)a * kBucket + w + lane * nw];
+    HeavyIO<F32>::load(s, f, pi, pst, pind);
+  }
+  for (int k = 0; k < mine; ++k) {
+    const int64_t i = __shfl_sync(0xffffffffu, pi, k);
+    double sk[6];
+    for (int c = 0; c < 6; ++c) sk[c] = __shfl_sync(0xffffffffu, pst[c], k);
+    const int indio = __shfl_sync(0xffffffffu, pind, k);
+    heavy_particle_from<F32>(p, s, f, sn, i, lane, len, [&](int e) -> const TriPre& { return st[e]; },
+                             [&](int e) { return sj[e]; }, sk, indio);
   }
 }
 template <bool F32>
@@ -651,6 +673,35 @@ __device__ __forceinline__ double ordered_sum(const double* a, int n) {
   return t;
 }
 
+// Sum of a[0..n) by one warp in a fixed order: lane l adds its contiguous
+// run left to right, then the 32 partial sums meet in a butterfly; lane 0's
+// value is the result (the same for every launch and launch layout)
+__device__ __forceinline__ double warp_tree_sum(const double* a, int n, int lane) {
+  const int c = (n + 31) / 32;
+  const int b = min(lane * c, n), e = min(b + c, n);
+  double t = 0.0;
+  for (int i = b; i < e; ++i) t += a[i];
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  return __shfl_sync(0xffffffffu, t, 0);
+}
+
+// Sarea and Volume (TotalVA, Src/memfuncs.cpp:161-190) from the triangle
+// terms a[] and v[], by warp 0 (Sarea) and warp 1 (Volume) of the block:
+// the threads t < 64 call it.  Left to right in one thread, the
+// reference's order; or, with p.tree_sums, as a fixed warp tree.
+__device__ __forceinline__ void area_volume_sums(const DevParams& p, const Membrane& m, const double* a,
+                                                 const double* v, int t) {
+  const int lane = t & 31;
+  const double* src = t < 32 ? a : v;
+  double* out = t < 32 ? &m.sc->Sarea : &m.sc->Volume;
+  if (p.tree_sums) {
+    const double r = warp_tree_sum(src, p.nt, lane);
+    if (lane == 0) *out = r;
+  } else if (lane == 0) {
+    *out = ordered_sum(src, p.nt);
+  }
+}
+
 __global__ void __launch_bounds__(256) k_m_sum(DevParams p, Membrane m) {
   extern __shared__ double sh[];
   const bool staged = p.nt <= kSumSmemT;
@@ -660,8 +711,7 @@ __global__ void __launch_bounds__(256) k_m_sum(DevParams p, Membrane m) {
   }
   const double* a = staged ? sh : m.area;
   const double* v = staged ? sh + p.nt : m.vol;
-  if (threadIdx.x == 0) m.sc->Sarea = ordered_sum(a, p.nt);
-  else if (threadIdx.x == 32) m.sc->Volume = ordered_sum(v, p.nt);
+  if (threadIdx.x < 64) area_volume_sums(p, m, a, v, threadIdx.x);
 }
 
 // per vertex: bond preparation (maincode.cpp:668-723), the number of bond
@@ -742,8 +792,7 @@ __device__ __forceinline__ void sum_edges_block(const DevParams& p, Membrane& m,
     }
     const double* a = staged ? sh : m.area;
     const double* v = staged ? sh + p.nt : m.vol;
-    if (threadIdx.x == 0) m.sc->Sarea = ordered_sum(a, p.nt);
-    else if (threadIdx.x == 32) m.sc->Volume = ordered_sum(v, p.nt);
+    if (threadIdx.x < 64) area_volume_sums(p, m, a, v, threadIdx.x);
     return;
   }
   const int k = (bid - 1) * blockDim.x + threadIdx.x;  // 0 .. 2E + V
@@ -1125,11 +1174,10 @@ __global__ void __launch_bounds__(kBlockT) k_membrane_block(DevParams p, Membran
     shb[p.nt + i] = m.vol[i];
   }
   __syncthreads();
-  // warps 0 and 1: Sarea and Volume left to right; the others: edge and
+  // warps 0 and 1: Sarea and Volume (area_volume_sums); the others: edge and
   // bending terms and the bond preparation
-  if (t == 0) m.sc->Sarea = ordered_sum(shb, p.nt);
-  else if (t == 32) m.sc->Volume = ordered_sum(shb + p.nt, p.nt);
-  else if (t >= 64) {
+  if (t < 64) area_volume_sums(p, m, shb, shb + p.nt, t);
+  else {
     const int n = 2 * p.ne + p.nv;
     for (int k = t - 64; k < n; k += T - 64) {
       if (k < p.ne) force_item(p, m, f.slot, k);
@@ -1170,7 +1218,7 @@ __global__ void __launch_bounds__(kClusterT)
   cl.sync();
   for (int i = g; i < p.nt; i += G) m_av_item(p, m, i);
   cl.sync();
-  // block 0's warps 0 and 1: Sarea and Volume left to right, staged in its
+  // block 0's warps 0 and 1: Sarea and Volume (area_volume_sums), staged in its
   // shared memory when they fit; every other thread of the cluster: the
   // edge and bending terms and the bond preparation
   const bool staged = p.nt <= kSumSmemT;
@@ -1178,11 +1226,9 @@ __global__ void __launch_bounds__(kClusterT)
     for (int i = t; i < p.nt; i += T) { shc[i] = m.area[i]; shc[p.nt + i] = m.vol[i]; }
     __syncthreads();
   }
-  if (cta == 0 && t == 0) {
-    m.sc->Sarea = ordered_sum(staged ? shc : m.area, p.nt);
-  } else if (cta == 0 && t == 32) {
-    m.sc->Volume = ordered_sum(staged ? shc + p.nt : m.vol, p.nt);
-  } else if (g >= 64) {
+  if (cta == 0 && t < 64) {
+    area_volume_sums(p, m, staged ? shc : m.area, staged ? shc + p.nt : m.vol, t);
+  } else {
     const int n = 2 * p.ne + p.nv;
     for (int k = g - 64; k < n; k += G - 64) {
       if (k < p.ne) force_item(p, m, f.slot, k);

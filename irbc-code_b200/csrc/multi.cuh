@@ -19,7 +19,11 @@ __global__ void __launch_bounds__(256) km_stream_f(Member* __restrict__ mem, con
                   i0 + (int64_t)u * blockDim.x);
 }
 
-__global__ void __launch_bounds__(256) km_stream_cells(Member* __restrict__ mem, const int2* __restrict__ tab,
+// one warp per listed cell: a cohort's members are often small
+// simulations with many listed cells of short lists and about ten
+// particles each, where a cell's latency, not its work, sets the time
+constexpr int kCellsT = 32;
+__global__ void __launch_bounds__(kCellsT, 16) km_stream_cells(Member* __restrict__ mem, const int2* __restrict__ tab,
                                                        int par) {
   KM_MEMBER;
   // the overflow counter of the next step starts at zero
@@ -35,7 +39,7 @@ int multi_stream(const MultiPlan& P, int par, cudaStream_t st, cudaEvent_t snap)
                          kHeavyList * (int)(sizeof(TriPre) + sizeof(int)));
   km_stream_f<<<P.blocks[MP_STREAM], 256, 0, st>>>(P.mem, P.table(MP_STREAM), par);
   if (snap) cudaStreamWaitEvent(st, snap, 0);
-  km_stream_cells<<<P.blocks[MP_CELLS], 256, P.cells_smem, st>>>(P.mem, P.table(MP_CELLS), par);
+  km_stream_cells<<<P.blocks[MP_CELLS], kCellsT, P.cells_smem, st>>>(P.mem, P.table(MP_CELLS), par);
   return 2;
 }
 
