@@ -532,6 +532,9 @@ def run_served(G, nreq=40, rate=2.0, scale=0.02, nthreads=8, schedule=None):
     lat = np.array([by_id[i]["t_end"] - by_id[i]["t_submit"] for i in ids])
     arrive = np.array([by_id[i]["t_submit"] for i in ids])
     ok = int(sum(r["status"] == 0 for r in got))
+    statuses = {}
+    for r in got:
+        statuses[str(r["status"])] = statuses.get(str(r["status"]), 0) + 1
     work = sum(r["ns"] * r["steps"] for r in got if r["status"] == 0)
     # the plain path: every request alone, one after another
     alone, alone_ok = [], True
@@ -548,7 +551,7 @@ def run_served(G, nreq=40, rate=2.0, scale=0.02, nthreads=8, schedule=None):
     plain_lat = np.array(plain_lat)
     plain_span = done - arrive[0] if len(arrive) else float("nan")
     span = t1 - t0
-    return {"metric": "served sweep requests", "requests": nreq, "completed": ok,
+    return {"metric": "served sweep requests", "requests": nreq, "completed": ok, "statuses": statuses,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "sims_per_hour": 3600.0 * len(got) / span, "value": work / span, "unit": UNIT,
             "plain_alone_p50_s": float(np.percentile(alone, 50)), "plain_alone_p99_s": float(np.percentile(alone, 99)),
@@ -629,12 +632,23 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-batch", dest="batch", action="store_false")
     ap.add_argument("--no-serve", dest="serve", action="store_false")
+    # the batched or served leg alone (profiling runs)
+    ap.add_argument("--batch-only", action="store_true")
+    ap.add_argument("--serve-only", action="store_true")
+    ap.add_argument("--batch-replicas", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=240)
     args = ap.parse_args()
     # at least 3; and past the third collision, so the first 24-step graph
     # is captured before the timed steps
     args.warmup = max(args.warmup, 36)
     if args.impl == "reference":
         run_reference(args)
+    elif args.batch_only:
+        import irbc_b200 as G
+        print(json.dumps({"batched": run_batched(G, nrep=args.batch_replicas, steps=args.batch_steps)}))
+    elif args.serve_only:
+        import irbc_b200 as G
+        print(json.dumps({"served": run_served(G)}))
     else:
         run_ours(args)
 

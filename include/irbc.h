@@ -102,6 +102,8 @@ void irbc_params_default(irbc_params* p);              /* define.h:35-73 */
  * define.h:182-429 and the grid build of maincode.cpp:112-154. */
 int irbc_create(const irbc_params* p, irbc_handle** out);
 void irbc_destroy(irbc_handle* h);
+/* the message of h's last error; with h = NULL, why the calling thread's last
+ * irbc_create failed */
 const char* irbc_last_error(const irbc_handle* h);
 /* bytes of device memory a simulation with these parameters needs (for
  * admission by HBM footprint); nv/ne/nt are the mesh sizes */

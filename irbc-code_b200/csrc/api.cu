@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -26,6 +27,7 @@ std::atomic<int64_t> g_launches{0};
 }
 
 struct irbc_handle {
+  uint64_t uid = 0;        // unique for the life of the process (a freed handle's address can return)
   void* rec = nullptr;     // device staging of irbc_record_async
   irbc_params P{};
   DevParams dp{};
@@ -526,7 +528,16 @@ extern "C" int64_t irbc_footprint_bytes(const irbc_params* p, int32_t nv, int32_
   return b;
 }
 
+// why the calling thread's last irbc_create failed (irbc_last_error(NULL))
+static thread_local std::string g_create_err;
+static int create_failed(int code, const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  g_create_err = std::string("irbc_create: ") + what + (e != cudaSuccess ? std::string(": ") + cudaGetErrorString(e) : "");
+  return code;
+}
+
 extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
+  g_create_err.clear();
   irbc_handle* h = nullptr;
   if (!p || !out) return IRBC_ERR_ARG;
   *out = nullptr;
@@ -536,10 +547,17 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   int64_t nx = (int64_t)(p->Lx / p->a), ny = (int64_t)(p->Ly / p->a), nz = (int64_t)(p->Lz / p->a) + 1;
   if (nx * ny * nz >= (1LL << 31) || p->Ns >= (1LL << 31)) return IRBC_ERR_ARG;
   h = new irbc_handle();
+  {
+    static std::atomic<uint64_t> next_uid{1};
+    h->uid = next_uid.fetch_add(1);
+  }
   h->P = *p;
   cudaError_t e = cudaSetDevice(p->device);
-  if (e != cudaSuccess) { delete h; return IRBC_ERR_CUDA; }
-  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) { delete h; return IRBC_ERR_CUDA; }
+  if (e != cudaSuccess) { delete h; return create_failed(IRBC_ERR_CUDA, "cudaSetDevice"); }
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return create_failed(IRBC_ERR_CUDA, "stream");
+  }
   {
     // the membrane chain is latency bound: give its stream the higher priority
     int lo = 0, hi = 0;
@@ -553,6 +571,14 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
     for (cudaEvent_t* e : {&h->ev_snap, &h->ev_mem, &h->ev_coll, &h->ev_str[0], &h->ev_str[1], &h->ev_vbin,
                            &h->ev_health})
       cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+  }
+  {
+    // the kernels' shared-memory limits, before this simulation's first
+    // launch (and never racing another thread's launches)
+    static std::mutex limits_mu;
+    std::lock_guard<std::mutex> lk(limits_mu);
+    set_kernel_limits();
+    cudaGetLastError();
   }
   fill_devparams(h);
   build_ligands(h);
@@ -597,7 +623,7 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
     A(dalloc(&h->sf.pid, s.n));
     A(dalloc(&h->sf.pid2, s.n));
   }
-  if (rc) { irbc_destroy(h); return rc; }
+  if (rc) { irbc_destroy(h); return create_failed(rc, "device allocation"); }
   cudaMemsetAsync(c.lstart, 0, sizeof(int) * (c.n + 1), h->st);
   cudaMemsetAsync(h->m.ligi, 0, sizeof(int) * h->dp.nlig, h->st);
   cudaMemsetAsync(h->m.sc, 0, sizeof(MemScalars), h->st);
@@ -607,7 +633,7 @@ extern "C" int irbc_create(const irbc_params* p, irbc_handle** out) {
   cudaMemsetAsync(s.pid, 0, sizeof(int) * std::max<int64_t>(1, s.n), h->st);
   cudaMemcpyAsync(h->m.xlig, h->xlig.data(), sizeof(double) * h->dp.nlig, cudaMemcpyHostToDevice, h->st);
   cudaMemcpyAsync(h->m.ylig, h->ylig.data(), sizeof(double) * h->dp.nlig, cudaMemcpyHostToDevice, h->st);
-  if (cudaStreamSynchronize(h->st) != cudaSuccess) { irbc_destroy(h); return IRBC_ERR_CUDA; }
+  if (cudaStreamSynchronize(h->st) != cudaSuccess) { irbc_destroy(h); return create_failed(IRBC_ERR_CUDA, "set-up copies"); }
   // the vertex bitonic sort stages up to 8192 keys in dynamic shared memory
   h->launches0 = g_launches.load();
   *out = h;
@@ -649,7 +675,7 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   delete h;
 }
 
-extern "C" const char* irbc_last_error(const irbc_handle* h) { return h ? h->err.c_str() : "null handle"; }
+extern "C" const char* irbc_last_error(const irbc_handle* h) { return h ? h->err.c_str() : g_create_err.c_str(); }
 extern "C" int64_t irbc_ncell(const irbc_handle* h) { return h ? h->dp.ncell : -1; }
 extern "C" int32_t irbc_nlig(const irbc_handle* h) { return h ? h->dp.nlig : -1; }
 extern "C" int64_t irbc_launch_count(const irbc_handle* h) { return h ? launches_in(h) : -1; }
@@ -1014,8 +1040,11 @@ extern "C" int irbc_set_state(irbc_handle* h, const irbc_view* v) {
 
 extern "C" int64_t irbc_llist_total(irbc_handle* h) {
   if (!h) return IRBC_ERR_ARG;
+  cudaSetDevice(h->P.device);
   int t = 0;
-  if (cudaMemcpy(&t, h->c.lstart + h->c.n, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+  // on the handle's stream: after the list update that wrote the total
+  if (cudaMemcpyAsync(&t, h->c.lstart + h->c.n, sizeof(int), cudaMemcpyDeviceToHost, h->st) != cudaSuccess ||
+      cudaStreamSynchronize(h->st) != cudaSuccess)
     return IRBC_ERR_CUDA;
   return t;
 }
@@ -1455,6 +1484,7 @@ struct Cohort {
   cudaEvent_t ev_join = nullptr;
   MultiPlan plan;                       // device tables of `members`
   std::vector<irbc_handle*> members;    // the plan's members, in order
+  std::vector<uint64_t> uids;           // their handles' unique ids
   std::vector<Member> host;             // their descriptors as uploaded
   size_t cap = 0;                       // members the device tables have room for
   size_t tab_cap = 0;                   // block-table entries they have room for
@@ -1501,7 +1531,9 @@ int64_t cohort_key(const irbc_handle* h) {
 }
 
 static Member member_of(irbc_handle* h) {
+  // every byte defined (padding too), so that descriptors compare bytewise
   Member M;
+  std::memset(&M, 0, sizeof(M));
   M.p = h->dp;
   M.s = h->s;
   M.f = h->sf;
@@ -1511,6 +1543,8 @@ static Member member_of(irbc_handle* h) {
   // the staging capacity follows the longest list (as stream_any does for
   // plain launches)
   M.fb.hcap = heavy_cap(h->c.lmax);
+  // host-only counters that no kernel reads
+  M.s.ncoll = M.s.resorted = 0;
   return M;
 }
 
@@ -1523,11 +1557,13 @@ static int cohort_upload(Cohort* c) {
   MultiPlan& P = c->plan;
   P.n = (int)n;
   c->host.resize(n);
+  c->uids.resize(n);
   std::vector<std::array<int, MP_NPHASE>> nbk(n);
   int64_t tot[MP_NPHASE] = {};
   P.cells_smem = P.vbin_smem = P.sum_smem = 0;
   for (size_t r = 0; r < n; ++r) {
     c->host[r] = member_of(c->members[r]);
+    c->uids[r] = c->members[r]->uid;
     int sm[3];
     multi_blocks(c->host[r], nbk[r].data());
     multi_smem(c->host[r], sm);
@@ -1561,25 +1597,25 @@ static int cohort_upload(Cohort* c) {
         cudaMalloc((void**)&P.blk, c->tab_cap * sizeof(int2)) != cudaSuccess)
       return IRBC_ERR_CUDA;
   }
-  // staging memory: plain (pageable) copies, finished when the calls return
-  if (cudaMemcpy(P.mem, c->host.data(), n * sizeof(Member), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(P.blk, tab.data(), tab.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess)
+  // From pageable memory a copy returns once its data is staged, before it
+  // lands; a plain cudaMemcpy would land through the legacy stream, which
+  // the cohort's non-blocking streams do not follow.  So: queued on the
+  // cohort's own stream, and waited for, before any kernel reads the tables.
+  if (cudaMemcpyAsync(P.mem, c->host.data(), n * sizeof(Member), cudaMemcpyHostToDevice, c->ms) != cudaSuccess ||
+      cudaMemcpyAsync(P.blk, tab.data(), tab.size() * sizeof(int2), cudaMemcpyHostToDevice, c->ms) != cudaSuccess ||
+      cudaStreamSynchronize(c->ms) != cudaSuccess)
     return IRBC_ERR_CUDA;
   return 0;
 }
 
 // whether the uploaded descriptor of member r still describes its handle:
-// the fields that calls between steps can move (list updates and state
-// loads grow the lists and buckets, a new mesh moves the membrane arrays)
-// and the wall speed
+// the same handle (its unique id: a destroyed handle's address, and its
+// buffers' addresses, can come back for a new simulation of another size)
+// and every byte of the descriptor the same
 static bool member_current(const Cohort* c, size_t r) {
+  if (c->uids[r] != c->members[r]->uid) return false;
   const Member now = member_of(c->members[r]);
-  const Member& was = c->host[r];
-  return now.p.wallspeed == was.p.wallspeed && now.fb.hcap == was.fb.hcap && now.fb.bcap == was.fb.bcap &&
-         now.c.lidx == was.c.lidx && now.c.lstart == was.c.lstart && now.fb.bcnt == was.fb.bcnt &&
-         now.fb.bucket == was.fb.bucket && now.fb.border == was.fb.border && now.m.x == was.m.x &&
-         now.m.sc == was.m.sc && now.fb.slot == was.fb.slot && now.fb.pre[0] == was.fb.pre[0] &&
-         now.f.pos == was.f.pos && now.p.nv == was.p.nv && now.p.Sarea0 == was.p.Sarea0;
+  return std::memcmp(&now, &c->host[r], sizeof(Member)) == 0;
 }
 
 int cohort_step(Cohort* c, const std::vector<irbc_handle*>& all, int64_t n, std::vector<int>& status) {
@@ -1614,7 +1650,8 @@ int cohort_step(Cohort* c, const std::vector<irbc_handle*>& all, int64_t n, std:
     return IRBC_ERR_CUDA;
   // the device tables: rebuilt when the members changed or a member's
   // buffers, capacities or wall speed moved
-  bool stale = hs != c->members;
+  bool stale = hs.size() != c->members.size() || c->uids.size() != hs.size();
+  for (size_t r = 0; !stale && r < hs.size(); ++r) stale = hs[r] != c->members[r] || c->uids[r] != hs[r]->uid;
   for (size_t r = 0; !stale && r < hs.size(); ++r) stale = !member_current(c, r);
   if (stale) {
     c->members = hs;

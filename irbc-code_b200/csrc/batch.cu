@@ -411,6 +411,9 @@ struct irbc_server {
 namespace {
 // admits what fits, steps one round, retires what finished; returns false
 // when there is nothing to do
+template <class Finish>
+void step_active(irbc_server* s, const irbc_schedule& sched, Finish& finish);
+
 bool serve_round(irbc_server* s) {
   std::vector<Request> admit;
   irbc_schedule sched;
@@ -448,31 +451,58 @@ bool serve_round(irbc_server* s) {
     s->results.push_back(res);
     s->cv.notify_all();
   };
-  for (Request& r : admit) {
-    const double t_start = now_s(s->t0);
+  // The admitted requests are created and set up on the device (solvent
+  // draw, inside/outside ray test, lists, knobs) by threads of their own
+  // while the simulations admitted earlier take this round's steps, so that
+  // a new request's set-up does not stall the running ones.
+  struct Ready {
     irbc_handle* h = nullptr;
-    int rc = irbc_create(&r.p, &h);
-    if (!rc) rc = irbc_init(h, r.V.data(), (int32_t)(r.V.size() / 3), r.E.data(), (int32_t)(r.E.size() / 2),
-                            r.T.data(), (int32_t)(r.T.size() / 3), r.nknobs);
-    // the one-block membrane form only where the mesh fits it
-    if (!rc && scheduled && apply_schedule(h, sched)) {
-      irbc_schedule wide = sched;
-      wide.membrane = 1;
-      rc = apply_schedule(h, wide);
-    }
-    if (rc) {
-      finish(r, h, rc, t_start);
+    int rc = 0;
+    double t_start = 0;
+  };
+  std::vector<Ready> ready(admit.size());
+  std::vector<std::thread> setup;
+  for (size_t k = 0; k < admit.size(); ++k) {
+    setup.emplace_back([s, &admit, &ready, k, sched, scheduled] {
+      Request& r = admit[k];
+      Ready& out = ready[k];
+      out.t_start = now_s(s->t0);
+      int rc = irbc_create(&r.p, &out.h);
+      if (!rc)
+        rc = irbc_init(out.h, r.V.data(), (int32_t)(r.V.size() / 3), r.E.data(), (int32_t)(r.E.size() / 2),
+                       r.T.data(), (int32_t)(r.T.size() / 3), r.nknobs);
+      // the one-block membrane form only where the mesh fits it
+      if (!rc && scheduled && apply_schedule(out.h, sched)) {
+        irbc_schedule wide = sched;
+        wide.membrane = 1;
+        rc = apply_schedule(out.h, wide);
+      }
+      out.rc = rc;
+    });
+  }
+  const bool stepped = !s->active.empty();
+  if (stepped) step_active(s, sched, finish);
+  for (std::thread& th : setup) th.join();
+  for (size_t k = 0; k < admit.size(); ++k) {
+    if (ready[k].rc) {
+      finish(admit[k], ready[k].h, ready[k].rc, ready[k].t_start);
       continue;
     }
     Active a;
-    a.r = std::move(r);
-    a.h = h;
-    a.t_start = t_start;
+    a.r = std::move(admit[k]);
+    a.h = ready[k].h;
+    a.t_start = ready[k].t_start;
     std::lock_guard<std::mutex> lk(s->mu);
     s->active.push_back(std::move(a));
     s->n_active = (int64_t)s->active.size();
   }
-  if (s->active.empty()) return !admit.empty();
+  return stepped || !admit.empty();
+}
+
+// one round of steps for the admitted simulations; the ones that finish
+// (or fail) are retired through `finish`
+template <class Finish>
+void step_active(irbc_server* s, const irbc_schedule& sched, Finish& finish) {
   std::vector<irbc_handle*> hs;
   std::vector<int64_t> steps;
   for (const Active& a : s->active) {
@@ -502,7 +532,6 @@ bool serve_round(irbc_server* s) {
   std::lock_guard<std::mutex> lk(s->mu);
   s->active = std::move(still);
   s->n_active = (int64_t)s->active.size();
-  return true;
 }
 
 // whether the loop has work: simulations to step, or a pending request

@@ -398,25 +398,14 @@ __device__ __forceinline__ void stream_cells_block(const DevParams& p, Solvent& 
     }
     return;
   }
+  // Every thread reads the cell's bucket count and list bounds itself, so
+  // that the particle loads below go out beside the list's staging instead
+  // of after it.  The count is reset once everyone has read it (after the
+  // barrier); an empty bucket stays 0 and needs no reset.
   const int a = border[bid];
-  __shared__ int s_n;
-  if (threadIdx.x == 0) {
-    s_n = min(bcnt[a], kBucket);
-    bcnt[a] = 0;
-  }
-  __syncthreads();
-  const int n = s_n;
+  const int n = min(bcnt[a], kBucket);
   if (n == 0) return;
   const int c = acell[a];
-  const int l0 = lstart[c], len = lstart[c + 1] - l0;  // len <= hcap (hand_off)
-  TriPre* st = reinterpret_cast<TriPre*>(sh);
-  int* sj = reinterpret_cast<int*>(st + len);
-  for (int e = threadIdx.x; e < len; e += blockDim.x) {
-    const int jj = lidx[l0 + e];
-    sj[e] = jj;
-    st[e] = pre[jj];
-  }
-  __syncthreads();
   // this warp's particles are q = w, w + nw, ... (n <= kBucket = 32): lane
   // j loads the j-th one's state, so all their loads are in flight at once;
   // then the warp walks them one after another, each state broadcast from
@@ -429,6 +418,16 @@ __device__ __forceinline__ void stream_cells_block(const DevParams& p, Solvent& 
     pi = bucket[(int64_t)a * kBucket + w + lane * nw];
     HeavyIO<F32>::load(s, f, pi, pst, pind);
   }
+  const int l0 = lstart[c], len = lstart[c + 1] - l0;  // len <= hcap (hand_off)
+  TriPre* st = reinterpret_cast<TriPre*>(sh);
+  int* sj = reinterpret_cast<int*>(st + len);
+  for (int e = threadIdx.x; e < len; e += blockDim.x) {
+    const int jj = lidx[l0 + e];
+    sj[e] = jj;
+    st[e] = pre[jj];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) bcnt[a] = 0;
   for (int k = 0; k < mine; ++k) {
     const int64_t i = __shfl_sync(0xffffffffu, pi, k);
     double sk[6];
@@ -1078,14 +1077,6 @@ void launch_rank_lengths(const Cells& c, int* len, cudaStream_t st) {
   if (c.nact > 0) k_rank_lengths<<<nb(c.nact, 256), 256, 0, st>>>(c, c.nact, len);
 }
 
-bool first_on_device(int key) {
-  static std::atomic<uint64_t> done[8] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || key < 0 || key >= 8) return true;
-  const uint64_t bit = 1ull << dev;
-  return (done[key].fetch_or(bit) & bit) == 0;
-}
-
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st) {
   k_snap<<<nb(p.nv, 128), 128, 0, st>>>(p, m, f.snap[buf]);
   k_tri_prep<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.pre[buf]);
@@ -1108,15 +1099,18 @@ int fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaSt
   return 2;
 }
 
+// lists up to this many entries are walked by one-warp blocks
+constexpr int kShortList = 128;
 template <bool F32>
 static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
                                 cudaStream_t st) {
+  // (the limit for the largest staging: set_kernel_limits)
   const int smem = f.hcap * (int)(sizeof(TriPre) + sizeof(int));
-  // the limit for the largest staging, once per device
-  if (first_on_device(F32 ? 1 : 0))
-    cudaFuncSetAttribute(k_stream_cells<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kHeavyList * (int)(sizeof(TriPre) + sizeof(int)));
-  k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, 256, smem, st>>>(
+  // short lists (small simulations: many listed cells of a few dozen
+  // entries, ~10 particles each): one warp per cell, so that many cells are
+  // in flight per SM; long lists: eight warps share a cell's staging
+  const int threads = f.hcap <= kShortList ? 32 : 256;
+  k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, threads, smem, st>>>(
       p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
       c.totals + 4, f.border);
 }
@@ -1135,19 +1129,9 @@ void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, in
   }
 }
 
-static void set_sum_attrs() {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_m_sum, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kSumSmemT * sizeof(double));
-    cudaFuncSetAttribute(k_sum_edges, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kSumSmemT * sizeof(double));
-    attr = true;
-  }
-}
-
 // drift and the per-triangle TotalVA terms; with_sum also forms Sarea and
 // Volume (otherwise fast_forces_tail does, beside the edge terms)
 int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_sum) {
-  set_sum_attrs();
   k_m_drift<<<nb(p.nv, 128), 128, 0, st>>>(p, m);
   k_m_av<<<nb(p.nt, 128), 128, 0, st>>>(p, m);
   if (!with_sum) return 2;
@@ -1270,8 +1254,6 @@ int fast_membrane_step(const DevParams& p, Membrane& m, FastBufs& f, uint64_t ep
   if (f.cluster) {
     // the snapshot the kick writes was read by the previous streaming
     if (next_kick && readers) cudaStreamWaitEvent(st, readers, 0);
-    if (first_on_device(7))
-      cudaFuncSetAttribute(k_membrane_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     // one cluster of kClusterCTAs blocks
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(kClusterCTAs);
@@ -1291,9 +1273,6 @@ int fast_membrane_step(const DevParams& p, Membrane& m, FastBufs& f, uint64_t ep
   if (!f.one_block)
     return fast_drift_va(p, m, st, false) + fast_forces_tail(p, m, f, epoch, next_kick, next_buf, st, true, readers);
   const size_t smem = block_smem(p);
-  // the limit for the largest mesh this kernel takes, once per device
-  if (first_on_device(2))
-    cudaFuncSetAttribute(k_membrane_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   k_membrane_block<<<1, kBlockT, smem, st>>>(p, m, f, epoch);
   int n = 1;
   if (next_kick) {
@@ -1305,7 +1284,6 @@ int fast_membrane_step(const DevParams& p, Membrane& m, FastBufs& f, uint64_t ep
 
 int fast_forces_tail(const DevParams& p, Membrane& m, FastBufs& f, uint64_t epoch, int next_kick, int next_buf,
                      cudaStream_t st, bool sum_pending, cudaEvent_t readers) {
-  set_sum_attrs();
   const size_t sm = (sum_pending && p.nt <= kSumSmemT) ? 2 * (size_t)p.nt * sizeof(double) : 0;
   k_sum_edges<<<1 + nb(2 * p.ne + p.nv, 256), 256, sm, st>>>(p, m, f.slot, sum_pending ? 1 : 0, f.vd, f.vw, f.vX);
   k_force_tri<<<nb(p.nt, 128), 128, 0, st>>>(p, m, f.slot);

@@ -74,5 +74,8 @@ int fast_membrane_step(const DevParams& p, Membrane& m, FastBufs& f, uint64_t ep
                        cudaStream_t st, cudaEvent_t readers = nullptr);
 // whether a mesh suits the one-block membrane step
 bool one_block_fits(const DevParams& p);
+// every kernel's dynamic shared-memory limit on the current device (before
+// any launch; irbc_create calls it)
+void set_kernel_limits();
 
 }  // namespace irbc

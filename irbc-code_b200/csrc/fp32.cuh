@@ -136,17 +136,21 @@ void launch_resort_f(SolventF& f, Solvent& s, cudaStream_t st) {
 // ---- streaming ------------------------------------------------------------------
 // free flight, walls and wrap in float (maincode.cpp:516-560); particles in
 // cells with triangles are handed to k_stream_cells<true> (double precision)
-__device__ __forceinline__ void stream_f_item(const DevParams& p, const SolventF& f, const int* __restrict__ lstart,
-                                              const int* __restrict__ lrank, int* bcnt, int* bucket, int* queue,
-                                              int* qn, int hcap, int64_t i) {
-  if (i >= f.n) return;
-  const float Lx = (float)p.Lx, Ly = (float)p.Ly, Lz = (float)p.Lz, dt = (float)p.dtmd;
-  float4 q = f.pos[i], v = f.vel[i];
+// the shifted-free cell of a position (the list lookup of the streaming)
+__device__ __forceinline__ int stream_cell_f(const DevParams& p, float4 q, float Lx, float Ly) {
   int fx = (int)floorf(bbound(q.x, Lx));
   int fy = (int)floorf(bbound(q.y, Ly));
   int fz = (int)floorf(q.z + 1.0f);
-  int pid = cell_of(p, fx, fy, fz);
-  const int l0 = __ldg(lstart + pid), l1 = __ldg(lstart + pid + 1);
+  return cell_of(p, fx, fy, fz);
+}
+
+// free flight, walls and wrap of particle i, loaded as (q, v), whose cell
+// pid has the list [l0, l1): particles in cells with triangles are handed
+// to k_stream_cells<true> (double precision)
+__device__ __forceinline__ void stream_f_apply(const DevParams& p, const SolventF& f, const int* __restrict__ lrank,
+                                               int* bcnt, int* bucket, int* queue, int* qn, int hcap, int64_t i,
+                                               float4 q, float4 v, int pid, int l0, int l1) {
+  const float Lx = (float)p.Lx, Ly = (float)p.Ly, Lz = (float)p.Lz, dt = (float)p.dtmd;
   if (l1 > l0) {
     hand_off(lrank, pid, l1 - l0, hcap, (int)i, bcnt, bucket, queue, qn);
     return;
@@ -169,6 +173,17 @@ __device__ __forceinline__ void stream_f_item(const DevParams& p, const SolventF
   raise_health(p, solvent_bad(p, X, Y, Z, v.x, v.y, v.z), HEALTH_SOLVENT);
   f.pos[i] = make_float4(X, Y, Z, q.w);
 }
+
+__device__ __forceinline__ void stream_f_item(const DevParams& p, const SolventF& f, const int* __restrict__ lstart,
+                                              const int* __restrict__ lrank, int* bcnt, int* bucket, int* queue,
+                                              int* qn, int hcap, int64_t i) {
+  if (i >= f.n) return;
+  const float4 q = f.pos[i], v = f.vel[i];
+  const int pid = stream_cell_f(p, q, (float)p.Lx, (float)p.Ly);
+  const int l0 = __ldg(lstart + pid), l1 = __ldg(lstart + pid + 1);
+  stream_f_apply(p, f, lrank, bcnt, bucket, queue, qn, hcap, i, q, v, pid, l0, l1);
+}
+
 __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const int* __restrict__ lstart,
                                                   const int* __restrict__ lrank, int* bcnt, int* bucket,
                                                   int* queue, int* qn, int hcap) {

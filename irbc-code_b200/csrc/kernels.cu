@@ -438,8 +438,6 @@ __global__ void k_copy_back(Solvent s) {
 void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cudaStream_t st) {
   int n2 = 1;
   while (n2 < p.nv) n2 <<= 1;
-  if (first_on_device(3))
-    cudaFuncSetAttribute(k_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
   cudaMemsetAsync(c.ncm, 0, sizeof(int) * c.n, st);
   k_vbin<<<1, 1024, sizeof(uint64_t) * n2, st>>>(p, m, c.ncm, epoch);
 }
@@ -1297,9 +1295,12 @@ __global__ void __launch_bounds__(kScanT) km_scan_final(Member* __restrict__ mem
   scan_final_block(M.c.cnt, M.c.wrank, M.c.mrank, M.c.start, M.c.wrank, M.c.mrank, M.c.n, M.c.scan_part, b);
 }
 
+void set_collide_kernel_limits() {
+  cudaFuncSetAttribute(k_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
+  cudaFuncSetAttribute(km_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
+}
+
 int multi_collide_front(const MultiPlan& P, uint64_t eoff, cudaStream_t st) {
-  if (first_on_device(4))
-    cudaFuncSetAttribute(km_vbin, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * sizeof(uint64_t));
   km_zero<<<P.blocks[MP_ZERO], 256, 0, st>>>(P.mem, P.table(MP_ZERO));
   km_vbin<<<P.blocks[MP_VBIN], 1024, P.vbin_smem, st>>>(P.mem, P.table(MP_VBIN), eoff);
   return 2;

@@ -12,18 +12,39 @@ __global__ void __launch_bounds__(256) km_stream_f(Member* __restrict__ mem, con
                                                    int par) {
   KM_MEMBER;
   const DevParams& p = M.p;
-  const int64_t i0 = (int64_t)b * blockDim.x * kMultiStreamPer + threadIdx.x;
+  const SolventF& f = M.f;
+  const int* __restrict__ lstart = M.c.lstart;
+  const int64_t n = f.n, i0 = (int64_t)b * blockDim.x * kMultiStreamPer + threadIdx.x;
+  const float Lx = (float)p.Lx, Ly = (float)p.Ly;
+  // every load of the thread's particles first, then their cells' list
+  // bounds, then the updates: the latencies overlap
+  constexpr int K = kMultiStreamPer;
+  float4 q[K], v[K];
+  int pid[K], l0[K], l1[K];
 #pragma unroll
-  for (int u = 0; u < kMultiStreamPer; ++u)
-    stream_f_item(p, M.f, M.c.lstart, M.c.lrank, M.fb.bcnt, M.fb.bucket, M.fb.queue, M.fb.qn + par, M.fb.hcap,
-                  i0 + (int64_t)u * blockDim.x);
+  for (int u = 0; u < K; ++u) {
+    const int64_t i = i0 + (int64_t)u * blockDim.x;
+    if (i < n) { q[u] = f.pos[i]; v[u] = f.vel[i]; }
+  }
+#pragma unroll
+  for (int u = 0; u < K; ++u) {
+    const int64_t i = i0 + (int64_t)u * blockDim.x;
+    if (i < n) {
+      pid[u] = stream_cell_f(p, q[u], Lx, Ly);
+      l0[u] = __ldg(lstart + pid[u]);
+      l1[u] = __ldg(lstart + pid[u] + 1);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < K; ++u) {
+    const int64_t i = i0 + (int64_t)u * blockDim.x;
+    if (i < n)
+      stream_f_apply(p, f, M.c.lrank, M.fb.bcnt, M.fb.bucket, M.fb.queue, M.fb.qn + par, M.fb.hcap, i, q[u], v[u],
+                     pid[u], l0[u], l1[u]);
+  }
 }
 
-// one warp per listed cell: a cohort's members are often small
-// simulations with many listed cells of short lists and about ten
-// particles each, where a cell's latency, not its work, sets the time
-constexpr int kCellsT = 32;
-__global__ void __launch_bounds__(kCellsT, 16) km_stream_cells(Member* __restrict__ mem, const int2* __restrict__ tab,
+__global__ void __launch_bounds__(256) km_stream_cells(Member* __restrict__ mem, const int2* __restrict__ tab,
                                                        int par) {
   KM_MEMBER;
   // the overflow counter of the next step starts at zero
@@ -34,12 +55,13 @@ __global__ void __launch_bounds__(kCellsT, 16) km_stream_cells(Member* __restric
 }
 
 int multi_stream(const MultiPlan& P, int par, cudaStream_t st, cudaEvent_t snap) {
-  if (first_on_device(5))
-    cudaFuncSetAttribute(km_stream_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kHeavyList * (int)(sizeof(TriPre) + sizeof(int)));
   km_stream_f<<<P.blocks[MP_STREAM], 256, 0, st>>>(P.mem, P.table(MP_STREAM), par);
   if (snap) cudaStreamWaitEvent(st, snap, 0);
-  km_stream_cells<<<P.blocks[MP_CELLS], kCellsT, P.cells_smem, st>>>(P.mem, P.table(MP_CELLS), par);
+  // as the plain launch (launch_stream_cells): one warp per listed cell
+  // when every member's lists are short, eight warps per cell otherwise
+  const int longest = P.cells_smem / (int)(sizeof(TriPre) + sizeof(int));
+  const int threads = longest <= kShortList ? 32 : 256;
+  km_stream_cells<<<P.blocks[MP_CELLS], threads, P.cells_smem, st>>>(P.mem, P.table(MP_CELLS), par);
   return 2;
 }
 
@@ -73,8 +95,6 @@ __global__ void __launch_bounds__(kTailT) km_tail(Member* __restrict__ mem, cons
 }
 
 int multi_membrane(const MultiPlan& P, uint64_t eoff, cudaStream_t st) {
-  if (first_on_device(6))
-    cudaFuncSetAttribute(km_sum_edges, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kSumSmemT * sizeof(double));
   km_drift<<<P.blocks[MP_DRIFT], 128, 0, st>>>(P.mem, P.table(MP_DRIFT));
   km_av<<<P.blocks[MP_AV], 128, 0, st>>>(P.mem, P.table(MP_AV));
   km_sum_edges<<<P.blocks[MP_SUM_EDGES], 256, P.sum_smem, st>>>(P.mem, P.table(MP_SUM_EDGES));
@@ -136,6 +156,27 @@ int multi_collide_back(const MultiPlan& P, uint64_t eoff, bool resort, cudaStrea
   km_move<<<P.blocks[MP_MOVE], 256, 0, st>>>(P.mem, P.table(MP_MOVE), 0);
   km_move<<<P.blocks[MP_MOVE], 256, 0, st>>>(P.mem, P.table(MP_MOVE), 1);
   return 4;
+}
+
+// ---- kernel limits (host) ---------------------------------------------------------------
+// Every kernel's dynamic shared-memory limit on the current device, set
+// before any launch: irbc_create calls this for each new simulation, so a
+// launch issued by one host thread never races another thread's first-
+// launch attribute call (the request server sets new simulations up on
+// threads of their own while others step).
+void set_kernel_limits() {
+  const int cells = kHeavyList * (int)(sizeof(TriPre) + sizeof(int));
+  const int sums = 2 * kSumSmemT * (int)sizeof(double);
+  const auto dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaFuncSetAttribute(k_stream_cells<true>, dyn, cells);
+  cudaFuncSetAttribute(k_stream_cells<false>, dyn, cells);
+  cudaFuncSetAttribute(km_stream_cells, dyn, cells);
+  cudaFuncSetAttribute(k_m_sum, dyn, sums);
+  cudaFuncSetAttribute(k_sum_edges, dyn, sums);
+  cudaFuncSetAttribute(km_sum_edges, dyn, sums);
+  cudaFuncSetAttribute(k_membrane_block, dyn, 96 * 1024);
+  cudaFuncSetAttribute(k_membrane_cluster, dyn, 200 * 1024);
+  set_collide_kernel_limits();
 }
 
 // ---- the tables' sizes (host) -------------------------------------------------------

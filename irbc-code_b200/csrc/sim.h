@@ -106,9 +106,8 @@ void launch_unpermute(const Solvent& s, int velocities, int* bad, cudaStream_t s
 void launch_classify(const DevParams& p, Solvent& s, const Membrane& m, cudaStream_t st);
 // a collision = launch_vbin (membrane only) + launch_collide_count (solvent
 // only) in any order or on two streams, then launch_collide_finish
-// true the first time it is called for (key, current device): for settings
-// such as a kernel's shared-memory limit that persist per device
-bool first_on_device(int key);
+// the shared-memory limits of the collision kernels on the current device
+void set_collide_kernel_limits();
 void launch_vbin(const DevParams& p, Membrane& m, Cells& c, uint64_t epoch, cudaStream_t st);
 void launch_collide_count(const DevParams& p, Solvent& s, Cells& c, uint64_t epoch, cudaStream_t st);
 // resort: also re-sort the arrays physically by this collision's cells

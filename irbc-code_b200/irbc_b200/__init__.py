@@ -283,7 +283,8 @@ class Simulation:
         self.h = C.c_void_p()
         rc = self.L.irbc_create(C.byref(params), C.byref(self.h))
         if rc != 0:
-            raise IrbcError("irbc_create failed (%d): no CUDA device or bad parameters" % rc)
+            why = self.L.irbc_last_error(None)
+            raise IrbcError("irbc_create failed (%d): %s" % (rc, why.decode() if why else "bad parameters"))
         self.ncell = int(self.L.irbc_ncell(self.h))
         self.nlig = int(self.L.irbc_nlig(self.h))
         self.nv = 0
