@@ -1684,6 +1684,11 @@ int cohort_step(Cohort* c, const std::vector<irbc_handle*>& all, int64_t n, std:
         h->colsteps = 0;
         h->snap_ready = false;
       }
+      // the vertex binning reads the positions, and the tiles rotate the
+      // vertex velocities, of the previous step's membrane step (side
+      // stream): the collision waits for it (step_one bins on the side
+      // stream for the same reason)
+      if (cudaStreamWaitEvent(ms, c->ev_mem, 0) != cudaSuccess) return IRBC_ERR_CUDA;
       launched += multi_collide_front(c->plan, (uint64_t)k, ms);
       launched += multi_collide_count(c->plan, (uint64_t)k, ms);
       launched += multi_collide_scan(c->plan, ms);
