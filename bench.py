@@ -530,6 +530,8 @@ def run_served(G, nreq=40, rate=2.0, scale=0.02, nthreads=8, schedule=None):
     by_id = {r["id"]: r for r in got}
     ids = sorted(by_id)
     lat = np.array([by_id[i]["t_end"] - by_id[i]["t_submit"] for i in ids])
+    wait = np.array([by_id[i]["t_start"] - by_id[i]["t_submit"] for i in ids])
+    service = np.array([by_id[i]["t_end"] - by_id[i]["t_start"] for i in ids])
     arrive = np.array([by_id[i]["t_submit"] for i in ids])
     ok = int(sum(r["status"] == 0 for r in got))
     statuses = {}
@@ -553,6 +555,8 @@ def run_served(G, nreq=40, rate=2.0, scale=0.02, nthreads=8, schedule=None):
     span = t1 - t0
     return {"metric": "served sweep requests", "requests": nreq, "completed": ok, "statuses": statuses,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "admission_wait_p50_s": float(np.percentile(wait, 50)),
+            "service_p50_s": float(np.percentile(service, 50)),
             "sims_per_hour": 3600.0 * len(got) / span, "value": work / span, "unit": UNIT,
             "plain_alone_p50_s": float(np.percentile(alone, 50)), "plain_alone_p99_s": float(np.percentile(alone, 99)),
             "plain_p50_s": float(np.percentile(plain_lat, 50)), "plain_p99_s": float(np.percentile(plain_lat, 99)),

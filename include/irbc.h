@@ -273,8 +273,9 @@ int irbc_batch_step(irbc_batch* b, int64_t n);
  *   graphs    irbc_set_graphs for every member (0 or 1; default 0)
  *   chunk     steps a pool thread issues to one member before it turns to
  *             its next member (a multiple of 24 in 24..2400; default 24)
- *   fused     1 (the default): FP32 members in the same phase (created or
- *             admitted together, stepped together) advance as one cohort,
+ *   fused     1 (a batch's default; the server's default is 0): FP32
+ *             members in the same phase (created or admitted together,
+ *             stepped together) advance as one cohort,
  *             each phase of the step ONE kernel launch over all of them,
  *             its blocks split among the members; streams, membrane and
  *             graphs then apply only to the other members (FP64, or out of
@@ -316,12 +317,14 @@ int irbc_tune_select(int32_t n, irbc_tune_measure measure, void* ctx, int32_t re
 int irbc_batch_autotune(irbc_batch* b, int64_t trial_steps, int32_t repeats, double margin, irbc_schedule* best,
                         int64_t* steps_taken);
 /* The server takes whole simulations as requests: parameters, mesh, knob
- * count and step count.  Its loop admits a pending request when its
- * footprint (irbc_footprint_bytes) fits in the device-memory budget
- * (budget_bytes <= 0: 85% of the free memory at creation), creates and
- * initialises it, and advances every admitted simulation in rounds of
- * round_steps steps with a pool of nthreads host threads; requests that
- * arrive meanwhile join at the next round.  A finished simulation yields an
+ * count and step count.  A pending request is admitted, in arrival order,
+ * as soon as its footprint (irbc_footprint_bytes) fits in the device-memory
+ * budget (budget_bytes <= 0: 85% of the free memory at creation); two
+ * set-up threads create and initialise admitted requests on the device
+ * while the stepping loop advances every set-up simulation in rounds of
+ * round_steps steps (a pool of nthreads host threads, or cohorts under a
+ * fused schedule); a request set up during a round joins at the next one.
+ * A finished simulation yields an
  * irbc_result: its times on the server clock (seconds since creation), its
  * observables (irbc_observables) and, when submitted with keep = 1, its
  * handle; otherwise the server frees it.  A kept handle's device memory
@@ -356,9 +359,9 @@ int32_t irbc_server_poll(irbc_server* s, irbc_result* out, int32_t max, double w
 int irbc_server_status(irbc_server* s, int64_t out[6]);
 double irbc_server_clock(irbc_server* s);
 /* the launch schedule (irbc_schedule) for simulations admitted from now on
- * and for the rounds' issue chunk; membrane = 2 applies only to meshes that
- * fit the one-block form, the others keep the wide kernels.  Results do not
- * depend on it. */
+ * and for the rounds' issue chunk (default {2, 1, 0, 24, 0}: the pool);
+ * membrane = 2 applies only to meshes that fit the one-block form, the
+ * others keep the wide kernels.  Results do not depend on it. */
 int irbc_server_set_schedule(irbc_server* s, const irbc_schedule* sched);
 /* destroys a kept handle (a polled result of a keep = 1 request) and frees
  * its share of the budget; IRBC_ERR_ARG for a handle the server did not hand

@@ -1560,17 +1560,23 @@ static int cohort_upload(Cohort* c) {
   c->uids.resize(n);
   std::vector<std::array<int, MP_NPHASE>> nbk(n);
   int64_t tot[MP_NPHASE] = {};
-  P.cells_smem = P.vbin_smem = P.sum_smem = 0;
+  P.vbin_smem = P.sum_smem = 0;
+  P.cells_short = 0;
+  P.cells_cap[0] = P.cells_cap[1] = 1;
+  std::vector<int> cls(n);  // the near-membrane class of each member: 0 one-warp blocks, 1 eight-warp
   for (size_t r = 0; r < n; ++r) {
     c->host[r] = member_of(c->members[r]);
     c->uids[r] = c->members[r]->uid;
-    int sm[3];
+    int sm[2];
     multi_blocks(c->host[r], nbk[r].data());
     multi_smem(c->host[r], sm);
     for (int k = 0; k < MP_NPHASE; ++k) tot[k] += nbk[r][k];
-    P.cells_smem = std::max(P.cells_smem, sm[0]);
-    P.vbin_smem = std::max(P.vbin_smem, sm[1]);
-    P.sum_smem = std::max(P.sum_smem, sm[2]);
+    const int hcap = c->host[r].fb.hcap;
+    cls[r] = stage_threads(hcap) == 32 ? 0 : 1;
+    if (cls[r] == 0) P.cells_short += nbk[r][MP_CELLS];
+    P.cells_cap[cls[r]] = std::max(P.cells_cap[cls[r]], stage_cap(hcap));
+    P.vbin_smem = std::max(P.vbin_smem, sm[0]);
+    P.sum_smem = std::max(P.sum_smem, sm[1]);
   }
   // the block tables: phase by phase, member by member
   int64_t all = 0;
@@ -1583,8 +1589,12 @@ static int cohort_upload(Cohort* c) {
   std::vector<int2> tab((size_t)all);
   for (int k = 0; k < MP_NPHASE; ++k) {
     int64_t q = P.off[k];
-    for (size_t r = 0; r < n; ++r)
-      for (int b = 0; b < nbk[r][k]; ++b) tab[(size_t)q++] = make_int2((int)r, b);
+    // the near-membrane blocks class by class (one launch per class)
+    for (int pass = 0; pass < (k == MP_CELLS ? 2 : 1); ++pass)
+      for (size_t r = 0; r < n; ++r) {
+        if (k == MP_CELLS && cls[r] != pass) continue;
+        for (int b = 0; b < nbk[r][k]; ++b) tab[(size_t)q++] = make_int2((int)r, b);
+      }
   }
   if (n > c->cap || (size_t)all > c->tab_cap) {
     if (P.mem) cudaFree(P.mem);

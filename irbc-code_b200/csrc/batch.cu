@@ -387,15 +387,28 @@ struct irbc_server {
   int64_t budget = 0, used = 0;
   int64_t round = 240;
   int32_t max_active = 256;
-  irbc_schedule sched{2, 1, 0, 24, 1};  // for simulations admitted from now on
+  // for simulations admitted from now on; the pool by default: requests
+  // differ in box, mesh and list lengths, and a cohort's phases wait for
+  // its slowest member where the pool's streams overlap them
+  irbc_schedule sched{2, 1, 0, 24, 0};
   bool scheduled = false;                // set explicitly: applied at admission
   StepPool pool;
   std::vector<irbc::Cohort*> cohorts;    // fused schedules: one per group of simulations
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   std::mutex mu;
   std::condition_variable cv;
-  std::deque<Request> pending;
-  std::vector<Active> active;
+  std::deque<Request> pending;  // waiting for room in the budget
+  // set up (created and initialised on the device), waiting for the next
+  // round; a failed set-up carries its error
+  struct Ready {
+    Request r;
+    irbc_handle* h = nullptr;
+    int rc = 0;
+    double t_start = 0;
+  };
+  std::deque<Ready> ready;
+  int32_t setting_up = 0;       // requests in the hands of the set-up threads
+  std::vector<Active> active;   // owned by the stepping loop
   std::deque<irbc_result> results;
   // finished simulations handed out with keep = 1: their memory stays
   // charged to the budget until irbc_server_release
@@ -405,104 +418,91 @@ struct irbc_server {
   int64_t particle_steps = 0;
   bool stop = false;
   std::thread loop;
+  std::vector<std::thread> setup;
   explicit irbc_server(int nthreads) : pool(nthreads) {}
 };
 
 namespace {
-// admits what fits, steps one round, retires what finished; returns false
-// when there is nothing to do
-template <class Finish>
-void step_active(irbc_server* s, const irbc_schedule& sched, Finish& finish);
+constexpr int kSetupThreads = 2;
 
-bool serve_round(irbc_server* s) {
-  std::vector<Request> admit;
-  irbc_schedule sched;
-  bool scheduled;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    sched = s->sched;
-    scheduled = s->scheduled;
-    while (!s->pending.empty() && (int32_t)(s->active.size() + admit.size()) < s->max_active &&
-           s->used + s->pending.front().footprint <= s->budget) {
-      s->used += s->pending.front().footprint;
-      admit.push_back(std::move(s->pending.front()));
+// a result for request r (under no lock); h is destroyed unless it is
+// handed out
+void finish_request(irbc_server* s, const Request& r, irbc_handle* h, int32_t status, double t_start) {
+  irbc_result res{};
+  res.id = r.id;
+  res.status = status;
+  res.steps = r.nsteps;
+  res.ns = r.p.Ns;
+  res.t_submit = r.t_submit;
+  res.t_start = t_start;
+  res.t_end = now_s(s->t0);
+  if (h && status == 0) irbc_observables(h, res.obs, 8);
+  const bool hand_out = h && r.keep && status == 0;
+  if (hand_out) {
+    res.handle = h;
+  } else if (h) {
+    irbc_destroy(h);
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (hand_out) s->kept.push_back({h, r.footprint});
+  else s->used -= r.footprint;
+  s->results.push_back(res);
+  s->cv.notify_all();
+}
+
+// whether the head of the queue can be admitted now (under s->mu)
+bool can_admit(const irbc_server* s) {
+  return !s->pending.empty() && s->used + s->pending.front().footprint <= s->budget &&
+         s->n_active + (int64_t)s->ready.size() + s->setting_up < s->max_active;
+}
+
+// A set-up thread: admits the head of the queue as soon as the budget has
+// room for it, creates and initialises it on the device (solvent draw,
+// inside/outside ray test, lists, knobs) while the admitted simulations go
+// on stepping, and hands it to the stepping loop for its next round.
+void setup_loop(irbc_server* s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    Request r;
+    irbc_schedule sched;
+    bool scheduled;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv.wait(lk, [s] { return s->stop || can_admit(s); });
+      if (s->stop) return;
+      r = std::move(s->pending.front());
       s->pending.pop_front();
+      s->used += r.footprint;
+      s->setting_up += 1;
+      sched = s->sched;
+      scheduled = s->scheduled;
     }
-  }
-  auto finish = [s](const Request& r, irbc_handle* h, int32_t status, double t_start) {
-    irbc_result res{};
-    res.id = r.id;
-    res.status = status;
-    res.steps = r.nsteps;
-    res.ns = r.p.Ns;
-    res.t_submit = r.t_submit;
-    res.t_start = t_start;
-    res.t_end = now_s(s->t0);
-    if (h && status == 0) irbc_observables(h, res.obs, 8);
-    const bool hand_out = h && r.keep && status == 0;
-    if (hand_out) {
-      res.handle = h;
-    } else if (h) {
-      irbc_destroy(h);
+    irbc_server::Ready out;
+    out.t_start = now_s(s->t0);
+    int rc = irbc_create(&r.p, &out.h);
+    if (!rc)
+      rc = irbc_init(out.h, r.V.data(), (int32_t)(r.V.size() / 3), r.E.data(), (int32_t)(r.E.size() / 2),
+                     r.T.data(), (int32_t)(r.T.size() / 3), r.nknobs);
+    // the one-block membrane form only where the mesh fits it
+    if (!rc && scheduled && apply_schedule(out.h, sched)) {
+      irbc_schedule wide = sched;
+      wide.membrane = 1;
+      rc = apply_schedule(out.h, wide);
     }
+    // its set-up work is done before it joins a round
+    if (!rc) rc = irbc_sync(out.h);
+    out.rc = rc;
+    out.r = std::move(r);
     std::lock_guard<std::mutex> lk(s->mu);
-    if (hand_out) s->kept.push_back({h, r.footprint});
-    else s->used -= r.footprint;
-    s->results.push_back(res);
+    s->ready.push_back(std::move(out));
+    s->setting_up -= 1;
     s->cv.notify_all();
-  };
-  // The admitted requests are created and set up on the device (solvent
-  // draw, inside/outside ray test, lists, knobs) by threads of their own
-  // while the simulations admitted earlier take this round's steps, so that
-  // a new request's set-up does not stall the running ones.
-  struct Ready {
-    irbc_handle* h = nullptr;
-    int rc = 0;
-    double t_start = 0;
-  };
-  std::vector<Ready> ready(admit.size());
-  std::vector<std::thread> setup;
-  for (size_t k = 0; k < admit.size(); ++k) {
-    setup.emplace_back([s, &admit, &ready, k, sched, scheduled] {
-      Request& r = admit[k];
-      Ready& out = ready[k];
-      out.t_start = now_s(s->t0);
-      int rc = irbc_create(&r.p, &out.h);
-      if (!rc)
-        rc = irbc_init(out.h, r.V.data(), (int32_t)(r.V.size() / 3), r.E.data(), (int32_t)(r.E.size() / 2),
-                       r.T.data(), (int32_t)(r.T.size() / 3), r.nknobs);
-      // the one-block membrane form only where the mesh fits it
-      if (!rc && scheduled && apply_schedule(out.h, sched)) {
-        irbc_schedule wide = sched;
-        wide.membrane = 1;
-        rc = apply_schedule(out.h, wide);
-      }
-      out.rc = rc;
-    });
   }
-  const bool stepped = !s->active.empty();
-  if (stepped) step_active(s, sched, finish);
-  for (std::thread& th : setup) th.join();
-  for (size_t k = 0; k < admit.size(); ++k) {
-    if (ready[k].rc) {
-      finish(admit[k], ready[k].h, ready[k].rc, ready[k].t_start);
-      continue;
-    }
-    Active a;
-    a.r = std::move(admit[k]);
-    a.h = ready[k].h;
-    a.t_start = ready[k].t_start;
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->active.push_back(std::move(a));
-    s->n_active = (int64_t)s->active.size();
-  }
-  return stepped || !admit.empty();
 }
 
 // one round of steps for the admitted simulations; the ones that finish
-// (or fail) are retired through `finish`
-template <class Finish>
-void step_active(irbc_server* s, const irbc_schedule& sched, Finish& finish) {
+// (or fail) are retired
+void step_active(irbc_server* s, const irbc_schedule& sched) {
   std::vector<irbc_handle*> hs;
   std::vector<int64_t> steps;
   for (const Active& a : s->active) {
@@ -514,41 +514,53 @@ void step_active(irbc_server* s, const irbc_schedule& sched, Finish& finish) {
   std::vector<int> status;
   step_members(s->pool, s->cohorts, hs, steps, sched, status);
   std::vector<Active> still;
-  std::vector<size_t> done;
+  int64_t work = 0;
   for (size_t i = 0; i < s->active.size(); ++i) {
     Active& a = s->active[i];
     a.done += steps[i];
-    {
-      std::lock_guard<std::mutex> lk(s->mu);
-      s->particle_steps += steps[i] * a.r.p.Ns;
-    }
-    if (status[i] || a.done >= a.r.nsteps) done.push_back(i);
-  }
-  for (size_t i : done) finish(s->active[i].r, s->active[i].h, status[i], s->active[i].t_start);
-  for (size_t i = 0, d = 0; i < s->active.size(); ++i) {
-    if (d < done.size() && done[d] == i) { ++d; continue; }
-    still.push_back(std::move(s->active[i]));
+    work += steps[i] * a.r.p.Ns;
+    if (status[i] || a.done >= a.r.nsteps) finish_request(s, a.r, a.h, status[i], a.t_start);
+    else still.push_back(std::move(a));
   }
   std::lock_guard<std::mutex> lk(s->mu);
+  s->particle_steps += work;
   s->active = std::move(still);
   s->n_active = (int64_t)s->active.size();
+  s->cv.notify_all();  // room under max_active
 }
 
-// whether the loop has work: simulations to step, or a pending request
-// that fits the budget now (under s->mu)
-bool has_work(const irbc_server* s) {
-  return !s->active.empty() || (!s->pending.empty() && s->used + s->pending.front().footprint <= s->budget);
-}
-
+// The stepping loop: at each round boundary the simulations set up since
+// the last one join; then every admitted simulation takes the round's steps.
 void serve_loop(irbc_server* s) {
   cudaSetDevice(s->device);
   for (;;) {
+    std::deque<irbc_server::Ready> joined;
+    irbc_schedule sched;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv.wait(lk, [s] { return s->stop || has_work(s); });
+      s->cv.wait(lk, [s] { return s->stop || !s->active.empty() || !s->ready.empty(); });
       if (s->stop) break;
+      joined.swap(s->ready);
+      sched = s->sched;
     }
-    serve_round(s);
+    for (irbc_server::Ready& q : joined) {
+      if (q.rc) {
+        finish_request(s, q.r, q.h, q.rc, q.t_start);
+        continue;
+      }
+      Active a;
+      a.r = std::move(q.r);
+      a.h = q.h;
+      a.t_start = q.t_start;
+      if (a.r.nsteps == 0) {
+        finish_request(s, a.r, a.h, 0, a.t_start);
+        continue;
+      }
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->active.push_back(std::move(a));
+      s->n_active = (int64_t)s->active.size();
+    }
+    if (!s->active.empty()) step_active(s, sched);
   }
   for (Active& a : s->active) irbc_destroy(a.h);
   for (irbc::Cohort* c : s->cohorts) irbc::cohort_destroy(c);
@@ -573,6 +585,7 @@ extern "C" int irbc_server_create(int32_t device, int64_t budget_bytes, int32_t 
   s->budget = budget_bytes;
   s->round = round_steps;
   s->loop = std::thread(serve_loop, s);
+  for (int k = 0; k < kSetupThreads; ++k) s->setup.emplace_back(setup_loop, s);
   *out = s;
   return 0;
 }
@@ -662,6 +675,10 @@ extern "C" void irbc_server_destroy(irbc_server* s) {
   }
   s->cv.notify_all();
   s->loop.join();
+  for (std::thread& th : s->setup) th.join();
+  // set up but never stepped
+  for (irbc_server::Ready& q : s->ready)
+    if (q.h) irbc_destroy(q.h);
   // handles of results never polled were never handed out
   for (irbc_result& r : s->results)
     if (r.handle) irbc_destroy(r.handle);

@@ -278,11 +278,13 @@ __device__ __forceinline__ bool tri_crossing(const DevParams& p, const TriPre& q
 // the sequential loop.  Inside the periodic stencil bands every entry gets
 // the full test (its shifted corners are not precomputed).  tri(e) gives the
 // TriPre of list entry e, jj(e) its triangle.
+// The walk covers entries [cur, end) and leaves cur at or past end, so a
+// list can be walked in consecutive pieces with the same result.
 template <class TriAt, class IdAt>
-__device__ __forceinline__ void heavy_walk(const DevParams& p, const Snap& sn, TriAt tri, IdAt jj, int len, int lane,
+__device__ __forceinline__ void heavy_walk(const DevParams& p, const Snap& sn, TriAt tri, IdAt jj, int end, int lane,
                                            int indio, double& X, double& Y, double& Z, double& VX, double& VY,
-                                           double& VZ, double& fulldt) {
-  int cur = 0;
+                                           double& VZ, double& fulldt, int& cur) {
+  const int len = end;
   while (cur < len) {
     const bool pre = !in_stencil(p, X, Y);
     const int e = cur + lane;
@@ -341,7 +343,8 @@ __device__ __forceinline__ void heavy_particle_from(const DevParams& p, Solvent&
   double st[6], st0[6];
   for (int k = 0; k < 6; ++k) st0[k] = st[k] = st_in[k];
   double fulldt = 0.0;
-  heavy_walk(p, sn, tri, ids, len, lane, indio, st[0], st[1], st[2], st[3], st[4], st[5], fulldt);
+  int cur = 0;
+  heavy_walk(p, sn, tri, ids, len, lane, indio, st[0], st[1], st[2], st[3], st[4], st[5], fulldt, cur);
   if (lane == 0) {
     finish_stream(p, fulldt, st[0], st[1], st[2], st[3], st[4], st[5]);
     raise_health(p, solvent_bad(p, st[0], st[1], st[2], st[3], st[4], st[5]), HEALTH_SOLVENT);
@@ -375,7 +378,7 @@ __device__ __forceinline__ void stream_cells_block(const DevParams& p, Solvent& 
                                                    const int* __restrict__ bucket, const Snap& sn,
                                                    const TriPre* __restrict__ pre, const int* queue, const int* qn,
                                                    const int* __restrict__ nactp, const int* __restrict__ border,
-                                                   int bid, int nblk) {
+                                                   int bid, int nblk, int cap) {
   extern __shared__ double sh[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int nact = *nactp;
@@ -401,40 +404,61 @@ __device__ __forceinline__ void stream_cells_block(const DevParams& p, Solvent& 
   // Every thread reads the cell's bucket count and list bounds itself, so
   // that the particle loads below go out beside the list's staging instead
   // of after it.  The count is reset once everyone has read it (after the
-  // barrier); an empty bucket stays 0 and needs no reset.
+  // first barrier); an empty bucket stays 0 and needs no reset.
   const int a = border[bid];
   const int n = min(bcnt[a], kBucket);
   if (n == 0) return;
   const int c = acell[a];
   // this warp's particles are q = w, w + nw, ... (n <= kBucket = 32): lane
-  // j loads the j-th one's state, so all their loads are in flight at once;
-  // then the warp walks them one after another, each state broadcast from
-  // its lane
+  // j loads the j-th one's state and keeps its walk state (position,
+  // velocity, time spent, list cursor) between the pieces of the list
   const int mine = n > w ? (n - w + nw - 1) / nw : 0;
   int64_t pi = -1;
-  double pst[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  int pind = 0;
+  double pst[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, p0[6], pfd = 0.0;
+  int pind = 0, pcur = 0;
   if (lane < mine) {
     pi = bucket[(int64_t)a * kBucket + w + lane * nw];
     HeavyIO<F32>::load(s, f, pi, pst, pind);
   }
+  for (int k = 0; k < 6; ++k) p0[k] = pst[k];
   const int l0 = lstart[c], len = lstart[c + 1] - l0;  // len <= hcap (hand_off)
+  // the list in pieces of `cap` entries (the shared staging): every
+  // particle walks a piece before the next is staged, so each walk still
+  // visits the entries in list order
   TriPre* st = reinterpret_cast<TriPre*>(sh);
-  int* sj = reinterpret_cast<int*>(st + len);
-  for (int e = threadIdx.x; e < len; e += blockDim.x) {
-    const int jj = lidx[l0 + e];
-    sj[e] = jj;
-    st[e] = pre[jj];
+  int* sj = reinterpret_cast<int*>(st + cap);
+  for (int c0 = 0; c0 == 0 || c0 < len; c0 += cap) {
+    const int c1 = min(len, c0 + cap);
+    if (c0 > 0) __syncthreads();  // the previous piece's walks are done
+    for (int e = threadIdx.x; e < c1 - c0; e += blockDim.x) {
+      const int jj = lidx[l0 + c0 + e];
+      sj[e] = jj;
+      st[e] = pre[jj];
+    }
+    __syncthreads();
+    if (c0 == 0 && threadIdx.x == 0) bcnt[a] = 0;
+    for (int k = 0; k < mine; ++k) {
+      int cur = __shfl_sync(0xffffffffu, pcur, k);
+      if (cur >= c1) continue;  // warp-uniform
+      double X = __shfl_sync(0xffffffffu, pst[0], k), Y = __shfl_sync(0xffffffffu, pst[1], k);
+      double Z = __shfl_sync(0xffffffffu, pst[2], k), VX = __shfl_sync(0xffffffffu, pst[3], k);
+      double VY = __shfl_sync(0xffffffffu, pst[4], k), VZ = __shfl_sync(0xffffffffu, pst[5], k);
+      double fd = __shfl_sync(0xffffffffu, pfd, k);
+      const int indio = __shfl_sync(0xffffffffu, pind, k);
+      heavy_walk(p, sn, [&](int e) -> const TriPre& { return st[e - c0]; }, [&](int e) { return sj[e - c0]; }, c1,
+                 lane, indio, X, Y, Z, VX, VY, VZ, fd, cur);
+      if (lane == k) {
+        pst[0] = X; pst[1] = Y; pst[2] = Z; pst[3] = VX; pst[4] = VY; pst[5] = VZ;
+        pfd = fd;
+        pcur = cur;
+      }
+    }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) bcnt[a] = 0;
-  for (int k = 0; k < mine; ++k) {
-    const int64_t i = __shfl_sync(0xffffffffu, pi, k);
-    double sk[6];
-    for (int c = 0; c < 6; ++c) sk[c] = __shfl_sync(0xffffffffu, pst[c], k);
-    const int indio = __shfl_sync(0xffffffffu, pind, k);
-    heavy_particle_from<F32>(p, s, f, sn, i, lane, len, [&](int e) -> const TriPre& { return st[e]; },
-                             [&](int e) { return sj[e]; }, sk, indio);
+  // each lane ends its own particle: walls, wrap, health, write-back
+  if (lane < mine) {
+    finish_stream(p, pfd, pst[0], pst[1], pst[2], pst[3], pst[4], pst[5]);
+    raise_health(p, solvent_bad(p, pst[0], pst[1], pst[2], pst[3], pst[4], pst[5]), HEALTH_SOLVENT);
+    HeavyIO<F32>::store(s, f, pi, pst, p0);
   }
 }
 template <bool F32>
@@ -444,9 +468,9 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
                                                       const int* __restrict__ bucket, Snap sn,
                                                       const TriPre* __restrict__ pre, const int* queue,
                                                       const int* qn, const int* __restrict__ nactp,
-                                                      const int* __restrict__ border) {
+                                                      const int* __restrict__ border, int cap) {
   stream_cells_block<F32>(p, s, f, lstart, lidx, acell, bcnt, bucket, sn, pre, queue, qn, nactp, border,
-                          (int)blockIdx.x, (int)gridDim.x);
+                          (int)blockIdx.x, (int)gridDim.x, cap);
 }
 
 // ========================================================= membrane step ====
@@ -1099,20 +1123,18 @@ int fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaSt
   return 2;
 }
 
-// lists up to this many entries are walked by one-warp blocks
-constexpr int kShortList = 128;
 template <bool F32>
 static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
                                 cudaStream_t st) {
-  // (the limit for the largest staging: set_kernel_limits)
-  const int smem = f.hcap * (int)(sizeof(TriPre) + sizeof(int));
   // short lists (small simulations: many listed cells of a few dozen
   // entries, ~10 particles each): one warp per cell, so that many cells are
-  // in flight per SM; long lists: eight warps share a cell's staging
-  const int threads = f.hcap <= kShortList ? 32 : 256;
-  k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, threads, smem, st>>>(
+  // in flight per SM; long lists: eight warps share a cell's staging.  The
+  // staging holds a piece of the list at a time (stage_cap), so its size
+  // does not grow with the longest list.
+  const int cap = stage_cap(f.hcap);
+  k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, stage_threads(f.hcap), stage_bytes(cap), st>>>(
       p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
-      c.totals + 4, f.border);
+      c.totals + 4, f.border, cap);
 }
 
 void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,

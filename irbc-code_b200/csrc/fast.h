@@ -21,6 +21,19 @@ struct Snap {
 constexpr int kBucket = 32;
 constexpr int kHeavyList = 1024;
 constexpr int kOverflowBlocks = 8;
+// The near-membrane kernel stages a listed cell's TriPre records in shared
+// memory a piece at a time: one-warp blocks for staging capacities up to
+// kShortList entries (kStageShort entries per piece), eight-warp blocks
+// above (kStageLong per piece).  The kernel's registers allow two
+// eight-warp blocks per SM, which a whole 1024-entry list per block also
+// allows, so a bucketed list (at most kHeavyList entries) is one piece.
+constexpr int kShortList = 128, kStageShort = 128, kStageLong = kHeavyList;
+inline int stage_threads(int hcap) { return hcap <= kShortList ? 32 : 256; }
+inline int stage_cap(int hcap) {
+  const int c = hcap <= kShortList ? kStageShort : kStageLong;
+  return hcap < c ? (hcap > 0 ? hcap : 1) : c;
+}
+inline int stage_bytes(int cap) { return cap * (int)(sizeof(TriPre) + sizeof(int)); }
 
 struct FastBufs {
   Snap snap[2];

@@ -44,25 +44,34 @@ __global__ void __launch_bounds__(256) km_stream_f(Member* __restrict__ mem, con
   }
 }
 
-__global__ void __launch_bounds__(256) km_stream_cells(Member* __restrict__ mem, const int2* __restrict__ tab,
-                                                       int par) {
+__global__ void __launch_bounds__(256, 2) km_stream_cells(Member* __restrict__ mem, const int2* __restrict__ tab,
+                                                       int par, int cap) {
   KM_MEMBER;
   // the overflow counter of the next step starts at zero
   if (b == 0 && threadIdx.x == 0) M.fb.qn[par ^ 1] = 0;
   stream_cells_block<true>(M.p, M.s, M.f, M.c.lstart, M.c.lidx, M.c.acell, M.fb.bcnt, M.fb.bucket, M.fb.snap[par],
                            M.fb.pre[par], M.fb.queue, M.fb.qn + par, M.c.totals + 4, M.fb.border, b,
-                           (int)M.fb.bcap + kOverflowBlocks);
+                           (int)M.fb.bcap + kOverflowBlocks, cap);
 }
 
 int multi_stream(const MultiPlan& P, int par, cudaStream_t st, cudaEvent_t snap) {
   km_stream_f<<<P.blocks[MP_STREAM], 256, 0, st>>>(P.mem, P.table(MP_STREAM), par);
   if (snap) cudaStreamWaitEvent(st, snap, 0);
-  // as the plain launch (launch_stream_cells): one warp per listed cell
-  // when every member's lists are short, eight warps per cell otherwise
-  const int longest = P.cells_smem / (int)(sizeof(TriPre) + sizeof(int));
-  const int threads = longest <= kShortList ? 32 : 256;
-  km_stream_cells<<<P.blocks[MP_CELLS], threads, P.cells_smem, st>>>(P.mem, P.table(MP_CELLS), par);
-  return 2;
+  // as the plain launch (launch_stream_cells): one warp per listed cell for
+  // the members with short lists, eight warps per cell for the others, one
+  // launch per class
+  const int n0 = P.cells_short, n1 = P.blocks[MP_CELLS] - P.cells_short;
+  int k = 1;
+  if (n0 > 0) {
+    km_stream_cells<<<n0, 32, stage_bytes(P.cells_cap[0]), st>>>(P.mem, P.table(MP_CELLS), par, P.cells_cap[0]);
+    ++k;
+  }
+  if (n1 > 0) {
+    km_stream_cells<<<n1, 256, stage_bytes(P.cells_cap[1]), st>>>(P.mem, P.table(MP_CELLS) + n0, par,
+                                                                   P.cells_cap[1]);
+    ++k;
+  }
+  return k;
 }
 
 // ---- membrane chain (the wide kernels' phases) --------------------------------
@@ -165,7 +174,7 @@ int multi_collide_back(const MultiPlan& P, uint64_t eoff, bool resort, cudaStrea
 // launch attribute call (the request server sets new simulations up on
 // threads of their own while others step).
 void set_kernel_limits() {
-  const int cells = kHeavyList * (int)(sizeof(TriPre) + sizeof(int));
+  const int cells = stage_bytes(kStageLong);
   const int sums = 2 * kSumSmemT * (int)sizeof(double);
   const auto dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaFuncSetAttribute(k_stream_cells<true>, dyn, cells);
@@ -204,13 +213,12 @@ void multi_blocks(const Member& M, int out[MP_NPHASE]) {
   out[MP_MOVE] = (int)nbf(ns, 256);
 }
 
-void multi_smem(const Member& M, int out[3]) {
+void multi_smem(const Member& M, int out[2]) {
   const DevParams& p = M.p;
-  out[0] = M.fb.hcap * (int)(sizeof(TriPre) + sizeof(int));
   int n2 = 1;
   while (n2 < p.nv) n2 <<= 1;
-  out[1] = (int)sizeof(uint64_t) * n2;
-  out[2] = p.nt <= kSumSmemT ? 2 * p.nt * (int)sizeof(double) : 0;
+  out[0] = (int)sizeof(uint64_t) * n2;
+  out[1] = p.nt <= kSumSmemT ? 2 * p.nt * (int)sizeof(double) : 0;
 }
 
 }  // namespace irbc

@@ -42,7 +42,11 @@ struct MultiPlan {
   int64_t off[MP_NPHASE] = {};   // where phase k's table starts
   int n = 0;
   int blocks[MP_NPHASE] = {};    // each phase's grid
-  int cells_smem = 0;            // near-membrane streaming: the largest member's staging
+  // near-membrane streaming: phase MP_CELLS's table lists the blocks of the
+  // members staged by one-warp blocks first (cells_short of them), then the
+  // others; cells_cap[k]: the staging piece of each class's launch
+  int cells_short = 0;
+  int cells_cap[2] = {1, 1};
   int vbin_smem = 0;             // vertex binning: the largest member's sort
   int sum_smem = 0;              // ordered Sarea / Volume sums: the largest member's staging
   const int2* table(int k) const { return blk + off[k]; }
@@ -53,8 +57,8 @@ constexpr int kMultiStreamPer = 4;
 
 // blocks of each phase for one member (host)
 void multi_blocks(const Member& M, int out[MP_NPHASE]);
-// dynamic shared memory of the phases for one member (host): cells, vbin, sum
-void multi_smem(const Member& M, int out[3]);
+// dynamic shared memory of the phases for one member (host): vbin, sum
+void multi_smem(const Member& M, int out[2]);
 
 // fused launches; par = the step's parity: the snapshot buffer the
 // streaming reads and the overflow counter it uses (fb.qn[par]; the
