@@ -106,31 +106,44 @@ __device__ __forceinline__ void grid_shift(const DevParams& p, uint64_t epoch, d
 }
 
 // counting-sort slots: particle i0 + u * stride (u < K) of cell c[u] (-1:
-// none) gets a slot in its cell's counter.  Lanes of a warp with the same
-// cell share one atomic (the leader adds the group's size); the K claims
-// of a thread are issued before any result is used.
+// none) gets a slot in its cell's counter.  The particles are nearly sorted
+// by cell in memory (the physical re-sort), so lanes with equal cells mostly
+// form runs of consecutive lanes: a run's first lane adds the run's length
+// with one atomic and the run's lanes take consecutive slots from its
+// result.  Equal cells in separate runs take separate atomics; the slots
+// stay distinct and their order within a cell is free (the collision ranks
+// a cell's particles by reference index).  Runs are found with a ballot and
+// a shuffle, not with match_any (whose address-unit throughput bound the
+// count kernel).  The in-range lanes of a warp are a prefix of it (the
+// index grows with the lane).  The K claims of a thread are issued before
+// any result is used.
 constexpr int kCountPer = 4;
 template <int K>
 __device__ __forceinline__ void claim_slots(int* cnt, const int c[K], int64_t i0, int stride, int64_t n,
                                             int slot[K]) {
   const int lane = threadIdx.x & 31;
-  unsigned peers[K];
-  int leader[K], rank[K], base[K];
+  const unsigned upto = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);  // lanes <= this one
+  int head[K], base[K];
 #pragma unroll
   for (int u = 0; u < K; ++u) {
     const bool in = i0 + (int64_t)u * stride < n;
-    const unsigned act = __ballot_sync(0xffffffffu, in);
-    peers[u] = 0u; leader[u] = 0; rank[u] = 0; base[u] = 0;
-    if (in) {
-      peers[u] = __match_any_sync(act, c[u]);
-      leader[u] = __ffs(peers[u]) - 1;
-      rank[u] = __popc(peers[u] & ((1u << lane) - 1));
-      if (lane == leader[u]) base[u] = atomicAdd(&cnt[c[u]], __popc(peers[u]));
+    const int prev = __shfl_up_sync(0xffffffffu, c[u], 1);
+    const bool starts = in && (lane == 0 || prev != c[u]);
+    const unsigned heads = __ballot_sync(0xffffffffu, starts);
+    const int nin = __popc(__ballot_sync(0xffffffffu, in));
+    const unsigned mine = heads & upto;
+    head[u] = mine ? 31 - __clz(mine) : lane;
+    base[u] = 0;
+    if (starts) {
+      const unsigned after = heads & ~upto;
+      const int end = after ? __ffs(after) - 1 : nin;
+      base[u] = atomicAdd(&cnt[c[u]], end - lane);
     }
   }
 #pragma unroll
   for (int u = 0; u < K; ++u) {
-    if (i0 + (int64_t)u * stride < n) slot[u] = __shfl_sync(peers[u], base[u], leader[u]) + rank[u];
+    const int b = __shfl_sync(0xffffffffu, base[u], head[u]);
+    if (i0 + (int64_t)u * stride < n) slot[u] = b + (lane - head[u]);
   }
 }
 
