@@ -8,50 +8,74 @@
 namespace irbc {
 
 // ---- streaming -------------------------------------------------------------
-__global__ void __launch_bounds__(256) km_stream_f(Member* __restrict__ mem, const int2* __restrict__ tab,
+__global__ void __launch_bounds__(256, 4) km_stream_f(Member* __restrict__ mem, const int2* __restrict__ tab,
                                                    int par) {
   KM_MEMBER;
-  const DevParams& p = M.p;
-  const SolventF& f = M.f;
+  // copies: the descriptor is not reloaded after the stores below
+  const DevParams p = M.p;
+  const SolventF f = M.f;
   const int* __restrict__ lstart = M.c.lstart;
-  const int64_t n = f.n, i0 = (int64_t)b * blockDim.x * kMultiStreamPer + threadIdx.x;
+  const int* __restrict__ lrank = M.c.lrank;
+  int* const bcnt = M.fb.bcnt;
+  int* const bucket = M.fb.bucket;
+  int* const queue = M.fb.queue;
+  int* const qn = M.fb.qn + par;
+  const int hcap = M.fb.hcap;
+  const int64_t n = f.n;
   const float Lx = (float)p.Lx, Ly = (float)p.Ly;
-  // every load of the thread's particles first, then their cells' list
-  // bounds, then the updates: the latencies overlap
   constexpr int K = kMultiStreamPer;
-  float4 q[K], v[K];
-  int pid[K], l0[K], l1[K];
+  for (int pass = 0; pass < kMultiStreamPasses; ++pass) {
+    const int64_t i0 = ((int64_t)b * kMultiStreamPasses + pass) * blockDim.x * K + threadIdx.x;
+    if (i0 >= n) break;
+    // every load of the thread's particles first, then their cells' list
+    // bounds, then the updates: the latencies overlap
+    float4 q[K], v[K];
+    int pid[K], l0[K], l1[K];
 #pragma unroll
-  for (int u = 0; u < K; ++u) {
-    const int64_t i = i0 + (int64_t)u * blockDim.x;
-    if (i < n) { q[u] = f.pos[i]; v[u] = f.vel[i]; }
-  }
-#pragma unroll
-  for (int u = 0; u < K; ++u) {
-    const int64_t i = i0 + (int64_t)u * blockDim.x;
-    if (i < n) {
-      pid[u] = stream_cell_f(p, q[u], Lx, Ly);
-      l0[u] = __ldg(lstart + pid[u]);
-      l1[u] = __ldg(lstart + pid[u] + 1);
+    for (int u = 0; u < K; ++u) {
+      const int64_t i = i0 + (int64_t)u * blockDim.x;
+      if (i < n) { q[u] = f.pos[i]; v[u] = f.vel[i]; }
     }
-  }
 #pragma unroll
-  for (int u = 0; u < K; ++u) {
-    const int64_t i = i0 + (int64_t)u * blockDim.x;
-    if (i < n)
-      stream_f_apply(p, f, M.c.lrank, M.fb.bcnt, M.fb.bucket, M.fb.queue, M.fb.qn + par, M.fb.hcap, i, q[u], v[u],
-                     pid[u], l0[u], l1[u]);
+    for (int u = 0; u < K; ++u) {
+      const int64_t i = i0 + (int64_t)u * blockDim.x;
+      if (i < n) {
+        pid[u] = stream_cell_f(p, q[u], Lx, Ly);
+        l0[u] = __ldg(lstart + pid[u]);
+        l1[u] = __ldg(lstart + pid[u] + 1);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < K; ++u) {
+      const int64_t i = i0 + (int64_t)u * blockDim.x;
+      if (i < n) stream_f_apply(p, f, lrank, bcnt, bucket, queue, qn, hcap, i, q[u], v[u], pid[u], l0[u], l1[u]);
+    }
   }
 }
 
 __global__ void __launch_bounds__(256, 2) km_stream_cells(Member* __restrict__ mem, const int2* __restrict__ tab,
                                                        int par, int cap) {
   KM_MEMBER;
+  // copies: the descriptor is not reloaded after the walk's stores; the
+  // snapshot buffer of this parity chosen without indexing the descriptor
+  DevParams p = M.p;
+  Solvent s = M.s;
+  SolventF f = M.f;
+  const Snap sn = par ? M.fb.snap[1] : M.fb.snap[0];
+  const TriPre* const pre = par ? M.fb.pre[1] : M.fb.pre[0];
+  int* const qn = M.fb.qn;
   // the overflow counter of the next step starts at zero
-  if (b == 0 && threadIdx.x == 0) M.fb.qn[par ^ 1] = 0;
-  stream_cells_block<true>(M.p, M.s, M.f, M.c.lstart, M.c.lidx, M.c.acell, M.fb.bcnt, M.fb.bucket, M.fb.snap[par],
-                           M.fb.pre[par], M.fb.queue, M.fb.qn + par, M.c.totals + 4, M.fb.border, b,
-                           (int)M.fb.bcap + kOverflowBlocks, cap);
+  if (b == 0 && threadIdx.x == 0) qn[par ^ 1] = 0;
+  // one-warp blocks take kMultiCellsPer of the member's listed cells (its
+  // blocks of the single-simulation kernel) one after another
+  const int per = blockDim.x == 32 ? kMultiCellsPer : 1;
+  const int nblk = (int)M.fb.bcap + kOverflowBlocks;
+  for (int k = 0; k < per; ++k) {
+    const int vb = b * per + k;
+    if (vb >= nblk) break;
+    stream_cells_block<true>(p, s, f, M.c.lstart, M.c.lidx, M.c.acell, M.fb.bcnt, M.fb.bucket, sn, pre, M.fb.queue,
+                             qn + par, M.c.totals + 4, M.fb.border, vb, nblk, cap);
+  }
 }
 
 int multi_stream(const MultiPlan& P, int par, cudaStream_t st, cudaEvent_t snap) {
@@ -144,7 +168,13 @@ __global__ void __launch_bounds__(256) km_perm(Member* __restrict__ mem, const i
 __global__ void __launch_bounds__(32 * kTileWarps) km_tile(Member* __restrict__ mem, const int2* __restrict__ tab,
                                                            uint64_t eoff) {
   KM_MEMBER;
-  cells_tile_block<true>(M.p, M.s, M.f, M.c, M.m, eoff, b);
+  // copies: the descriptor is not reloaded after the tile's stores
+  const DevParams p = M.p;
+  Solvent s = M.s;
+  SolventF f = M.f;
+  const Cells c = M.c;
+  const Membrane m = M.m;
+  cells_tile_block<true>(p, s, f, c, m, eoff, b);
 }
 __global__ void __launch_bounds__(256) km_move(Member* __restrict__ mem, const int2* __restrict__ tab, int back) {
   KM_MEMBER;
@@ -192,8 +222,12 @@ void set_kernel_limits() {
 void multi_blocks(const Member& M, int out[MP_NPHASE]) {
   const DevParams& p = M.p;
   const int64_t ns = M.f.n, nc = M.c.n;
-  out[MP_STREAM] = (int)nbf(ns, 256 * kMultiStreamPer);
-  out[MP_CELLS] = (int)M.fb.bcap + kOverflowBlocks;
+  out[MP_STREAM] = (int)nbf(ns, 256 * kMultiStreamPer * kMultiStreamPasses);
+  {
+    // one-warp blocks (short lists) take kMultiCellsPer cells each
+    const int64_t cb = M.fb.bcap + kOverflowBlocks;
+    out[MP_CELLS] = (int)(stage_threads(M.fb.hcap) == 32 ? (cb + kMultiCellsPer - 1) / kMultiCellsPer : cb);
+  }
   out[MP_DRIFT] = (int)nb(p.nv, 128);
   out[MP_AV] = (int)nb(p.nt, 128);
   out[MP_SUM_EDGES] = 1 + (int)nb(2 * p.ne + p.nv, 256);

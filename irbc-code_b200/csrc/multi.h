@@ -52,8 +52,14 @@ struct MultiPlan {
   const int2* table(int k) const { return blk + off[k]; }
 };
 
-// particles per thread of the fused bulk streaming kernel
-constexpr int kMultiStreamPer = 4;
+// the fused bulk streaming kernel: particles per thread in flight at once,
+// and passes per block (a block covers 256 * kMultiStreamPer *
+// kMultiStreamPasses particles of its member, so that reading the member's
+// descriptor is paid once per that many)
+constexpr int kMultiStreamPer = 2, kMultiStreamPasses = 4;
+// listed cells per one-warp block of the fused near-membrane kernel (for
+// the same reason)
+constexpr int kMultiCellsPer = 4;
 
 // blocks of each phase for one member (host)
 void multi_blocks(const Member& M, int out[MP_NPHASE]);
@@ -80,7 +86,11 @@ int multi_collide_scan(const MultiPlan& P, cudaStream_t st);
 int multi_collide_back(const MultiPlan& P, uint64_t eoff, bool resort, cudaStream_t st);
 
 #ifdef __CUDACC__
-// this block's member and its block index within that member
+// this block's member and its block index within that member.  M refers
+// to the descriptor in global memory; a kernel that stores to global memory
+// in its loop copies the parts it reads into its own variables first
+// (through the reference, the compiler must reload them after each store,
+// which it cannot tell apart from the descriptor).
 #define KM_MEMBER                                   \
   const int2 km_e_ = __ldg(tab + blockIdx.x);       \
   const int b = km_e_.y;                            \
