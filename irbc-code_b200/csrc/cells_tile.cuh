@@ -2,14 +2,17 @@
 // and the rotation of CollisionDyn / CollisionDynmem / CollisionDynpara
 // (:700-810), as one kernel over tiles of 32 consecutive collision cells.
 //
-// One warp per tile.  The tile's particles are contiguous in perm (the
-// counting sort's output), so the warp gathers their velocity records into
-// shared memory with independent loads (no dependent chain per cell) and
-// ranks each particle within its cell by reference index (the order of
-// Cells[].sol).  Each lane then forms its cell's vcm / axis / ThE with the
-// sums in the reference's order, and the warp rotates the tile's particles
-// and writes their records back.  A tile with more particles than the shared buffer holds falls
-// back to one lane per cell reading global memory.
+// One block of two warps per tile.  The tile's particles are contiguous in
+// perm (the counting sort's output), so the block gathers their velocity
+// records into shared memory with independent loads (no dependent chain
+// per cell) and ranks each particle within its cell by reference index
+// (the order of Cells[].sol).  Lane l of the first warp then forms cell l's
+// vcm and ThE with the sums in the reference's order while lane l of the
+// second draws its axis, and the block rotates the tile's particles and
+// writes their records back.  Sharing a tile between two warps halves the
+// shared memory and the gather registers per warp.  A tile with more
+// particles than the shared buffer holds falls back to one lane per cell
+// reading global memory.
 //
 // Included by kernels.cu (FP64 solvent) and fp32.cuh (FP32-bulk solvent).
 #pragma once
@@ -63,9 +66,21 @@ __device__ __forceinline__ CellLook look_cell(const Cells& cl, const Membrane& m
   return k;
 }
 
+// the cell's membrane members: its vertices (entries [v0, v0 + nmem) of the
+// sorted (cell, vertex) keys) and whether it holds the parasite
+struct CellMembers {
+  int nmem, v0;
+  bool para;
+};
+
+// vcm (P[0..2]) and ThE (P[6]) of cell c given its n solvent particles in
+// reference order (vel_at(q, v) yields the q-th).  Sums in the order of
+// :164-258: solvent, wall ghost, vertices in vertex order, parasite,
+// membrane ghost.
 template <class VelAt>
-__device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, const Membrane& m, uint64_t epoch,
-                                         int64_t c, int n, const CellLook& look, VelAt vel_at, double P[7]) {
+__device__ __forceinline__ CellMembers cell_sums(const DevParams& p, const Cells& cl, const Membrane& m,
+                                                 uint64_t epoch, int64_t c, int n, const CellLook& look,
+                                                 VelAt vel_at, double P[7]) {
   const MemScalars* sc = m.sc;
   double vcm[3] = {0.0, 0.0, 0.0}, ncc = 0.0;
   int nc = 0;
@@ -134,18 +149,6 @@ __device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, co
     int nn = (int)ncc;
     if (nn != 0) { vcm[0] /= (double)nn; vcm[1] /= (double)nn; vcm[2] /= (double)nn; }
   }
-  // axis (:262-271): uniforms 3+2c and 4+2c of the COLLIDE_U stream (one
-  // Philox block when both fall into it)
-  double rand1, rand2;
-  {
-    const uint64_t k1 = 3 + 2 * (uint64_t)c, k2 = k1 + 1;
-    uint32_t o1[4], o2[4];
-    draw_block(p.seed, STREAM_COLLIDE_U, epoch, k1 >> 2, o1);
-    if ((k2 >> 2) == (k1 >> 2)) { for (int e = 0; e < 4; ++e) o2[e] = o1[e]; }
-    else draw_block(p.seed, STREAM_COLLIDE_U, epoch, k2 >> 2, o2);
-    rand1 = 2.0 * p.Pi * ((double)o1[k1 & 3u] * (1.0 / 4294967296.0));
-    rand2 = -1.0 + (2.0 * ((double)o2[k2 & 3u] * (1.0 / 4294967296.0)));
-  }
   double dvv = 0.0;
   for (int q = 0; q < n; ++q) {
     double v[3];
@@ -168,11 +171,34 @@ __device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, co
   double ThE = 1.0;
   if ((nc > 0) && (dvv != 0)) ThE = sqrt(3.0 * ((double)nc - 1.0) * p.Theta / (dvv));
   P[0] = vcm[0]; P[1] = vcm[1]; P[2] = vcm[2];
+  P[6] = ThE;
+  return CellMembers{nmem, v0, has_para};
+}
+
+// the collision axis of cell c (P[3..5], :262-271): uniforms 3+2c and 4+2c
+// of the COLLIDE_U stream (one Philox block when both fall into it)
+__device__ __forceinline__ void cell_axis(const DevParams& p, uint64_t epoch, int64_t c, double P[7]) {
+  double rand1, rand2;
+  {
+    const uint64_t k1 = 3 + 2 * (uint64_t)c, k2 = k1 + 1;
+    uint32_t o1[4], o2[4];
+    draw_block(p.seed, STREAM_COLLIDE_U, epoch, k1 >> 2, o1);
+    if ((k2 >> 2) == (k1 >> 2)) { for (int e = 0; e < 4; ++e) o2[e] = o1[e]; }
+    else draw_block(p.seed, STREAM_COLLIDE_U, epoch, k2 >> 2, o2);
+    rand1 = 2.0 * p.Pi * ((double)o1[k1 & 3u] * (1.0 / 4294967296.0));
+    rand2 = -1.0 + (2.0 * ((double)o2[k2 & 3u] * (1.0 / 4294967296.0)));
+  }
   P[3] = sqrt(1.0 - (rand2 * rand2)) * cos(rand1);
   P[4] = sqrt(1.0 - (rand2 * rand2)) * sin(rand1);
   P[5] = rand2;
-  P[6] = ThE;
-  // CollisionDynmem (:739-776) and CollisionDynpara (:779-810), in double
+}
+
+// CollisionDynmem (:739-776) and CollisionDynpara (:779-810), in double:
+// the cell's vertices and the parasite rotated with the cell's parameters
+__device__ __forceinline__ void cell_rotate_members(const DevParams& p, const Membrane& m, const CellMembers& cm,
+                                                    const double P[7]) {
+  const int nmem = cm.nmem, v0 = cm.v0;
+  const bool has_para = cm.para;
   for (int q = 0; q < nmem; ++q) {
     int i = (int)(m.vkey[v0 + q] & 0xffffffffu);
     double v[3] = {m.vx[i], m.vy[i], m.vz[i]};
@@ -187,13 +213,23 @@ __device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, co
   }
 }
 
-constexpr int kTileCells = 32;   // cells per warp (one per lane)
+// all seven parameters of cell c, then its vertices and parasite rotated
+template <class VelAt>
+__device__ __forceinline__ void cell_par(const DevParams& p, const Cells& cl, const Membrane& m, uint64_t epoch,
+                                         int64_t c, int n, const CellLook& look, VelAt vel_at, double P[7]) {
+  const CellMembers cm = cell_sums(p, cl, m, epoch, c, n, look, vel_at, P);
+  cell_axis(p, epoch, c, P);
+  cell_rotate_members(p, m, cm, P);
+}
+
+constexpr int kTileCells = 32;   // cells per tile (one per lane of the first warp)
 constexpr int kTileCap = 400;    // particles a tile holds in shared memory (mean 32 * navg)
-constexpr int kTileWarps = 2;    // warps per block
-constexpr int kTilePer = (kTileCap + 31) / 32;  // gathers in flight per lane (the whole tile)
+constexpr int kTileWarps = 2;    // warps per block; the block's two warps share one tile
+constexpr int kTileThreads = 32 * kTileWarps;
+constexpr int kTilePer = (kTileCap + kTileThreads - 1) / kTileThreads;  // gathers in flight per thread
 constexpr int kMaxSeg = 48;      // fallback: cells up to this size sort in registers
 
-// one warp's tile, in perm order; ord lists each cell's particles in
+// one block's tile, in perm order; ord lists each cell's particles in
 // reference order
 struct CellTile {
   double vx[kTileCap], vy[kTileCap], vz[kTileCap];
@@ -284,48 +320,51 @@ __device__ void cell_from_global(const DevParams& p, Solvent& s, SolventF& f, co
   }
 }
 
-// block `bid` of the collision tiles
+// block `bid` of the collision tiles: one tile of kTileCells consecutive
+// cells, shared by the block's two warps.  Both warps gather the tile's
+// particles and rank them; then warp 0 forms each cell's ordered sums
+// (vcm, ThE: lane l for cell l) while warp 1 draws each cell's rotation
+// axis, the two halves of the cell's parameters; warp 0 then rotates the
+// cells' membrane vertices and the parasite, and both warps rotate and
+// write back the particles.  Every value is computed by the same
+// operations in the same order as in cell_par.
 template <bool F32>
 __device__ __forceinline__ void cells_tile_block(const DevParams& p, Solvent& s, SolventF& f, const Cells& cl,
                                                  const Membrane& m, uint64_t eoff, int64_t bid) {
   const uint64_t epoch = epoch_of(p, eoff);
-  __shared__ CellTile tiles[kTileWarps];
-  const int lane = threadIdx.x & 31;
-  CellTile& t = tiles[threadIdx.x >> 5];
-  const int64_t c0 = (bid * kTileWarps + (threadIdx.x >> 5)) * kTileCells;
-  if (c0 >= p.ncell) return;  // whole warp
+  __shared__ CellTile t;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int64_t c0 = bid * kTileCells;
+  if (c0 >= p.ncell) return;  // whole block
   const int ncl = (int)min((int64_t)kTileCells, p.ncell - c0);
   const int* __restrict__ perm = s.perm;
   const int S0 = cl.start[c0];
   const int stl = cl.start[c0 + min(lane, ncl)] - S0;
-  const int total = cl.start[c0 + ncl] - S0;
+  const int total = cl.start[c0 + ncl] - S0;  // the same for the whole block
   if (total > kTileCap) {
-    if (lane < ncl) {
+    if (w == 0 && lane < ncl) {
       const int n = cl.start[c0 + lane + 1] - S0 - stl;
       cell_from_global<F32>(p, s, f, cl, m, epoch, c0 + lane, perm + S0 + stl, n);
     }
     return;
   }
-  t.st[lane] = stl;
-  if (lane == 0) t.st[kTileCells] = total;
-  __syncwarp();
-  {
-    const int e = t.st[lane + 1];
-    for (int j = stl; j < e; ++j) t.cell[j] = (unsigned char)lane;
+  if (w == 0) {
+    t.st[lane] = stl;
+    if (lane == 0) t.st[kTileCells] = total;
   }
-  // this lane's cell values, in flight during the gather
+  // warp 0's cell values, in flight during the gather
   CellLook look{};
-  if (lane < ncl) look = look_cell(cl, m, c0 + lane);
-  // gather: one record per particle; every perm entry of the tile is
-  // loaded first (coalesced), then every record, so the tile waits for
-  // two memory latencies, not two per batch.  Each lane keeps its slots'
-  // particle indices and reference indices for the write-back.
+  if (w == 0 && lane < ncl) look = look_cell(cl, m, c0 + lane);
+  // gather: one record per particle; every perm entry of the thread's
+  // slots is loaded first, then every record, so the tile waits for two
+  // memory latencies.  Each thread keeps its slots' particle and reference
+  // indices for the write-back.
   int qv[kTilePer], idv[kTilePer];
   {
     double vv[kTilePer][3];
 #pragma unroll
     for (int u = 0; u < kTilePer; ++u) {
-      const int j = u * 32 + lane;
+      const int j = u * kTileThreads + tid;
       qv[u] = j < total ? perm[S0 + j] : -1;
     }
 #pragma unroll
@@ -333,40 +372,56 @@ __device__ __forceinline__ void cells_tile_block(const DevParams& p, Solvent& s,
       if (qv[u] >= 0) load_particle<F32>(s, f, qv[u], idv[u], vv[u]);
 #pragma unroll
     for (int u = 0; u < kTilePer; ++u) {
-      const int j = u * 32 + lane;
+      const int j = u * kTileThreads + tid;
       if (qv[u] >= 0) {
         t.id[j] = idv[u];
         t.vx[j] = vv[u][0]; t.vy[j] = vv[u][1]; t.vz[j] = vv[u][2];
       }
     }
   }
-  __syncwarp();
+  __syncthreads();
+  if (w == 0) {
+    const int e = t.st[lane + 1];
+    for (int j = stl; j < e; ++j) t.cell[j] = (unsigned char)lane;
+  }
+  __syncthreads();
   // rank of each particle within its cell by reference index (indices are
   // unique): ord[b + rank] = its tile slot, the order of Cells[].sol
-  for (int j = lane; j < total; j += 32) {
+  for (int j = tid; j < total; j += kTileThreads) {
     const int l = t.cell[j], b = t.st[l], e = t.st[l + 1], me = t.id[j];
     int r = 0;
 #pragma unroll 4
     for (int u = b; u < e; ++u) r += (t.id[u] < me) ? 1 : 0;
     t.ord[b + r] = (unsigned short)j;
   }
-  __syncwarp();
+  __syncthreads();
+  CellMembers cm{0, 0, false};
   if (lane < ncl) {
-    const int b = stl, n = t.st[lane + 1] - stl;
     double P[7];
-    cell_par(p, cl, m, epoch, c0 + lane, n, look,
-             [&](int q, double v[3]) {
-               const int j = t.ord[b + q];
-               v[0] = t.vx[j]; v[1] = t.vy[j]; v[2] = t.vz[j];
-             },
-             P);
-    for (int e = 0; e < 7; ++e) t.P[lane][e] = P[e];
+    if (w == 0) {
+      const int b = stl, n = t.st[lane + 1] - stl;
+      cm = cell_sums(p, cl, m, epoch, c0 + lane, n, look,
+                     [&](int q, double v[3]) {
+                       const int j = t.ord[b + q];
+                       v[0] = t.vx[j]; v[1] = t.vy[j]; v[2] = t.vz[j];
+                     },
+                     P);
+      t.P[lane][0] = P[0]; t.P[lane][1] = P[1]; t.P[lane][2] = P[2]; t.P[lane][6] = P[6];
+    } else {
+      cell_axis(p, epoch, c0 + lane, P);
+      t.P[lane][3] = P[3]; t.P[lane][4] = P[4]; t.P[lane][5] = P[5];
+    }
   }
-  __syncwarp();
-  // rotation and write-back of this lane's slots
+  __syncthreads();
+  if (w == 0 && (cm.nmem > 0 || cm.para)) {
+    double P[7];
+    for (int e = 0; e < 7; ++e) P[e] = t.P[lane][e];
+    cell_rotate_members(p, m, cm, P);
+  }
+  // rotation and write-back of this thread's slots
 #pragma unroll
   for (int u = 0; u < kTilePer; ++u) {
-    const int j = u * 32 + lane;
+    const int j = u * kTileThreads + tid;
     if (qv[u] >= 0) {
       const double v[3] = {t.vx[j], t.vy[j], t.vz[j]};
       store_rotated<F32>(p, s, f, qv[u], idv[u], v, t.P[t.cell[j]]);
@@ -380,8 +435,7 @@ __global__ void __launch_bounds__(32 * kTileWarps) k_cells_tile(DevParams p, Sol
 }
 
 inline unsigned cells_tile_blocks(int64_t ncell) {
-  const int64_t per = (int64_t)kTileCells * kTileWarps;
-  return (unsigned)((ncell + per - 1) / per);
+  return (unsigned)((ncell + kTileCells - 1) / kTileCells);  // one tile per block
 }
 
 }  // namespace irbc
