@@ -369,7 +369,10 @@ def run_ours(args):
     if world == 1 and args.batch:
         line["batched"] = run_batched(G)
     if world == 1 and args.serve:
-        line["served"] = run_served(G, schedule=line.get("batched", {}).get("schedule"))
+        # the server's own default schedule (the pool): the batched leg's
+        # tuned schedule suits its uniform replicas, not the served mix of
+        # boxes and meshes
+        line["served"] = run_served(G)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
