@@ -8,7 +8,7 @@
 namespace irbc {
 
 // ---- streaming -------------------------------------------------------------
-__global__ void __launch_bounds__(256, 4) km_stream_f(Member* __restrict__ mem, const int2* __restrict__ tab,
+__global__ void __launch_bounds__(256, 8) km_stream_f(Member* __restrict__ mem, const int2* __restrict__ tab,
                                                    int par) {
   KM_MEMBER;
   // copies: the descriptor is not reloaded after the stores below

@@ -56,7 +56,7 @@ struct MultiPlan {
 // and passes per block (a block covers 256 * kMultiStreamPer *
 // kMultiStreamPasses particles of its member, so that reading the member's
 // descriptor is paid once per that many)
-constexpr int kMultiStreamPer = 2, kMultiStreamPasses = 4;
+constexpr int kMultiStreamPer = 1, kMultiStreamPasses = 8;
 // listed cells per one-warp block of the fused near-membrane kernel (for
 // the same reason)
 constexpr int kMultiCellsPer = 4;
