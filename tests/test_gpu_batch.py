@@ -165,3 +165,38 @@ def test_cluster_membrane_equals_wide_kernels(precision, which):
         s.close()
     assert H.compare(out[1], out[0], 0.0) == {}
     assert H.compare(out[2], out[0], 0.0) == {}
+
+
+def test_server_reports_a_failed_set_up_alone():
+    """A request whose set-up fails on the server's set-up thread (a knob
+    count above the mesh's vertex count: irbc_init rejects it) ends with
+    that error and gives its memory back; the requests around it finish and
+    equal themselves run alone."""
+    import irbc_b200 as G
+    V, E, T = H.troph()
+    nv = len(V) // 3 if np.ndim(V) == 1 else len(V)
+    reqs = []
+    for k in range(3):
+        _, p = _small(70 + k, precision=k % 2)
+        reqs.append((p, nv + 1 if k == 1 else 200, 72))
+    srv = G.Server(nthreads=2, round_steps=24)
+    ids = {}
+    for p, nk, steps in reqs:
+        ids[srv.submit(p, V, E, T, nk, steps, keep=True)] = (p, nk, steps)
+    got = []
+    while len(got) < len(reqs):
+        more = srv.poll(8, wait=60.0)
+        assert more, "server stalled"
+        got += more
+    for r in got:
+        p, nk, steps = ids[r["id"]]
+        if nk > nv:
+            assert r["status"] == G.ERR_ARG and r["sim"] is None
+            continue
+        assert r["status"] == 0
+        ref = _run_alone(p, V, E, T, nk, steps)
+        assert H.compare(r["sim"].get_state(), ref, 0.0) == {}
+        r["sim"].close()
+    st = srv.status()
+    assert st["used"] == 0 and st["active"] == 0, st
+    srv.close()
