@@ -372,7 +372,7 @@ def run_ours(args):
         # the server's own default schedule (the pool): the batched leg's
         # tuned schedule suits its uniform replicas, not the served mix of
         # boxes and meshes
-        line["served"] = run_served(G)
+        line["served"] = run_served(G, scale=args.serve_scale)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -644,6 +644,7 @@ def main():
     ap.add_argument("--serve-only", action="store_true")
     ap.add_argument("--batch-replicas", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=240)
+    ap.add_argument("--serve-scale", type=float, default=0.02)
     args = ap.parse_args()
     # at least 3; and past the third collision, so the first 24-step graph
     # is captured before the timed steps
@@ -655,7 +656,7 @@ def main():
         print(json.dumps({"batched": run_batched(G, nrep=args.batch_replicas, steps=args.batch_steps)}))
     elif args.serve_only:
         import irbc_b200 as G
-        print(json.dumps({"served": run_served(G)}))
+        print(json.dumps({"served": run_served(G, scale=args.serve_scale)}))
     else:
         run_ours(args)
 

@@ -360,6 +360,182 @@ __device__ __forceinline__ void heavy_particle(const DevParams& p, Solvent& s, S
   heavy_particle_from<F32>(p, s, f, sn, i, lane, len, tri, ids, st, indio);
 }
 
+// The overflow queue (particles of full buckets, lists longer than the
+// staging): warp gw of tw walks queued particles gw, gw + tw, ..., a warp per
+// particle, reading its cell's list from global memory.
+template <bool F32>
+__device__ __forceinline__ void overflow_walk(const DevParams& p, Solvent& s, SolventF& f,
+                                              const int* __restrict__ lstart, const int* __restrict__ lidx,
+                                              const Snap& sn, const TriPre* __restrict__ pre, const int* queue,
+                                              const int* qn, int64_t gw, int64_t tw, int lane) {
+  const int nq = *qn;
+  for (int64_t q = gw; q < nq; q += tw) {
+    const int64_t i = queue[q];
+    double X, Y, Z;
+    if constexpr (F32) { const float4 q4 = f.pos[i]; X = q4.x; Y = q4.y; Z = q4.z; }
+    else { X = s.x[i]; Y = s.y[i]; Z = s.z[i]; }
+    int fx = (int)floor(bbound(X, p.Lx));
+    int fy = (int)floor(bbound(Y, p.Ly));
+    int fz = (int)floor(Z + 1.0);
+    const int pid = cell_of(p, fx, fy, fz);
+    const int* L = lidx + lstart[pid];
+    heavy_particle<F32>(p, s, f, sn, i, lane, lstart[pid + 1] - lstart[pid],
+                        [&](int e) -> const TriPre& { return pre[L[e]]; }, [&](int e) { return L[e]; });
+  }
+}
+
+// one TriPre record through the read-only path as six 16-byte loads (the
+// records are 96 bytes from a 256-byte aligned base)
+__device__ __forceinline__ TriPre ldg_tri(const TriPre* __restrict__ q) {
+  const double2* r = reinterpret_cast<const double2*>(q);
+  const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3), e = __ldg(r + 4),
+                g = __ldg(r + 5);
+  TriPre t;
+  t.X[0] = a.x; t.X[1] = a.y; t.X[2] = b.x;
+  t.Xdt[0] = b.y; t.Xdt[1] = c.x; t.Xdt[2] = c.y;
+  t.A1[0] = d.x; t.A1[1] = d.y; t.A1[2] = e.x;
+  t.A2[0] = e.y; t.A2[1] = g.x; t.A2[2] = g.y;
+  return t;
+}
+
+// Short lists (hcap <= kShortList; small meshes: a few dozen entries and
+// about ten particles per listed cell): one warp per listed cell.  The warp
+// stages the list in its shared memory kLanePiece entries at a time, every
+// lane loading different entries, the records as twelve arrays (lanes that
+// read consecutive entries hit distinct banks).  The n particles of the
+// cell's bucket get G = 32 / n lanes each.  reflectionFed's loop
+// (Src/solfuncs.cpp:400-598) tests the entries in list order and changes
+// the particle's state only at a hit, after which the next entries are
+// tested with the new state.  So, per piece: (1) lane g of a particle
+// tests entries g, g + G, ... with the particle's state at the start of the
+// piece -- the crossing test on the precomputed normals, the full test for
+// a candidate -- up to its first hit, and the particle's first hit in list
+// order is the smallest of its lanes' (a shared atomicMin); up to that
+// entry these are exactly the loop's tests.  (2) The particle's owner lane
+// (g = 0) walks on from that entry one entry at a time, the loop itself:
+// the hit again (the same arithmetic, the same result), then the rest of
+// the piece with the changed state.  Hits are rare (a particle about to
+// cross the membrane), so (2) is mostly empty.  Virtual block vb < nact is
+// listed cell vb; the ones from nact on walk the overflow queue a warp per
+// particle.  tp / sj / shit: this warp's staging (twelve arrays of
+// kLanePiece doubles, triangle indices, first hit per particle).
+struct LaneStage {
+  double tp[12][kLanePiece];
+  int sj[kLanePiece];
+  int shit[32];
+};
+
+__device__ __forceinline__ TriPre staged_tri(const LaneStage& S, int e) {
+  TriPre q;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    q.X[k] = S.tp[k][e];
+    q.Xdt[k] = S.tp[3 + k][e];
+    q.A1[k] = S.tp[6 + k][e];
+    q.A2[k] = S.tp[9 + k][e];
+  }
+  return q;
+}
+
+template <bool F32>
+__device__ __forceinline__ void stream_cells_warp(const DevParams& p, Solvent& s, SolventF& f,
+                                                  const int* __restrict__ lstart, const int* __restrict__ lidx,
+                                                  const int* __restrict__ acell, int* bcnt,
+                                                  const int* __restrict__ bucket, const Snap& sn,
+                                                  const TriPre* __restrict__ pre, const int* queue, const int* qn,
+                                                  const int* __restrict__ nactp, int vb, int nvb, LaneStage& S) {
+  const int lane = threadIdx.x & 31;
+  const int nact = *nactp;
+  if (vb >= nact) {
+    overflow_walk<F32>(p, s, f, lstart, lidx, sn, pre, queue, qn, vb - nact, nvb - nact, lane);
+    return;
+  }
+  const int a = vb;
+  // the cell goes out beside the bucket count; lane 0 reads the count and
+  // resets it for the next step (an empty bucket stays 0)
+  const int c = __ldg(acell + a);
+  int n = 0;
+  if (lane == 0) {
+    n = bcnt[a];
+    if (n) bcnt[a] = 0;
+  }
+  n = min(__shfl_sync(0xffffffffu, n, 0), kBucket);
+  if (n == 0) return;
+  const int l0 = __ldg(lstart + c), len = __ldg(lstart + c + 1) - l0;
+  const int G = 32 / n;                     // lanes per particle
+  const int k = lane / G, g = lane - k * G;  // this lane's particle and its place among the particle's lanes
+  const bool act = k < n, own = act && g == 0;
+  int64_t i = -1;
+  double st[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, st0[6];
+  int indio = 0;
+  if (act) {
+    i = bucket[(int64_t)a * kBucket + k];
+    HeavyIO<F32>::load(s, f, i, st, indio);
+  }
+  for (int u = 0; u < 6; ++u) st0[u] = st[u];
+  double fulldt = 0.0;
+  for (int c0 = 0; c0 < len; c0 += kLanePiece) {
+    const int m = min(len - c0, kLanePiece);
+    if (c0 > 0) __syncwarp();  // every lane is done with the previous piece
+    int jj[kLanePiece / 32];
+#pragma unroll
+    for (int u = 0; u < kLanePiece / 32; ++u) {
+      const int e = lane + 32 * u;
+      jj[u] = e < m ? __ldg(lidx + l0 + c0 + e) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < kLanePiece / 32; ++u) {
+      const int e = lane + 32 * u;
+      if (e < m) {
+        const TriPre t = ldg_tri(pre + jj[u]);
+        S.sj[e] = jj[u];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          S.tp[r][e] = t.X[r];
+          S.tp[3 + r][e] = t.Xdt[r];
+          S.tp[6 + r][e] = t.A1[r];
+          S.tp[9 + r][e] = t.A2[r];
+        }
+      }
+    }
+    S.shit[lane] = m;
+    __syncwarp();
+    // (1) the particle's lanes, each up to its first hit, from the state at
+    // the start of the piece
+    if (act) {
+      const bool use_pre = !in_stencil(p, st[0], st[1]);
+      for (int e = g; e < m; e += G) {
+        const TriPre q = staged_tri(S, e);
+        if (use_pre && !tri_crossing(p, q, st[0], st[1], st[2], st[3], st[4], st[5], indio)) continue;
+        double x = st[0], y = st[1], z = st[2], vx = st[3], vy = st[4], vz = st[5], fd = 0.0;
+        if (tri_visit(p, sn, q, S.sj[e], x, y, z, vx, vy, vz, indio, fd, use_pre)) {
+          atomicMin(S.shit + k, e);
+          break;
+        }
+      }
+    }
+    __syncwarp();
+    // (2) the owner from the particle's first hit on, the loop itself;
+    // tri_visit changes the state (and adds the contact time) only at a hit
+    if (own) {
+      for (int e = S.shit[k]; e < m; ++e) {
+        const TriPre q = staged_tri(S, e);
+        const bool use_pre = !in_stencil(p, st[0], st[1]);
+        if (use_pre && !tri_crossing(p, q, st[0], st[1], st[2], st[3], st[4], st[5], indio)) continue;
+        tri_visit(p, sn, q, S.sj[e], st[0], st[1], st[2], st[3], st[4], st[5], indio, fulldt, use_pre);
+      }
+    }
+    // the particle's other lanes continue from the owner's state
+#pragma unroll
+    for (int u = 0; u < 6; ++u) st[u] = __shfl_sync(0xffffffffu, st[u], k * G);
+  }
+  if (own) {
+    finish_stream(p, fulldt, st[0], st[1], st[2], st[3], st[4], st[5]);
+    raise_health(p, solvent_bad(p, st[0], st[1], st[2], st[3], st[4], st[5]), HEALTH_SOLVENT);
+    HeavyIO<F32>::store(s, f, i, st, st0);
+  }
+}
+
 // Particles in cells with triangles (reflectionFed, Src/solfuncs.cpp:400-598,
 // then the walls and wrap).  Block a < nact takes the bucket of listed cell
 // a: its list's TriPre records and triangle indices are staged in shared
@@ -383,22 +559,8 @@ __device__ __forceinline__ void stream_cells_block(const DevParams& p, Solvent& 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int nact = *nactp;
   if (bid >= nact) {
-    const int nq = *qn;
-    const int64_t gw = (int64_t)(bid - nact) * nw + w;
-    const int64_t tw = (int64_t)(nblk - nact) * nw;
-    for (int64_t q = gw; q < nq; q += tw) {
-      const int64_t i = queue[q];
-      double X, Y, Z;
-      if constexpr (F32) { const float4 q4 = f.pos[i]; X = q4.x; Y = q4.y; Z = q4.z; }
-      else { X = s.x[i]; Y = s.y[i]; Z = s.z[i]; }
-      int fx = (int)floor(bbound(X, p.Lx));
-      int fy = (int)floor(bbound(Y, p.Ly));
-      int fz = (int)floor(Z + 1.0);
-      const int pid = cell_of(p, fx, fy, fz);
-      const int* L = lidx + lstart[pid];
-      heavy_particle<F32>(p, s, f, sn, i, lane, lstart[pid + 1] - lstart[pid],
-                          [&](int e) -> const TriPre& { return pre[L[e]]; }, [&](int e) { return L[e]; });
-    }
+    overflow_walk<F32>(p, s, f, lstart, lidx, sn, pre, queue, qn, (int64_t)(bid - nact) * nw + w,
+                       (int64_t)(nblk - nact) * nw, lane);
     return;
   }
   // Every thread reads the cell's bucket count and list bounds itself, so
@@ -471,6 +633,23 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
                                                       const int* __restrict__ border, int cap) {
   stream_cells_block<F32>(p, s, f, lstart, lidx, acell, bcnt, bucket, sn, pre, queue, qn, nactp, border,
                           (int)blockIdx.x, (int)gridDim.x, cap);
+}
+
+// the short-list form: kShortWarps warps per block, one virtual block each
+template <bool F32>
+__global__ void __launch_bounds__(32 * kShortWarps, kShortMinBlocks) k_stream_cells_short(DevParams p, Solvent s, SolventF f,
+                                                                         const int* __restrict__ lstart,
+                                                                         const int* __restrict__ lidx,
+                                                                         const int* __restrict__ acell, int* bcnt,
+                                                                         const int* __restrict__ bucket, Snap sn,
+                                                                         const TriPre* __restrict__ pre,
+                                                                         const int* queue, const int* qn,
+                                                                         const int* __restrict__ nactp, int nvb) {
+  __shared__ LaneStage stage[kShortWarps];
+  const int w = (int)(threadIdx.x >> 5);
+  const int vb = (int)blockIdx.x * kShortWarps + w;
+  if (vb >= nvb) return;
+  stream_cells_warp<F32>(p, s, f, lstart, lidx, acell, bcnt, bucket, sn, pre, queue, qn, nactp, vb, nvb, stage[w]);
 }
 
 // ========================================================= membrane step ====
@@ -1127,10 +1306,17 @@ template <bool F32>
 static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
                                 cudaStream_t st) {
   // short lists (small simulations: many listed cells of a few dozen
-  // entries, ~10 particles each): one warp per cell, so that many cells are
-  // in flight per SM; long lists: eight warps share a cell's staging.  The
-  // staging holds a piece of the list at a time (stage_cap), so its size
-  // does not grow with the longest list.
+  // entries, ~10 particles each): one warp per cell and one lane per
+  // particle, no staging; long lists: eight warps share a cell's staging,
+  // which holds a piece of the list at a time (stage_cap), so its size does
+  // not grow with the longest list.
+  const int nvb = (int)f.bcap + kOverflowBlocks;
+  if (stage_threads(f.hcap) == 32) {
+    k_stream_cells_short<F32><<<nb(nvb, kShortWarps), 32 * kShortWarps, 0, st>>>(
+        p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
+        c.totals + 4, nvb);
+    return;
+  }
   const int cap = stage_cap(f.hcap);
   k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, stage_threads(f.hcap), stage_bytes(cap), st>>>(
       p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,

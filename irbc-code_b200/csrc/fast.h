@@ -21,13 +21,21 @@ struct Snap {
 constexpr int kBucket = 32;
 constexpr int kHeavyList = 1024;
 constexpr int kOverflowBlocks = 8;
-// The near-membrane kernel stages a listed cell's TriPre records in shared
-// memory a piece at a time: one-warp blocks for staging capacities up to
-// kShortList entries (kStageShort entries per piece), eight-warp blocks
-// above (kStageLong per piece).  The kernel's registers allow two
-// eight-warp blocks per SM, which a whole 1024-entry list per block also
-// allows, so a bucketed list (at most kHeavyList entries) is one piece.
+// Lists of up to kShortList entries (staging capacity) are walked by one
+// warp per listed cell, its lanes shared among the cell's particles, from a
+// staging of kLanePiece entries per warp (kShortWarps such warps per
+// block).  Longer lists:
+// the near-membrane kernel stages a listed cell's TriPre records in shared
+// memory a piece at a time, eight warps per block (kStageLong entries per
+// piece).  The kernel's registers allow two eight-warp blocks per SM,
+// which a whole 1024-entry list per block also allows, so a bucketed list
+// (at most kHeavyList entries) is one piece.
 constexpr int kShortList = 128, kStageShort = 128, kStageLong = kHeavyList;
+constexpr int kShortWarps = 4, kLanePiece = 64;
+#ifndef IRBC_SHORT_MINB
+#define IRBC_SHORT_MINB 4
+#endif
+constexpr int kShortMinBlocks = IRBC_SHORT_MINB;
 inline int stage_threads(int hcap) { return hcap <= kShortList ? 32 : 256; }
 inline int stage_cap(int hcap) {
   const int c = hcap <= kShortList ? kStageShort : kStageLong;

@@ -66,28 +66,44 @@ __global__ void __launch_bounds__(256, 2) km_stream_cells(Member* __restrict__ m
   int* const qn = M.fb.qn;
   // the overflow counter of the next step starts at zero
   if (b == 0 && threadIdx.x == 0) qn[par ^ 1] = 0;
-  // one-warp blocks take kMultiCellsPer of the member's listed cells (its
-  // blocks of the single-simulation kernel) one after another
-  const int per = blockDim.x == 32 ? kMultiCellsPer : 1;
   const int nblk = (int)M.fb.bcap + kOverflowBlocks;
-  for (int k = 0; k < per; ++k) {
-    const int vb = b * per + k;
-    if (vb >= nblk) break;
-    stream_cells_block<true>(p, s, f, M.c.lstart, M.c.lidx, M.c.acell, M.fb.bcnt, M.fb.bucket, sn, pre, M.fb.queue,
-                             qn + par, M.c.totals + 4, M.fb.border, vb, nblk, cap);
-  }
+  stream_cells_block<true>(p, s, f, M.c.lstart, M.c.lidx, M.c.acell, M.fb.bcnt, M.fb.bucket, sn, pre, M.fb.queue,
+                           qn + par, M.c.totals + 4, M.fb.border, b, nblk, cap);
+}
+
+// members with short lists: kMultiCellsPer (= kShortWarps) warps per block,
+// each one virtual block of the single-simulation short-list kernel (a
+// listed cell, its particles' walks shared among the warp's lanes, or a
+// share of the overflow queue)
+__global__ void __launch_bounds__(32 * kShortWarps, kShortMinBlocks) km_stream_cells_short(Member* __restrict__ mem,
+                                                                          const int2* __restrict__ tab, int par) {
+  KM_MEMBER;
+  DevParams p = M.p;
+  Solvent s = M.s;
+  SolventF f = M.f;
+  const Snap sn = par ? M.fb.snap[1] : M.fb.snap[0];
+  const TriPre* const pre = par ? M.fb.pre[1] : M.fb.pre[0];
+  int* const qn = M.fb.qn;
+  if (b == 0 && threadIdx.x == 0) qn[par ^ 1] = 0;
+  __shared__ LaneStage stage[kMultiCellsPer];
+  const int nvb = (int)M.fb.bcap + kOverflowBlocks;
+  const int w = (int)(threadIdx.x >> 5);
+  const int vb = b * kMultiCellsPer + w;
+  if (vb >= nvb) return;
+  stream_cells_warp<true>(p, s, f, M.c.lstart, M.c.lidx, M.c.acell, M.fb.bcnt, M.fb.bucket, sn, pre, M.fb.queue,
+                          qn + par, M.c.totals + 4, vb, nvb, stage[w]);
 }
 
 int multi_stream(const MultiPlan& P, int par, cudaStream_t st, cudaEvent_t snap) {
   km_stream_f<<<P.blocks[MP_STREAM], 256, 0, st>>>(P.mem, P.table(MP_STREAM), par);
   if (snap) cudaStreamWaitEvent(st, snap, 0);
-  // as the plain launch (launch_stream_cells): one warp per listed cell for
-  // the members with short lists, eight warps per cell for the others, one
-  // launch per class
+  // as the plain launch (launch_stream_cells): one warp per listed cell and
+  // one lane per particle for the members with short lists, eight warps per
+  // cell for the others, one launch per class
   const int n0 = P.cells_short, n1 = P.blocks[MP_CELLS] - P.cells_short;
   int k = 1;
   if (n0 > 0) {
-    km_stream_cells<<<n0, 32, stage_bytes(P.cells_cap[0]), st>>>(P.mem, P.table(MP_CELLS), par, P.cells_cap[0]);
+    km_stream_cells_short<<<n0, 32 * kShortWarps, 0, st>>>(P.mem, P.table(MP_CELLS), par);
     ++k;
   }
   if (n1 > 0) {
@@ -224,7 +240,7 @@ void multi_blocks(const Member& M, int out[MP_NPHASE]) {
   const int64_t ns = M.f.n, nc = M.c.n;
   out[MP_STREAM] = (int)nbf(ns, 256 * kMultiStreamPer * kMultiStreamPasses);
   {
-    // one-warp blocks (short lists) take kMultiCellsPer cells each
+    // short lists: kMultiCellsPer one-warp virtual blocks per block
     const int64_t cb = M.fb.bcap + kOverflowBlocks;
     out[MP_CELLS] = (int)(stage_threads(M.fb.hcap) == 32 ? (cb + kMultiCellsPer - 1) / kMultiCellsPer : cb);
   }

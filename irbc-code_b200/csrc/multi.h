@@ -57,9 +57,9 @@ struct MultiPlan {
 // kMultiStreamPasses particles of its member, so that reading the member's
 // descriptor is paid once per that many)
 constexpr int kMultiStreamPer = 1, kMultiStreamPasses = 8;
-// listed cells per one-warp block of the fused near-membrane kernel (for
-// the same reason)
-constexpr int kMultiCellsPer = 4;
+// listed cells (one warp each) per block of the fused short-list
+// near-membrane kernel
+constexpr int kMultiCellsPer = kShortWarps;
 
 // blocks of each phase for one member (host)
 void multi_blocks(const Member& M, int out[MP_NPHASE]);
