@@ -506,13 +506,17 @@ def run_alone_timed(G, p, V, E, T, nk, steps):
     return dt, bool(np.isfinite(obs[:6]).all())
 
 
-def run_served(G, nreq=40, rate=2.0, scale=0.02, nthreads=8, schedule=None):
+def run_served(G, nreq=40, rate=2.0, scale=0.1, nthreads=8, schedule=None):
     """Poisson-arriving sweep requests admitted by the request server by
     device-memory footprint (served_requests), against the plain path: the
     same requests each run alone, and those alone times pushed through a
     one-at-a-time queue under the same arrival times.  `schedule`: a launch
     schedule (the batched leg's tuned one) applied to every admitted
-    request."""
+    request.  The step counts are the configuration's 10k..200k times
+    `scale`: at 0.1 the requests arriving at 2/s bring about twice the
+    plain path's capacity in work, so requests queue as they do at the
+    configuration's full step counts (which bring about twenty times); at
+    0.02 the GPU would sit idle half the time and nothing would queue."""
     import numpy as np
     reqs = served_requests(G, nreq, rate, scale)
     srv = G.Server(nthreads=nthreads, round_steps=96)
@@ -644,7 +648,7 @@ def main():
     ap.add_argument("--serve-only", action="store_true")
     ap.add_argument("--batch-replicas", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=240)
-    ap.add_argument("--serve-scale", type=float, default=0.02)
+    ap.add_argument("--serve-scale", type=float, default=0.1)
     args = ap.parse_args()
     # at least 3; and past the third collision, so the first 24-step graph
     # is captured before the timed steps

@@ -485,7 +485,8 @@ struct ProfScope {
 
 // the streaming kernels; in a profiling window the bulk kernel alone is
 // bracketed by a pair of events of its own
-void stream_any(irbc_handle* h, int buf, cudaStream_t st, cudaEvent_t snap = nullptr) {
+// returns the number of kernels it launched
+int stream_any(irbc_handle* h, int buf, cudaStream_t st, cudaEvent_t snap = nullptr) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->prof && !h->capturing) {
     h->ev_marks.push_back({PROF_STREAM_BULK, h->ev_used, h->ev_used + 1});
@@ -495,8 +496,8 @@ void stream_any(irbc_handle* h, int buf, cudaStream_t st, cudaEvent_t snap = nul
   // the staging capacity follows the longest list; captured steps keep the
   // largest, so that a replay stays valid after the lists grow
   h->fb.hcap = (h->graphs_on || h->capturing) ? kHeavyList : heavy_cap(h->c.lmax);
-  if (h->fp32) fast_stream_f(h->dp, h->sf, h->c, h->fb, buf, st, e0, e1, snap);
-  else fast_stream(h->dp, h->s, h->c, h->fb, buf, st, e0, e1, snap);
+  if (h->fp32) return fast_stream_f(h->dp, h->sf, h->c, h->fb, buf, st, e0, e1, snap);
+  return fast_stream(h->dp, h->s, h->c, h->fb, buf, st, e0, e1, snap);
 }
 
 }  // namespace
@@ -648,6 +649,7 @@ extern "C" void irbc_destroy(irbc_handle* h) {
   invalidate_graphs(h);
   free_fast(h->fb);
   dfree(h->fb.queue); dfree(h->fb.qn); dfree(h->fb.bcnt); dfree(h->fb.bucket); dfree(h->fb.border);
+  dfree(h->fb.arng);
   if (h->rec) cudaFree(h->rec);
   for (float4** q : {&h->sf.pos, &h->sf.vel, &h->sf.pos2, &h->sf.vel2}) dfree(*q);
   dfree(h->sf.pid); dfree(h->sf.pid2);
@@ -715,17 +717,19 @@ static int refresh_listed(irbc_handle* h) {
     dfree(f.bcnt);
     dfree(f.bucket);
     dfree(f.border);
+    dfree(f.arng);
     f.bcap = c.nact + c.nact / 2 + 64;
     CK(dalloc(&f.bcnt, f.bcap));
     CK(dalloc(&f.bucket, f.bcap * kBucket));
     CK(dalloc(&f.border, f.bcap));
+    CK(dalloc(&f.arng, f.bcap));
     CK(cudaMemsetAsync(f.bcnt, 0, sizeof(int) * f.bcap, h->st));
   }
   // the near-membrane streaming takes the listed cells longest list first,
   // so that the heaviest blocks do not start last (order of work only)
   if (c.nact > 0) {
     std::vector<int> len(c.nact), order(c.nact);
-    launch_rank_lengths(c, f.border, h->st);
+    launch_rank_lengths(c, f.border, f.arng, h->st);
     g_launches += 1;
     CK(cudaMemcpyAsync(len.data(), f.border, sizeof(int) * c.nact, cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
@@ -1123,9 +1127,8 @@ extern "C" int irbc_collide(irbc_handle* h, int64_t epoch) {
 extern "C" int irbc_stream(irbc_handle* h) {
   if (!h || !h->have_mesh) return IRBC_ERR_ARG;
   fast_snap_prep(h->dp, h->m, h->fb, 0, h->st);
-  stream_any(h, 0, h->st);
+  g_launches += 2 + stream_any(h, 0, h->st);
   h->snap_ready = false;
-  g_launches += 4;
   CK(cudaGetLastError());
   return 0;
 }
@@ -1186,11 +1189,11 @@ extern "C" int irbc_step_part1(irbc_handle* h) {
   }
   {
     ProfScope ps(h, PROF_STREAM);
-    stream_any(h, buf, h->st);
+    g_launches += stream_any(h, buf, h->st);
   }
   {
     ProfScope ps(h, PROF_MEMBRANE);
-    g_launches += 2 + fast_drift_va(h->dp, h->m, h->st, true);  // + streaming (2)
+    g_launches += fast_drift_va(h->dp, h->m, h->st, true);
   }
   h->snap_ready = false;
   CK(cudaGetLastError());
@@ -1272,9 +1275,8 @@ static int step_one(irbc_handle* h, int64_t eoff, bool last, bool dry) {
     CK(cudaEventRecord(h->ev_snap, ss));
     {
       ProfScope ps(h, PROF_STREAM, ms);
-      stream_any(h, buf, ms, h->ev_snap);
+      g_launches += stream_any(h, buf, ms, h->ev_snap);
     }
-    g_launches += 2;
     CK(cudaEventRecord(h->ev_str[buf], ms));
     {
       ProfScope ps(h, PROF_MEMBRANE, ss);

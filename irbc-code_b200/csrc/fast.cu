@@ -399,30 +399,29 @@ __device__ __forceinline__ TriPre ldg_tri(const TriPre* __restrict__ q) {
 }
 
 // Short lists (hcap <= kShortList; small meshes: a few dozen entries and
-// about ten particles per listed cell): one warp per listed cell.  The warp
-// stages the list in its shared memory kLanePiece entries at a time, every
-// lane loading different entries, the records as twelve arrays (lanes that
-// read consecutive entries hit distinct banks).  The n particles of the
-// cell's bucket get G = 32 / n lanes each.  reflectionFed's loop
-// (Src/solfuncs.cpp:400-598) tests the entries in list order and changes
-// the particle's state only at a hit, after which the next entries are
-// tested with the new state.  So, per piece: (1) lane g of a particle
-// tests entries g, g + G, ... with the particle's state at the start of the
-// piece -- the crossing test on the precomputed normals, the full test for
-// a candidate -- up to its first hit, and the particle's first hit in list
-// order is the smallest of its lanes' (a shared atomicMin); up to that
-// entry these are exactly the loop's tests.  (2) The particle's owner lane
-// (g = 0) walks on from that entry one entry at a time, the loop itself:
-// the hit again (the same arithmetic, the same result), then the rest of
-// the piece with the changed state.  Hits are rare (a particle about to
-// cross the membrane), so (2) is mostly empty.  Virtual block vb < nact is
-// listed cell vb; the ones from nact on walk the overflow queue a warp per
-// particle.  tp / sj / shit: this warp's staging (twelve arrays of
-// kLanePiece doubles, triangle indices, first hit per particle).
+// about ten particles per listed cell), in two launches.
+//
+// (1) stream_cells_warp: one warp per listed cell.  The warp stages the list
+// in its shared memory kLanePiece entries at a time, every lane loading
+// different entries, the records as twelve arrays (lanes that read
+// consecutive entries hit distinct banks).  The n particles of the cell's
+// bucket get G = 32 / n lanes each; lane g of a particle runs the crossing
+// test on the precomputed normals for entries g, g + G, ...  reflectionFed's
+// loop (Src/solfuncs.cpp:400-598) changes a particle's state only at a hit,
+// and a hit needs the crossing test to pass first, so a particle with no
+// candidate in its whole list leaves the loop unchanged: its owner lane
+// (g = 0) finishes it here (walls, wrap, write-back).  A particle with a
+// candidate, or one inside the periodic stencil bands (where every entry
+// gets the full test), is appended to the overflow queue instead: few
+// particles (about 0.6% of those in listed cells, plus the bands), and the
+// full test that only they need keeps its registers out of this kernel,
+// which would otherwise hold it to a quarter of the warps an SM can run.
+//
+// (2) the queue launch (overflow_walk): a warp per queued particle walks
+// its cell's list with the reference's loop from the start -- the bulk
+// kernel's overflow (full buckets) and the particles appended by (1).
 struct LaneStage {
   double tp[12][kLanePiece];
-  int sj[kLanePiece];
-  int shit[32];
 };
 
 __device__ __forceinline__ TriPre staged_tri(const LaneStage& S, int e) {
@@ -437,43 +436,39 @@ __device__ __forceinline__ TriPre staged_tri(const LaneStage& S, int e) {
   return q;
 }
 
+// listed cell a (a < bcap; ranks from nact on have nothing to do)
 template <bool F32>
 __device__ __forceinline__ void stream_cells_warp(const DevParams& p, Solvent& s, SolventF& f,
-                                                  const int* __restrict__ lstart, const int* __restrict__ lidx,
-                                                  const int* __restrict__ acell, int* bcnt,
-                                                  const int* __restrict__ bucket, const Snap& sn,
-                                                  const TriPre* __restrict__ pre, const int* queue, const int* qn,
-                                                  const int* __restrict__ nactp, int vb, int nvb, LaneStage& S) {
+                                                  const int* __restrict__ lidx, const int2* __restrict__ arng,
+                                                  int* bcnt, const int* __restrict__ bucket,
+                                                  const TriPre* __restrict__ pre, int* queue, int* qn,
+                                                  const int* __restrict__ nactp, int a, LaneStage& S) {
   const int lane = threadIdx.x & 31;
+  // The loads that depend only on a go out together with the count of
+  // listed cells: every rank below the bucket capacity has a bucket, a
+  // count and a range slot (stale beyond nact, and unused there), so the
+  // chain of dependent loads before the tests is count, state, list, records
+  const int2 rg = __ldg(arng + a);
+  const int slot = bucket[(int64_t)a * kBucket + lane];
+  int nraw = 0;
+  if (lane == 0) nraw = bcnt[a];
   const int nact = *nactp;
-  if (vb >= nact) {
-    overflow_walk<F32>(p, s, f, lstart, lidx, sn, pre, queue, qn, vb - nact, nvb - nact, lane);
-    return;
-  }
-  const int a = vb;
-  // the cell goes out beside the bucket count; lane 0 reads the count and
-  // resets it for the next step (an empty bucket stays 0)
-  const int c = __ldg(acell + a);
-  int n = 0;
-  if (lane == 0) {
-    n = bcnt[a];
-    if (n) bcnt[a] = 0;
-  }
-  n = min(__shfl_sync(0xffffffffu, n, 0), kBucket);
+  if (a >= nact) return;
+  // lane 0 resets the count for the next step (an empty bucket stays 0)
+  if (lane == 0 && nraw) bcnt[a] = 0;
+  const int n = min(__shfl_sync(0xffffffffu, nraw, 0), kBucket);
   if (n == 0) return;
-  const int l0 = __ldg(lstart + c), len = __ldg(lstart + c + 1) - l0;
+  const int l0 = rg.x, len = rg.y;
   const int G = 32 / n;                     // lanes per particle
   const int k = lane / G, g = lane - k * G;  // this lane's particle and its place among the particle's lanes
   const bool act = k < n, own = act && g == 0;
-  int64_t i = -1;
+  const int64_t i = __shfl_sync(0xffffffffu, slot, k);  // the particle in bucket slot k
   double st[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, st0[6];
   int indio = 0;
-  if (act) {
-    i = bucket[(int64_t)a * kBucket + k];
-    HeavyIO<F32>::load(s, f, i, st, indio);
-  }
+  if (act) HeavyIO<F32>::load(s, f, i, st, indio);
   for (int u = 0; u < 6; ++u) st0[u] = st[u];
-  double fulldt = 0.0;
+  const bool band = act && in_stencil(p, st[0], st[1]);
+  bool cand = false;
   for (int c0 = 0; c0 < len; c0 += kLanePiece) {
     const int m = min(len - c0, kLanePiece);
     if (c0 > 0) __syncwarp();  // every lane is done with the previous piece
@@ -488,7 +483,6 @@ __device__ __forceinline__ void stream_cells_warp(const DevParams& p, Solvent& s
       const int e = lane + 32 * u;
       if (e < m) {
         const TriPre t = ldg_tri(pre + jj[u]);
-        S.sj[e] = jj[u];
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
           S.tp[r][e] = t.X[r];
@@ -498,41 +492,27 @@ __device__ __forceinline__ void stream_cells_warp(const DevParams& p, Solvent& s
         }
       }
     }
-    S.shit[lane] = m;
     __syncwarp();
-    // (1) the particle's lanes, each up to its first hit, from the state at
-    // the start of the piece
-    if (act) {
-      const bool use_pre = !in_stencil(p, st[0], st[1]);
+    if (act && !band && !cand) {
       for (int e = g; e < m; e += G) {
-        const TriPre q = staged_tri(S, e);
-        if (use_pre && !tri_crossing(p, q, st[0], st[1], st[2], st[3], st[4], st[5], indio)) continue;
-        double x = st[0], y = st[1], z = st[2], vx = st[3], vy = st[4], vz = st[5], fd = 0.0;
-        if (tri_visit(p, sn, q, S.sj[e], x, y, z, vx, vy, vz, indio, fd, use_pre)) {
-          atomicMin(S.shit + k, e);
+        if (tri_crossing(p, staged_tri(S, e), st[0], st[1], st[2], st[3], st[4], st[5], indio)) {
+          cand = true;
           break;
         }
       }
     }
-    __syncwarp();
-    // (2) the owner from the particle's first hit on, the loop itself;
-    // tri_visit changes the state (and adds the contact time) only at a hit
-    if (own) {
-      for (int e = S.shit[k]; e < m; ++e) {
-        const TriPre q = staged_tri(S, e);
-        const bool use_pre = !in_stencil(p, st[0], st[1]);
-        if (use_pre && !tri_crossing(p, q, st[0], st[1], st[2], st[3], st[4], st[5], indio)) continue;
-        tri_visit(p, sn, q, S.sj[e], st[0], st[1], st[2], st[3], st[4], st[5], indio, fulldt, use_pre);
-      }
-    }
-    // the particle's other lanes continue from the owner's state
-#pragma unroll
-    for (int u = 0; u < 6; ++u) st[u] = __shfl_sync(0xffffffffu, st[u], k * G);
   }
+  // the particle's lanes are bits k*G .. k*G+G-1
+  const unsigned to_queue = __ballot_sync(0xffffffffu, act && (band || cand));
+  const unsigned mine = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (k * G));
   if (own) {
-    finish_stream(p, fulldt, st[0], st[1], st[2], st[3], st[4], st[5]);
-    raise_health(p, solvent_bad(p, st[0], st[1], st[2], st[3], st[4], st[5]), HEALTH_SOLVENT);
-    HeavyIO<F32>::store(s, f, i, st, st0);
+    if (to_queue & mine) {
+      queue[atomicAdd(qn, 1)] = (int)i;
+    } else {
+      finish_stream(p, 0.0, st[0], st[1], st[2], st[3], st[4], st[5]);
+      raise_health(p, solvent_bad(p, st[0], st[1], st[2], st[3], st[4], st[5]), HEALTH_SOLVENT);
+      HeavyIO<F32>::store(s, f, i, st, st0);
+    }
   }
 }
 
@@ -635,21 +615,30 @@ __global__ void __launch_bounds__(256) k_stream_cells(DevParams p, Solvent s, So
                           (int)blockIdx.x, (int)gridDim.x, cap);
 }
 
-// the short-list form: kShortWarps warps per block, one virtual block each
+// the short-list form: kShortWarps warps per block, one listed cell each
+// (ranks below the bucket capacity bcap)
 template <bool F32>
-__global__ void __launch_bounds__(32 * kShortWarps, kShortMinBlocks) k_stream_cells_short(DevParams p, Solvent s, SolventF f,
-                                                                         const int* __restrict__ lstart,
-                                                                         const int* __restrict__ lidx,
-                                                                         const int* __restrict__ acell, int* bcnt,
-                                                                         const int* __restrict__ bucket, Snap sn,
-                                                                         const TriPre* __restrict__ pre,
-                                                                         const int* queue, const int* qn,
-                                                                         const int* __restrict__ nactp, int nvb) {
+__global__ void __launch_bounds__(32 * kShortWarps, kShortMinBlocks)
+    k_stream_cells_short(DevParams p, Solvent s, SolventF f, const int* __restrict__ lidx,
+                         const int2* __restrict__ arng, int* bcnt, const int* __restrict__ bucket,
+                         const TriPre* __restrict__ pre, int* queue, int* qn, const int* __restrict__ nactp,
+                         int bcap) {
   __shared__ LaneStage stage[kShortWarps];
   const int w = (int)(threadIdx.x >> 5);
-  const int vb = (int)blockIdx.x * kShortWarps + w;
-  if (vb >= nvb) return;
-  stream_cells_warp<F32>(p, s, f, lstart, lidx, acell, bcnt, bucket, sn, pre, queue, qn, nactp, vb, nvb, stage[w]);
+  const int a = (int)blockIdx.x * kShortWarps + w;
+  if (a >= bcap) return;
+  stream_cells_warp<F32>(p, s, f, lidx, arng, bcnt, bucket, pre, queue, qn, nactp, a, stage[w]);
+}
+
+// the queue after the short-list form: a warp per queued particle
+template <bool F32>
+__global__ void __launch_bounds__(256, 2) k_stream_queue(DevParams p, Solvent s, SolventF f,
+                                                      const int* __restrict__ lstart, const int* __restrict__ lidx,
+                                                      Snap sn, const TriPre* __restrict__ pre, const int* queue,
+                                                      const int* qn) {
+  const int64_t tw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  overflow_walk<F32>(p, s, f, lstart, lidx, sn, pre, queue, qn, gw, tw, threadIdx.x & 31);
 }
 
 // ========================================================= membrane step ====
@@ -1270,14 +1259,16 @@ bool is_membrane_kernel(const void* fn) {
   return false;
 }
 
-__global__ void k_rank_lengths(Cells c, int nact, int* len) {
+__global__ void k_rank_lengths(Cells c, int nact, int* len, int2* rng) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= nact) return;
   const int cell = c.acell[a];
-  len[a] = c.lstart[cell + 1] - c.lstart[cell];
+  const int l0 = c.lstart[cell];
+  len[a] = c.lstart[cell + 1] - l0;
+  rng[a] = make_int2(l0, c.lstart[cell + 1] - l0);
 }
-void launch_rank_lengths(const Cells& c, int* len, cudaStream_t st) {
-  if (c.nact > 0) k_rank_lengths<<<nb(c.nact, 256), 256, 0, st>>>(c, c.nact, len);
+void launch_rank_lengths(const Cells& c, int* len, int2* rng, cudaStream_t st) {
+  if (c.nact > 0) k_rank_lengths<<<nb(c.nact, 256), 256, 0, st>>>(c, c.nact, len, rng);
 }
 
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st) {
@@ -1302,29 +1293,32 @@ int fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaSt
   return 2;
 }
 
+// returns the number of kernels it launched
 template <bool F32>
-static void launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
-                                cudaStream_t st) {
+static int launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, const Cells& c, FastBufs& f, int buf,
+                               cudaStream_t st) {
   // short lists (small simulations: many listed cells of a few dozen
   // entries, ~10 particles each): one warp per cell and one lane per
   // particle, no staging; long lists: eight warps share a cell's staging,
   // which holds a piece of the list at a time (stage_cap), so its size does
   // not grow with the longest list.
-  const int nvb = (int)f.bcap + kOverflowBlocks;
   if (stage_threads(f.hcap) == 32) {
-    k_stream_cells_short<F32><<<nb(nvb, kShortWarps), 32 * kShortWarps, 0, st>>>(
-        p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
-        c.totals + 4, nvb);
-    return;
+    if (f.bcap > 0)
+      k_stream_cells_short<F32><<<nb(f.bcap, kShortWarps), 32 * kShortWarps, 0, st>>>(
+          p, s, sf, c.lidx, f.arng, f.bcnt, f.bucket, f.pre[buf], f.queue, f.qn, c.totals + 4, (int)f.bcap);
+    k_stream_queue<F32><<<kQueueBlocks, 256, 0, st>>>(p, s, sf, c.lstart, c.lidx, f.snap[buf], f.pre[buf], f.queue,
+                                                      f.qn);
+    return f.bcap > 0 ? 2 : 1;
   }
   const int cap = stage_cap(f.hcap);
   k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, stage_threads(f.hcap), stage_bytes(cap), st>>>(
       p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
       c.totals + 4, f.border, cap);
+  return 1;
 }
 
-void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
-                 cudaEvent_t ev0, cudaEvent_t ev1, cudaEvent_t snap) {
+int fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
+                cudaEvent_t ev0, cudaEvent_t ev1, cudaEvent_t snap) {
   cudaMemsetAsync(f.qn, 0, sizeof(int), st);
   if (s.n) {
     if (ev0) cudaEventRecord(ev0, st);
@@ -1333,8 +1327,9 @@ void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, in
     if (ev1) cudaEventRecord(ev1, st);
     if (snap) cudaStreamWaitEvent(st, snap, 0);
     SolventF none;
-    launch_stream_cells<false>(p, s, none, c, f, buf, st);
+    return 1 + launch_stream_cells<false>(p, s, none, c, f, buf, st);
   }
+  return 0;
 }
 
 // drift and the per-triangle TotalVA terms; with_sum also forms Sarea and

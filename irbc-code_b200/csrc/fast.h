@@ -32,10 +32,12 @@ constexpr int kOverflowBlocks = 8;
 // (at most kHeavyList entries) is one piece.
 constexpr int kShortList = 128, kStageShort = 128, kStageLong = kHeavyList;
 constexpr int kShortWarps = 4, kLanePiece = 64;
-#ifndef IRBC_SHORT_MINB
-#define IRBC_SHORT_MINB 4
-#endif
-constexpr int kShortMinBlocks = IRBC_SHORT_MINB;
+// blocks of eight warps that walk the overflow queue after the short-list
+// kernel: per simulation alone, and per member of a cohort
+constexpr int kQueueBlocks = 64, kQueueBlocksMember = 32;
+// the short-list kernel runs without the full test's registers: 64 per
+// thread, eight blocks (32 warps) per SM
+constexpr int kShortMinBlocks = 8;
 inline int stage_threads(int hcap) { return hcap <= kShortList ? 32 : 256; }
 inline int stage_cap(int hcap) {
   const int c = hcap <= kShortList ? kStageShort : kStageLong;
@@ -52,6 +54,7 @@ struct FastBufs {
   int* bucket = nullptr;  // kBucket particle slots per listed cell
   int64_t bcap = 0;       // listed cells the buckets have room for
   int* border = nullptr;  // the listed cell (rank) of each k_stream_cells block: longest lists first
+  int2* arng = nullptr;   // (first entry, length) of each listed cell's list, by rank (bcap of them)
   bool one_block = false; // the membrane step as one block per launch (small meshes)
   bool cluster = false;   // the membrane step as one launch of a thread-block cluster (any mesh)
   int hcap = kHeavyList;  // list entries k_stream_cells stages (its shared memory); longer lists go
@@ -67,8 +70,9 @@ struct FastBufs {
 // these return the number of kernels they launched
 int fast_kick_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
 void fast_snap_prep(const DevParams& p, Membrane& m, FastBufs& f, int buf, cudaStream_t st);
-// list length of each listed cell (rank a < nact) into len[a]
-void launch_rank_lengths(const Cells& c, int* len, cudaStream_t st);
+// list length of each listed cell (rank a < nact) into len[a], and its
+// (first entry, length) into rng[a]
+void launch_rank_lengths(const Cells& c, int* len, int2* rng, cudaStream_t st);
 // the staging capacity for lists of at most lmax entries: lmax rounded up
 // to 64, at least 64, at most kHeavyList
 inline int heavy_cap(int lmax) {
@@ -76,10 +80,11 @@ inline int heavy_cap(int lmax) {
   return c < 64 ? 64 : (c > kHeavyList ? kHeavyList : c);
 }
 // ev0/ev1 (optional) are recorded around the bulk kernel k_stream_fast.  The
-// bulk kernel reads no membrane data; the near-membrane kernel reads the
-// snapshot `buf` and first waits for `snap` (optional: its producer)
-void fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
-                 cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr, cudaEvent_t snap = nullptr);
+// bulk kernel reads no membrane data; the near-membrane kernels read the
+// snapshot `buf` and first wait for `snap` (optional: its producer).
+// Returns the number of kernels it launched.
+int fast_stream(const DevParams& p, Solvent& s, const Cells& c, FastBufs& f, int buf, cudaStream_t st,
+                cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr, cudaEvent_t snap = nullptr);
 // these return the number of kernels they launched
 int fast_drift_va(const DevParams& p, Membrane& m, cudaStream_t st, bool with_sum);
 bool is_membrane_kernel(const void* fn);

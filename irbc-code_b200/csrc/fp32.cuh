@@ -190,8 +190,8 @@ __global__ void __launch_bounds__(256) k_stream_f(DevParams p, SolventF f, const
   stream_f_item(p, f, lstart, lrank, bcnt, bucket, queue, qn, hcap, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-void fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb, int buf, cudaStream_t st,
-                   cudaEvent_t ev0, cudaEvent_t ev1, cudaEvent_t snap) {
+int fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb, int buf, cudaStream_t st,
+                  cudaEvent_t ev0, cudaEvent_t ev1, cudaEvent_t snap) {
   cudaMemsetAsync(fb.qn, 0, sizeof(int), st);
   if (f.n) {
     if (ev0) cudaEventRecord(ev0, st);
@@ -201,8 +201,9 @@ void fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb
     if (snap) cudaStreamWaitEvent(st, snap, 0);
     Solvent none;
     none.n = f.n;
-    launch_stream_cells<true>(p, none, f, c, fb, buf, st);
+    return 1 + launch_stream_cells<true>(p, none, f, c, fb, buf, st);
   }
+  return 0;
 }
 
 }  // namespace irbc

@@ -21,8 +21,9 @@ void launch_collide_finish_f(const DevParams& p, SolventF& f, Solvent& s, Cells&
                              cudaStream_t st, bool resort);
 void launch_resort_f(SolventF& f, Solvent& s, cudaStream_t st);
 // ev0/ev1 (optional) are recorded around the bulk kernel k_stream_f; the
-// near-membrane kernel waits for `snap` (optional: the snapshot's producer)
-void fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb, int buf, cudaStream_t st,
-                   cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr, cudaEvent_t snap = nullptr);
+// near-membrane kernels wait for `snap` (optional: the snapshot's
+// producer).  Returns the number of kernels it launched.
+int fast_stream_f(const DevParams& p, SolventF& f, const Cells& c, FastBufs& fb, int buf, cudaStream_t st,
+                  cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr, cudaEvent_t snap = nullptr);
 
 }  // namespace irbc

@@ -72,26 +72,38 @@ __global__ void __launch_bounds__(256, 2) km_stream_cells(Member* __restrict__ m
 }
 
 // members with short lists: kMultiCellsPer (= kShortWarps) warps per block,
-// each one virtual block of the single-simulation short-list kernel (a
-// listed cell, its particles' walks shared among the warp's lanes, or a
-// share of the overflow queue)
-__global__ void __launch_bounds__(32 * kShortWarps, kShortMinBlocks) km_stream_cells_short(Member* __restrict__ mem,
-                                                                          const int2* __restrict__ tab, int par) {
+// each one listed cell of the single-simulation short-list kernel
+__global__ void __launch_bounds__(32 * kShortWarps, kShortMinBlocks)
+    km_stream_cells_short(Member* __restrict__ mem, const int2* __restrict__ tab, int par) {
+  KM_MEMBER;
+  DevParams p = M.p;
+  Solvent s = M.s;
+  SolventF f = M.f;
+  const TriPre* const pre = par ? M.fb.pre[1] : M.fb.pre[0];
+  int* const qn = M.fb.qn;
+  // the overflow counter of the next step starts at zero
+  if (b == 0 && threadIdx.x == 0) qn[par ^ 1] = 0;
+  __shared__ LaneStage stage[kMultiCellsPer];
+  const int w = (int)(threadIdx.x >> 5);
+  const int a = b * kMultiCellsPer + w;
+  if (a >= (int)M.fb.bcap) return;
+  stream_cells_warp<true>(p, s, f, M.c.lidx, M.fb.arng, M.fb.bcnt, M.fb.bucket, pre, M.fb.queue, qn + par,
+                          M.c.totals + 4, a, stage[w]);
+}
+
+// then their queues (the bulk kernel's overflow and the particles the
+// short-list kernel handed on): kQueueBlocksMember blocks per member
+__global__ void __launch_bounds__(256, 2) km_stream_queue(Member* __restrict__ mem, const int2* __restrict__ tab,
+                                                       int par) {
   KM_MEMBER;
   DevParams p = M.p;
   Solvent s = M.s;
   SolventF f = M.f;
   const Snap sn = par ? M.fb.snap[1] : M.fb.snap[0];
   const TriPre* const pre = par ? M.fb.pre[1] : M.fb.pre[0];
-  int* const qn = M.fb.qn;
-  if (b == 0 && threadIdx.x == 0) qn[par ^ 1] = 0;
-  __shared__ LaneStage stage[kMultiCellsPer];
-  const int nvb = (int)M.fb.bcap + kOverflowBlocks;
-  const int w = (int)(threadIdx.x >> 5);
-  const int vb = b * kMultiCellsPer + w;
-  if (vb >= nvb) return;
-  stream_cells_warp<true>(p, s, f, M.c.lstart, M.c.lidx, M.c.acell, M.fb.bcnt, M.fb.bucket, sn, pre, M.fb.queue,
-                          qn + par, M.c.totals + 4, vb, nvb, stage[w]);
+  const int64_t gw = (int64_t)b * 8 + (threadIdx.x >> 5);
+  overflow_walk<true>(p, s, f, M.c.lstart, M.c.lidx, sn, pre, M.fb.queue, M.fb.qn + par, gw,
+                      (int64_t)kQueueBlocksMember * 8, threadIdx.x & 31);
 }
 
 int multi_stream(const MultiPlan& P, int par, cudaStream_t st, cudaEvent_t snap) {
@@ -104,6 +116,10 @@ int multi_stream(const MultiPlan& P, int par, cudaStream_t st, cudaEvent_t snap)
   int k = 1;
   if (n0 > 0) {
     km_stream_cells_short<<<n0, 32 * kShortWarps, 0, st>>>(P.mem, P.table(MP_CELLS), par);
+    ++k;
+  }
+  if (P.blocks[MP_QUEUE] > 0) {
+    km_stream_queue<<<P.blocks[MP_QUEUE], 256, 0, st>>>(P.mem, P.table(MP_QUEUE), par);
     ++k;
   }
   if (n1 > 0) {
@@ -226,6 +242,11 @@ void set_kernel_limits() {
   cudaFuncSetAttribute(k_stream_cells<true>, dyn, cells);
   cudaFuncSetAttribute(k_stream_cells<false>, dyn, cells);
   cudaFuncSetAttribute(km_stream_cells, dyn, cells);
+  // eight blocks of the short-list kernels (24 KB of staging each) per SM
+  const auto carve = cudaFuncAttributePreferredSharedMemoryCarveout;
+  cudaFuncSetAttribute(k_stream_cells_short<true>, carve, (int)cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(k_stream_cells_short<false>, carve, (int)cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(km_stream_cells_short, carve, (int)cudaSharedmemCarveoutMaxShared);
   cudaFuncSetAttribute(k_m_sum, dyn, sums);
   cudaFuncSetAttribute(k_sum_edges, dyn, sums);
   cudaFuncSetAttribute(km_sum_edges, dyn, sums);
@@ -240,9 +261,11 @@ void multi_blocks(const Member& M, int out[MP_NPHASE]) {
   const int64_t ns = M.f.n, nc = M.c.n;
   out[MP_STREAM] = (int)nbf(ns, 256 * kMultiStreamPer * kMultiStreamPasses);
   {
-    // short lists: kMultiCellsPer one-warp virtual blocks per block
-    const int64_t cb = M.fb.bcap + kOverflowBlocks;
-    out[MP_CELLS] = (int)(stage_threads(M.fb.hcap) == 32 ? (cb + kMultiCellsPer - 1) / kMultiCellsPer : cb);
+    // short lists: kMultiCellsPer listed cells per block, then the queue
+    // walk; long lists: a block per listed cell and the overflow blocks
+    const bool shrt = stage_threads(M.fb.hcap) == 32;
+    out[MP_CELLS] = (int)(shrt ? (M.fb.bcap + kMultiCellsPer - 1) / kMultiCellsPer : M.fb.bcap + kOverflowBlocks);
+    out[MP_QUEUE] = shrt ? kQueueBlocksMember : 0;
   }
   out[MP_DRIFT] = (int)nb(p.nv, 128);
   out[MP_AV] = (int)nb(p.nt, 128);

@@ -26,7 +26,7 @@ struct Member {
 };
 
 enum MultiPhase : int {
-  MP_STREAM, MP_CELLS,                                            // streaming
+  MP_STREAM, MP_CELLS, MP_QUEUE,                                  // streaming
   MP_DRIFT, MP_AV, MP_SUM_EDGES, MP_FORCE_TRI, MP_GATHER, MP_TAIL,  // membrane
   MP_KICK, MP_TRI_PREP,                                           // next half-kick and snapshot
   MP_ZERO, MP_VBIN, MP_COUNT, MP_GHOST, MP_SCAN, MP_SCAN_TOP, MP_PERM, MP_TILE, MP_MOVE,  // collision
@@ -43,8 +43,9 @@ struct MultiPlan {
   int n = 0;
   int blocks[MP_NPHASE] = {};    // each phase's grid
   // near-membrane streaming: phase MP_CELLS's table lists the blocks of the
-  // members staged by one-warp blocks first (cells_short of them), then the
-  // others; cells_cap[k]: the staging piece of each class's launch
+  // members with short lists first (cells_short of them), then the others;
+  // cells_cap[k]: the staging piece of each class's launch.  MP_QUEUE: the
+  // queue walk after the short-list kernel (short-list members only)
   int cells_short = 0;
   int cells_cap[2] = {1, 1};
   int vbin_smem = 0;             // vertex binning: the largest member's sort
