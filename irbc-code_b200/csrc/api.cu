@@ -1564,8 +1564,8 @@ static int cohort_upload(Cohort* c) {
   int64_t tot[MP_NPHASE] = {};
   P.vbin_smem = P.sum_smem = 0;
   P.cells_short = 0;
-  P.cells_cap[0] = P.cells_cap[1] = 1;
-  std::vector<int> cls(n);  // the near-membrane class of each member: 0 one-warp blocks, 1 eight-warp
+  P.cells_cap = 1;
+  std::vector<int> cls(n);  // the near-membrane class of each member: 0 short lists, 1 long lists
   for (size_t r = 0; r < n; ++r) {
     c->host[r] = member_of(c->members[r]);
     c->uids[r] = c->members[r]->uid;
@@ -1574,9 +1574,9 @@ static int cohort_upload(Cohort* c) {
     multi_smem(c->host[r], sm);
     for (int k = 0; k < MP_NPHASE; ++k) tot[k] += nbk[r][k];
     const int hcap = c->host[r].fb.hcap;
-    cls[r] = stage_threads(hcap) == 32 ? 0 : 1;
+    cls[r] = short_lists(hcap) ? 0 : 1;
     if (cls[r] == 0) P.cells_short += nbk[r][MP_CELLS];
-    P.cells_cap[cls[r]] = std::max(P.cells_cap[cls[r]], stage_cap(hcap));
+    else P.cells_cap = std::max(P.cells_cap, stage_cap(hcap));
     P.vbin_smem = std::max(P.vbin_smem, sm[0]);
     P.sum_smem = std::max(P.sum_smem, sm[1]);
   }

@@ -516,7 +516,7 @@ __device__ __forceinline__ void stream_cells_warp(const DevParams& p, Solvent& s
   }
 }
 
-// Particles in cells with triangles (reflectionFed, Src/solfuncs.cpp:400-598,
+// Particles in cells with long lists (reflectionFed, Src/solfuncs.cpp:400-598,
 // then the walls and wrap).  Block a < nact takes the bucket of listed cell
 // a: its list's TriPre records and triangle indices are staged in shared
 // memory once, then each warp walks one particle of the bucket at a time
@@ -1302,7 +1302,7 @@ static int launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, con
   // particle, no staging; long lists: eight warps share a cell's staging,
   // which holds a piece of the list at a time (stage_cap), so its size does
   // not grow with the longest list.
-  if (stage_threads(f.hcap) == 32) {
+  if (short_lists(f.hcap)) {
     if (f.bcap > 0)
       k_stream_cells_short<F32><<<nb(f.bcap, kShortWarps), 32 * kShortWarps, 0, st>>>(
           p, s, sf, c.lidx, f.arng, f.bcnt, f.bucket, f.pre[buf], f.queue, f.qn, c.totals + 4, (int)f.bcap);
@@ -1311,7 +1311,7 @@ static int launch_stream_cells(const DevParams& p, Solvent& s, SolventF& sf, con
     return f.bcap > 0 ? 2 : 1;
   }
   const int cap = stage_cap(f.hcap);
-  k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, stage_threads(f.hcap), stage_bytes(cap), st>>>(
+  k_stream_cells<F32><<<(unsigned)f.bcap + kOverflowBlocks, 256, stage_bytes(cap), st>>>(
       p, s, sf, c.lstart, c.lidx, c.acell, f.bcnt, f.bucket, f.snap[buf], f.pre[buf], f.queue, f.qn,
       c.totals + 4, f.border, cap);
   return 1;

@@ -21,16 +21,16 @@ struct Snap {
 constexpr int kBucket = 32;
 constexpr int kHeavyList = 1024;
 constexpr int kOverflowBlocks = 8;
-// Lists of up to kShortList entries (staging capacity) are walked by one
-// warp per listed cell, its lanes shared among the cell's particles, from a
-// staging of kLanePiece entries per warp (kShortWarps such warps per
-// block).  Longer lists:
-// the near-membrane kernel stages a listed cell's TriPre records in shared
-// memory a piece at a time, eight warps per block (kStageLong entries per
-// piece).  The kernel's registers allow two eight-warp blocks per SM,
-// which a whole 1024-entry list per block also allows, so a bucketed list
-// (at most kHeavyList entries) is one piece.
-constexpr int kShortList = 128, kStageShort = 128, kStageLong = kHeavyList;
+// Lists of up to kShortList entries (staging capacity hcap) take the
+// short-list path: one warp per listed cell, its lanes shared among the
+// cell's particles, from a staging of kLanePiece entries per warp
+// (kShortWarps such warps per block), then the overflow queue's walk.
+// Longer lists: the near-membrane kernel stages a listed cell's TriPre
+// records in shared memory a piece at a time, eight warps per block
+// (kStageLong entries per piece).  The kernel's registers allow two
+// eight-warp blocks per SM, which a whole 1024-entry list per block also
+// allows, so a bucketed list (at most kHeavyList entries) is one piece.
+constexpr int kShortList = 128, kStageLong = kHeavyList;
 constexpr int kShortWarps = 4, kLanePiece = 64;
 // blocks of eight warps that walk the overflow queue after the short-list
 // kernel: per simulation alone, and per member of a cohort
@@ -38,11 +38,9 @@ constexpr int kQueueBlocks = 64, kQueueBlocksMember = 32;
 // the short-list kernel runs without the full test's registers: 64 per
 // thread, eight blocks (32 warps) per SM
 constexpr int kShortMinBlocks = 8;
-inline int stage_threads(int hcap) { return hcap <= kShortList ? 32 : 256; }
-inline int stage_cap(int hcap) {
-  const int c = hcap <= kShortList ? kStageShort : kStageLong;
-  return hcap < c ? (hcap > 0 ? hcap : 1) : c;
-}
+inline bool short_lists(int hcap) { return hcap <= kShortList; }
+// the staging piece of the long-list kernel
+inline int stage_cap(int hcap) { return hcap < kStageLong ? (hcap > 0 ? hcap : 1) : kStageLong; }
 inline int stage_bytes(int cap) { return cap * (int)(sizeof(TriPre) + sizeof(int)); }
 
 struct FastBufs {

@@ -53,6 +53,8 @@ __global__ void __launch_bounds__(256, 8) km_stream_f(Member* __restrict__ mem, 
   }
 }
 
+// members with long lists: a block per listed cell (and the overflow
+// blocks) of the single-simulation long-list kernel
 __global__ void __launch_bounds__(256, 2) km_stream_cells(Member* __restrict__ mem, const int2* __restrict__ tab,
                                                        int par, int cap) {
   KM_MEMBER;
@@ -123,8 +125,7 @@ int multi_stream(const MultiPlan& P, int par, cudaStream_t st, cudaEvent_t snap)
     ++k;
   }
   if (n1 > 0) {
-    km_stream_cells<<<n1, 256, stage_bytes(P.cells_cap[1]), st>>>(P.mem, P.table(MP_CELLS) + n0, par,
-                                                                   P.cells_cap[1]);
+    km_stream_cells<<<n1, 256, stage_bytes(P.cells_cap), st>>>(P.mem, P.table(MP_CELLS) + n0, par, P.cells_cap);
     ++k;
   }
   return k;
@@ -263,7 +264,7 @@ void multi_blocks(const Member& M, int out[MP_NPHASE]) {
   {
     // short lists: kMultiCellsPer listed cells per block, then the queue
     // walk; long lists: a block per listed cell and the overflow blocks
-    const bool shrt = stage_threads(M.fb.hcap) == 32;
+    const bool shrt = short_lists(M.fb.hcap);
     out[MP_CELLS] = (int)(shrt ? (M.fb.bcap + kMultiCellsPer - 1) / kMultiCellsPer : M.fb.bcap + kOverflowBlocks);
     out[MP_QUEUE] = shrt ? kQueueBlocksMember : 0;
   }

@@ -44,10 +44,10 @@ struct MultiPlan {
   int blocks[MP_NPHASE] = {};    // each phase's grid
   // near-membrane streaming: phase MP_CELLS's table lists the blocks of the
   // members with short lists first (cells_short of them), then the others;
-  // cells_cap[k]: the staging piece of each class's launch.  MP_QUEUE: the
+  // cells_cap: the staging piece of the long-list launch.  MP_QUEUE: the
   // queue walk after the short-list kernel (short-list members only)
   int cells_short = 0;
-  int cells_cap[2] = {1, 1};
+  int cells_cap = 1;
   int vbin_smem = 0;             // vertex binning: the largest member's sort
   int sum_smem = 0;              // ordered Sarea / Volume sums: the largest member's staging
   const int2* table(int k) const { return blk + off[k]; }
