@@ -210,9 +210,9 @@ __device__ __forceinline__ bool in_stencil(const DevParams& p, double x, double 
 }
 
 // hand-off of a particle whose cell has triangles: into the bucket of its
-// cell (rank lrank among the listed cells) when the list fits the shared
-// staging of k_stream_cells and the bucket has room, else onto the overflow
-// queue
+// cell (rank lrank among the listed cells) when the list fits the staging
+// capacity hcap of the near-membrane kernels and the bucket has room, else
+// onto the overflow queue
 __device__ __forceinline__ void hand_off(const int* __restrict__ lrank, int pid, int len, int hcap, int i,
                                          int* bcnt, int* bucket, int* queue, int* qn) {
   if (len <= hcap) {
@@ -225,8 +225,8 @@ __device__ __forceinline__ void hand_off(const int* __restrict__ lrank, int pid,
 }
 
 // one thread per particle: free flight, walls and wrap for particles whose
-// cell has no triangles; the others are handed to k_stream_cells and left
-// untouched here
+// cell has no triangles; the others are handed to the near-membrane kernels
+// and left untouched here
 __global__ void __launch_bounds__(256) k_stream_fast(DevParams p, Solvent s, const int* __restrict__ lstart,
                                                      const int* __restrict__ lrank, int* bcnt, int* bucket,
                                                      int* queue, int* qn, int hcap) {

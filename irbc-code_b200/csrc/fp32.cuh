@@ -135,7 +135,8 @@ void launch_resort_f(SolventF& f, Solvent& s, cudaStream_t st) {
 
 // ---- streaming ------------------------------------------------------------------
 // free flight, walls and wrap in float (maincode.cpp:516-560); particles in
-// cells with triangles are handed to k_stream_cells<true> (double precision)
+// cells with triangles are handed to the near-membrane kernels (double
+// precision)
 // the shifted-free cell of a position (the list lookup of the streaming)
 __device__ __forceinline__ int stream_cell_f(const DevParams& p, float4 q, float Lx, float Ly) {
   int fx = (int)floorf(bbound(q.x, Lx));
@@ -146,7 +147,7 @@ __device__ __forceinline__ int stream_cell_f(const DevParams& p, float4 q, float
 
 // free flight, walls and wrap of particle i, loaded as (q, v), whose cell
 // pid has the list [l0, l1): particles in cells with triangles are handed
-// to k_stream_cells<true> (double precision)
+// to the near-membrane kernels (double precision)
 __device__ __forceinline__ void stream_f_apply(const DevParams& p, const SolventF& f, const int* __restrict__ lrank,
                                                int* bcnt, int* bucket, int* queue, int* qn, int hcap, int64_t i,
                                                float4 q, float4 v, int pid, int l0, int l1) {
